@@ -1,0 +1,187 @@
+/*
+ * specsim3d_gpu.h -- C ABI of the B200 implementation of the SPECSIM3D
+ * spectral simulation path (library: specsim3d_b200/lib/libspecsim3d_gpu.so).
+ *
+ * The reference (src/specsim3d.f90) has no library interface: its stages are
+ * inline code of `program specsim3d`.  Every entry point below names the
+ * reference lines whose behaviour it replaces.  Plain C types only; no
+ * CUDA or torch types appear in the signatures.
+ *
+ * Conventions
+ *   - Every function returns an int status: 0 on success, a SS3D_E* code on
+ *     failure, with a message available from ss3d_last_error().  The library
+ *     never calls exit().
+ *   - Fortran integer -> int32_t (int), real(dp) -> double, integer(8) -> int64_t.
+ *   - Grid arrays follow the Fortran layout res(nx,ny,nz,nreal): x fastest, i.e.
+ *     C order [nreal][nz][ny][nx].
+ *   - Output and in/out arrays may be host or device pointers; the library
+ *     detects which.  The library owns device memory behind opaque handles.
+ *   - Handles are thread-compatible, not thread-safe.  Work is issued on the
+ *     stream set with ss3d_set_stream (default: the legacy default stream) and
+ *     every call returns after its results are complete.
+ */
+#ifndef SPECSIM3D_GPU_H
+#define SPECSIM3D_GPU_H
+
+#include <stdint.h>
+
+#ifdef __cplusplus
+extern "C" {
+#endif
+
+#define SS3D_OK 0
+#define SS3D_EINVAL 1     /* invalid argument (message says which) */
+#define SS3D_ECUDA 2      /* CUDA runtime error */
+#define SS3D_ENOMEM 3     /* device memory exhausted */
+#define SS3D_ETOOLARGE 4  /* periodic grid above 2^27 nodes (f90:1253) or axis above the supported length */
+#define SS3D_ENODATA 5    /* conditioning: no datum inside the grid (f90:804) */
+
+#define SS3D_FP64 0       /* plain form: FP64 throughout */
+#define SS3D_FP32 1       /* precision form: FP32 synthesis and FFTs on the FP64 spectrum */
+
+#define SS3D_OUT_F32 0    /* float32 output (the .bin/.vtk/.vti value type) */
+#define SS3D_OUT_F64 1    /* float64 output (the reference's res array) */
+
+/* One nested structure: `itype sill ahmax ahmin avert azimuth dip plunge`
+ * (type(structure), f90:95-100; parameter-file line f90:1167-1168). */
+typedef struct ss3d_struct {
+    int itype;          /* 1 spherical, 2 exponential, 3 gaussian */
+    double sill, ahmax, ahmin, avert, azimuth, dip, plunge;
+} ss3d_struct;
+
+/* Spectrum diagnostics printed by the reference at f90:1289-1292. */
+typedef struct ss3d_spec_stats {
+    int np[3];          /* periodic grid npx, npy, npz (f90:1234-1251) */
+    double c0;          /* C(0), "target variance" */
+    double maximag;     /* max |Im S| */
+    double maxreal;     /* max |Re S| */
+    double spos;        /* sum of positive S */
+    double sneg;        /* sum of negative S (clipped to zero in amp) */
+} ss3d_spec_stats;
+
+typedef struct ss3d_spectrum ss3d_spectrum;
+
+/* ---------------------------------------------------------------- host-side model */
+
+/* GSLIB rotation of one structure: rot and axes are 3x3 row-major
+ * (rot[3*r+c] = Fortran rot(r+1,c+1)).  Replaces setrot, f90:107-139. */
+int ss3d_setrot(const ss3d_struct *s, double rot[9], double axes[9]);
+
+/* Covariance C(h) of nst nested structures plus nugget at lag (dx,dy,dz).
+ * Replaces covariance, f90:153-178. */
+int ss3d_covariance(const ss3d_struct *st, int nst, double nugget, double dx, double dy, double dz, double *c);
+
+/* Periodic grid of the ipad rule.  Replaces nextpow2/cutoff and the grid block
+ * f90:142-188, f90:1234-1253; returns SS3D_ETOOLARGE above 2^27 nodes. */
+int ss3d_grid_size(const ss3d_struct *st, int nst, const double d[3], const int n[3], int ipad, int np[3]);
+
+/* ---------------------------------------------------------------- spectrum */
+
+/* Covariance grid on the periodic grid, forward 3D FFT, S = FFT/N and
+ * amp = sqrt(max(Re S, 0)), all on the GPU in FP64, kept resident in device
+ * memory.  Replaces f90:1256-1292.  stats may be NULL. */
+int ss3d_spectrum_create(const ss3d_struct *st, int nst, double nugget, const double d[3], const int n[3], int ipad,
+                         ss3d_spectrum **out, ss3d_spec_stats *stats);
+void ss3d_spectrum_free(ss3d_spectrum *sp);
+
+/* Grid sizes and stats of a spectrum (np, n may be NULL). */
+int ss3d_spectrum_info(const ss3d_spectrum *sp, int np[3], int n[3], ss3d_spec_stats *stats);
+
+/* Device memory held by the spectrum (bytes), for admission control. */
+int64_t ss3d_spectrum_bytes(const ss3d_spectrum *sp);
+
+/* Copy of the FP64 amplitude on the Hermitian half spectrum, amp[k][j][i],
+ * i < npx/2+1 (host pointer).  Test hook for the f90:1277-1288 values. */
+int ss3d_spectrum_amp(const ss3d_spectrum *sp, double *amp);
+
+/* ---------------------------------------------------------------- realizations */
+
+/* Realizations r_first .. r_first+nreal-1 (0-based) of the reference stream for
+ * seed iseed: Hermitian coefficient synthesis with the Park-Miller stream
+ * reproduced bit-exactly by jump-ahead, inverse 3D FFT, crop to nx,ny,nz.
+ * Replaces f90:1302-1345.  r_first = 0, nreal = N gives exactly the
+ * reference's realizations 1..N; any sub-range gives the same values as the
+ * corresponding part of the full run (exact sharding).
+ *   igauss     0 fixed amplitudes + random phases, 1 Gaussian coefficients
+ *   precision  SS3D_FP64 or SS3D_FP32
+ *   out        res(nx,ny,nz,nreal) of out_dtype (SS3D_OUT_F32 / SS3D_OUT_F64),
+ *              host or device memory
+ *   zstats     NULL or 3*nreal doubles: mean, variance, max|Im| per realization
+ *              (the line printed at f90:1343-1344; max|Im| is 0 because the
+ *              Hermitian half-spectrum inverse is real by construction). */
+int ss3d_realize(const ss3d_spectrum *sp, int iseed, int64_t r_first, int nreal, int igauss, int precision,
+                 void *out, int out_dtype, double *zstats);
+
+/* Test hooks for the synthesis (host output arrays, half spectrum [k][j][i],
+ * i < npx/2+1):
+ *   ss3d_debug_states: Park-Miller state after the first draw that produced
+ *     each coefficient of realization r (the partner's draw for conjugate rows)
+ *   ss3d_debug_coefficients: the coefficients themselves (re, im interleaved). */
+int ss3d_debug_states(const ss3d_spectrum *sp, int iseed, int64_t r, int igauss, uint32_t *states);
+int ss3d_debug_coefficients(const ss3d_spectrum *sp, int iseed, int64_t r, int igauss, int precision, double *coef);
+
+/* ---------------------------------------------------------------- variogram */
+
+/* Experimental semivariograms of nreal fields res(nx,ny,nz,nreal) (FP64, host or
+ * device) along ndir integer directions (sx,sy,sz), lags 1..nlag[d], over all
+ * node pairs.  gam(nlagmax, ndir, nreal) column-major as in the reference;
+ * npairs(nlagmax, ndir) (may be NULL) are the exact pair counts.
+ * Replaces npair_count / vario_lag / the task loop of vario_report, f90:394-480. */
+int ss3d_vario(const double *res, const int n[3], int nreal, int ndir, const int *sx, const int *sy, const int *sz,
+               const int *nlag, double *gam, int64_t *npairs);
+
+/* ---------------------------------------------------------------- conditioning */
+
+/* Conditioning block of the parameter file (f90:740-750). */
+typedef struct ss3d_cond_params {
+    int ixc, iyc, izc, ivc, iwc;   /* data columns (1-based; izc, iwc may be 0) */
+    double tmin, tmax;             /* trimming limits */
+    int itrans;                    /* 1: normal score + back transform */
+    double skmean;                 /* mean removed when itrans = 0 */
+    double zmin, zmax;             /* back-transform limits */
+    int ltail; double ltpar;       /* lower tail (1 linear, 2 power) */
+    int utail; double utpar;       /* upper tail (1 linear, 2 power, 4 hyperbolic) */
+    double radius[3];              /* search radii: max, med, vert */
+    double angles[3];              /* search angles: azimuth, dip, plunge */
+    int ndmax;                     /* 1..100 */
+} ss3d_cond_params;
+
+typedef struct ss3d_cond_stats {
+    int nd, nmerged, nout;         /* data used, merged, outside the grid */
+    int nsb[3];                    /* super blocks per axis */
+    int64_t nsum;                  /* total neighbours over all nodes */
+    int nfail, nnone, nexact;      /* regularised systems, empty nodes, data nodes */
+    double data_mean, data_var;    /* of the normal scores (itrans = 1) */
+} ss3d_cond_stats;
+
+/* Conditioning by kriging of the residual: data snapping and merging, optional
+ * normal-score transform (host), super-block neighbour search and simple
+ * kriging at every node (GPU), back transform (GPU).  res(nx,ny,nz,nreal) FP64
+ * host or device, modified in place.  rows: nrows x nvar data values
+ * (row-major, the numeric rows of the GSLIB data file).  precision SS3D_FP64
+ * solves in FP64; SS3D_FP32 solves in FP32 with one FP64 residual refinement.
+ * The optional outputs (each of nrows doubles, may be NULL) receive the
+ * normal-score table (vrt, gtt) and the data actually used.
+ * Replaces condition_field f90:782-924, krige_node f90:949-1038,
+ * chol_solve f90:1040-1079, nscore/backtr f90:557-697. */
+int ss3d_condition(double *res, const int n[3], int nreal, const double xmin[3], const double d[3],
+                   const ss3d_struct *st, int nst, double nugget, const ss3d_cond_params *cp, const double *rows,
+                   int nrows, int nvar, int precision, ss3d_cond_stats *cs, double *vrt, double *gtt, double *dxs,
+                   double *dys, double *dzs, double *dval, double *dg);
+
+/* ---------------------------------------------------------------- runtime */
+
+/* Stream (a cudaStream_t passed as void*) on which later calls issue work;
+ * NULL selects the legacy default stream. */
+int ss3d_set_stream(void *stream);
+
+/* Message of the last failing call on this thread ("" if none). */
+const char *ss3d_last_error(void);
+
+/* Library version string. */
+const char *ss3d_version(void);
+
+#ifdef __cplusplus
+}
+#endif
+#endif

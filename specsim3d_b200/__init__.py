@@ -1,0 +1,205 @@
+"""specsim3d_b200 -- B200-native SPECSIM3D spectral simulation path.
+
+Python face of the C ABI (include/specsim3d_gpu.h), mirroring the stages of
+the reference program src/specsim3d.f90:
+
+    Model / grid_size      setrot, covariance, ipad rule     f90:107-188, 1234-1253
+    Spectrum               covariance grid + FFT + sqrt      f90:1256-1292
+    Spectrum.realize       Hermitian synthesis + inverse FFT f90:1302-1345
+    vario                  experimental variograms           f90:394-480
+    condition              kriging of the residual           f90:700-1081
+
+Arrays follow the Fortran layout res(nx,ny,nz,nreal), i.e. numpy shape
+(nreal, nz, ny, nx).  Outputs can be numpy arrays (host) or torch CUDA tensors
+(device); the library detects which.  All compute runs on the GPU; there is no
+CPU fallback.
+"""
+import ctypes
+
+import numpy as np
+
+from . import _lib as L
+from ._lib import FP32, FP64, OUT_F32, OUT_F64, SpecsimError
+
+__all__ = ["Spectrum", "grid_size", "covariance", "setrot", "vario", "condition", "FP32", "FP64",
+           "SpecsimError", "set_stream"]
+
+
+def _np3(v, dtype):
+    return np.ascontiguousarray(np.asarray(v, dtype=dtype).reshape(3))
+
+
+def setrot(struct):
+    """rot, axes (3x3 each) of one structure tuple (itype, sill, ahmax, ahmin, avert, az, dip, plunge)."""
+    rot = np.zeros(9)
+    axes = np.zeros(9)
+    L.check(L.lib().ss3d_setrot(L.structs_array([struct]), L.dptr(rot), L.dptr(axes)))
+    return rot.reshape(3, 3), axes.reshape(3, 3)
+
+
+def covariance(structs, nugget, dx, dy, dz):
+    arr = L.structs_array(structs)
+    c = ctypes.c_double()
+    L.check(L.lib().ss3d_covariance(arr, len(arr), float(nugget), float(dx), float(dy), float(dz), ctypes.byref(c)))
+    return c.value
+
+
+def grid_size(structs, d, n, ipad):
+    """Periodic grid (npx, npy, npz) of the ipad rule (f90:1234-1253)."""
+    arr = L.structs_array(structs)
+    np_ = np.zeros(3, dtype=np.int32)
+    L.check(L.lib().ss3d_grid_size(arr, len(arr), L.dptr(_np3(d, np.float64)), L.iptr(_np3(n, np.int32)),
+                                   int(ipad), L.iptr(np_)))
+    return tuple(int(v) for v in np_)
+
+
+def set_stream(stream):
+    """Issue later calls on a torch.cuda.Stream (or raw cudaStream_t int); None = default stream."""
+    h = None if stream is None else (stream.cuda_stream if hasattr(stream, "cuda_stream") else int(stream))
+    L.check(L.lib().ss3d_set_stream(ctypes.c_void_p(h)))
+
+
+def _out_ptr(out):
+    """(pointer, dtype code, nbytes) of a numpy array or a torch tensor."""
+    if isinstance(out, np.ndarray):
+        if not out.flags.c_contiguous:
+            raise ValueError("output array must be C-contiguous")
+        code = {np.dtype(np.float32): OUT_F32, np.dtype(np.float64): OUT_F64}[out.dtype]
+        return ctypes.c_void_p(out.ctypes.data), code
+    # torch tensor
+    import torch
+    if not out.is_contiguous():
+        raise ValueError("output tensor must be contiguous")
+    code = {torch.float32: OUT_F32, torch.float64: OUT_F64}[out.dtype]
+    return ctypes.c_void_p(out.data_ptr()), code
+
+
+class Spectrum:
+    """Device-resident amplitude spectrum of one model on one grid (f90:1256-1292)."""
+
+    def __init__(self, structs, nugget, d, n, ipad):
+        self.structs = [tuple(s) for s in structs]
+        self.nugget = float(nugget)
+        self.d = tuple(float(v) for v in d)
+        self.n = tuple(int(v) for v in n)
+        self.ipad = int(ipad)
+        arr = L.structs_array(self.structs)
+        h = ctypes.c_void_p()
+        st = L.SpecStats()
+        L.check(L.lib().ss3d_spectrum_create(arr, len(arr), self.nugget, L.dptr(_np3(self.d, np.float64)),
+                                             L.iptr(_np3(self.n, np.int32)), self.ipad, ctypes.byref(h),
+                                             ctypes.byref(st)))
+        self._h = h
+        self.np = tuple(st.np)
+        self.stats = dict(c0=st.c0, maximag=st.maximag, maxreal=st.maxreal, spos=st.spos, sneg=st.sneg)
+
+    @property
+    def handle(self):
+        return self._h
+
+    def close(self):
+        if self._h:
+            L.lib().ss3d_spectrum_free(self._h)
+            self._h = None
+
+    def __del__(self):
+        try:
+            self.close()
+        except Exception:
+            pass
+
+    @property
+    def nbytes(self):
+        return int(L.lib().ss3d_spectrum_bytes(self._h))
+
+    def amp(self):
+        """FP64 amplitude on the half spectrum, shape (npz, npy, npx//2+1)."""
+        npx, npy, npz = self.np
+        h = npx // 2 + 1 if npx >= 2 else 1
+        a = np.zeros((npz, npy, h))
+        L.check(L.lib().ss3d_spectrum_amp(self._h, ctypes.c_void_p(a.ctypes.data)))
+        return a
+
+    def realize(self, iseed, nreal, igauss=0, precision=FP64, r_first=0, out=None, dtype=np.float64, zstats=False):
+        """Realizations r_first..r_first+nreal-1 of seed iseed (f90:1302-1345).
+
+        Returns an array of shape (nreal, nz, ny, nx) (``out`` if given: numpy
+        host array or torch CUDA tensor of float32/float64), and with
+        zstats=True also the (nreal, 3) mean / variance / max|Im| table."""
+        nx, ny, nz = self.n
+        if out is None:
+            out = np.empty((nreal, nz, ny, nx), dtype=dtype)
+        ptr, code = _out_ptr(out)
+        zs = np.zeros((max(nreal, 1), 3)) if zstats else None
+        L.check(L.lib().ss3d_realize(self._h, int(iseed), int(r_first), int(nreal), int(igauss), int(precision), ptr,
+                                     code, ctypes.c_void_p(zs.ctypes.data) if zs is not None else None))
+        return (out, zs[:nreal]) if zstats else out
+
+    def debug_states(self, iseed, r, igauss):
+        npx, npy, npz = self.np
+        h = npx // 2 + 1 if npx >= 2 else 1
+        s = np.zeros((npz, npy, h), dtype=np.uint32)
+        L.check(L.lib().ss3d_debug_states(self._h, int(iseed), int(r), int(igauss), ctypes.c_void_p(s.ctypes.data)))
+        return s
+
+    def debug_coefficients(self, iseed, r, igauss, precision=FP64):
+        npx, npy, npz = self.np
+        h = npx // 2 + 1 if npx >= 2 else 1
+        c = np.zeros((npz, npy, h, 2))
+        L.check(L.lib().ss3d_debug_coefficients(self._h, int(iseed), int(r), int(igauss), int(precision),
+                                                ctypes.c_void_p(c.ctypes.data)))
+        return c[..., 0] + 1j * c[..., 1]
+
+
+def vario(res, dirs):
+    """Experimental variograms (f90:394-480).
+
+    res: float64 array (nreal, nz, ny, nx) (numpy or torch CUDA tensor).
+    dirs: list of (sx, sy, sz, nlag).  Returns gam of shape (nreal, ndir, nlagmax)
+    and the pair counts (ndir, nlagmax)."""
+    nreal, nz, ny, nx = res.shape
+    dirs = [tuple(int(v) for v in d) for d in dirs]
+    ndir = len(dirs)
+    nlagmax = max(d[3] for d in dirs)
+    sx, sy, sz, nl = (np.ascontiguousarray(np.array([d[k] for d in dirs], dtype=np.int32)) for k in range(4))
+    gam = np.zeros((nreal, ndir, nlagmax))
+    npairs = np.zeros((ndir, nlagmax), dtype=np.int64)
+    ptr, code = _out_ptr(res)
+    if code != OUT_F64:
+        raise ValueError("vario needs float64 fields")
+    n = np.array([nx, ny, nz], dtype=np.int32)
+    L.check(L.lib().ss3d_vario(ptr, L.iptr(n), nreal, ndir, L.iptr(sx), L.iptr(sy), L.iptr(sz), L.iptr(nl),
+                               ctypes.c_void_p(gam.ctypes.data), ctypes.c_void_p(npairs.ctypes.data)))
+    return gam, npairs
+
+
+def condition(res, xmin, d, structs, nugget, params, rows, precision=FP64):
+    """Conditioning by kriging of the residual, in place on res (f90:700-1081).
+
+    params: dict with the conditioning-block fields of ss3d_cond_params.
+    rows: (nrows, nvar) float64 data rows.  Returns (stats dict, extras dict)."""
+    nreal, nz, ny, nx = res.shape
+    cp = L.CondParams()
+    for k, v in params.items():
+        if k in ("radius", "angles"):
+            getattr(cp, k)[:] = [float(x) for x in v]
+        else:
+            setattr(cp, k, v)
+    rows = np.ascontiguousarray(np.asarray(rows, dtype=np.float64))
+    nrows, nvar = rows.shape
+    outs = {k: np.zeros(max(nrows, 1)) for k in ("vrt", "gtt", "dxs", "dys", "dzs", "dval", "dg")}
+    cs = L.CondStats()
+    arr = L.structs_array(structs)
+    ptr, code = _out_ptr(res)
+    if code != OUT_F64:
+        raise ValueError("condition needs float64 fields")
+    n = np.array([nx, ny, nz], dtype=np.int32)
+    L.check(L.lib().ss3d_condition(ptr, L.iptr(n), nreal, L.dptr(_np3(xmin, np.float64)),
+                                   L.dptr(_np3(d, np.float64)), arr, len(arr), float(nugget), ctypes.byref(cp),
+                                   ctypes.c_void_p(rows.ctypes.data), nrows, nvar, int(precision), ctypes.byref(cs),
+                                   *[ctypes.c_void_p(outs[k].ctypes.data) for k in
+                                     ("vrt", "gtt", "dxs", "dys", "dzs", "dval", "dg")]))
+    stats = dict(nd=cs.nd, nmerged=cs.nmerged, nout=cs.nout, nsb=tuple(cs.nsb), nsum=cs.nsum, nfail=cs.nfail,
+                 nnone=cs.nnone, nexact=cs.nexact, data_mean=cs.data_mean, data_var=cs.data_var)
+    nd = cs.nd
+    return stats, {k: v[:nd] for k, v in outs.items()}

@@ -1,0 +1,593 @@
+// ss3d_api.cu -- host side of the C ABI declared in include/specsim3d_gpu.h:
+// model setup (setrot, grid sizing), device context (twiddle and jump-ahead
+// tables), spectrum handles, realization batching with host/device output.
+#include <cuda_runtime.h>
+
+#include <cmath>
+#include <cstdarg>
+#include <cstdio>
+#include <cstdlib>
+#include <cstring>
+#include <mutex>
+#include <string>
+#include <vector>
+
+#include "../../include/specsim3d_gpu.h"
+#include "ss3d_internal.h"
+
+using namespace ss3d;
+
+// ---------------------------------------------------------------- errors and stream
+static thread_local std::string g_err;
+static cudaStream_t g_stream = 0;
+
+static int fail(int code, const char* fmt, ...) {
+  char buf[1024];
+  va_list ap;
+  va_start(ap, fmt);
+  vsnprintf(buf, sizeof buf, fmt, ap);
+  va_end(ap);
+  g_err = buf;
+  return code;
+}
+
+static int cuda_fail(cudaError_t e, const char* what) {
+  cudaGetLastError();  // clear a sticky-free error
+  return fail(e == cudaErrorMemoryAllocation ? SS3D_ENOMEM : SS3D_ECUDA, "%s: %s", what, cudaGetErrorString(e));
+}
+
+#define CK(call)                                     \
+  do {                                               \
+    cudaError_t e_ = (call);                         \
+    if (e_ != cudaSuccess) return cuda_fail(e_, #call); \
+  } while (0)
+
+extern "C" const char* ss3d_last_error(void) { return g_err.c_str(); }
+extern "C" const char* ss3d_version(void) { return "specsim3d_b200 0.1 (sm_100a)"; }
+extern "C" int ss3d_set_stream(void* stream) {
+  g_stream = (cudaStream_t)stream;
+  return SS3D_OK;
+}
+
+// ---------------------------------------------------------------- device context
+namespace {
+struct DevCtx {
+  bool ready = false;
+  float2* twf = nullptr;
+  double2* twd = nullptr;
+  uint32_t* ptab = nullptr;
+};
+std::mutex g_ctx_mu;
+DevCtx g_ctx[64];
+
+int get_ctx(DevCtx** out) {
+  int dev = 0;
+  CK(cudaGetDevice(&dev));
+  if (dev < 0 || dev >= 64) return fail(SS3D_EINVAL, "device ordinal %d out of range", dev);
+  std::lock_guard<std::mutex> lk(g_ctx_mu);
+  DevCtx& c = g_ctx[dev];
+  if (!c.ready) {
+    const int ntw = (1 << (TW_LOG_MAX + 1)) - 1;
+    std::vector<float2> hf(ntw);
+    std::vector<double2> hd(ntw);
+    for (int L = 0; L <= TW_LOG_MAX; ++L) {
+      int n = 1 << L;
+      for (int m = 0; m < n; ++m) {
+        long double ang = -2.0L * 3.141592653589793238462643383279502884L * (long double)m / (long double)n;
+        long double c0 = cosl(ang), s0 = sinl(ang);
+        hd[n - 1 + m] = make_double2((double)c0, (double)s0);
+        hf[n - 1 + m] = make_float2((float)c0, (float)s0);
+      }
+    }
+    // tab[l*2048 + v] = 16807^(v * 2048^l) mod (2^31 - 1)
+    std::vector<uint32_t> ht(3 * 2048);
+    uint32_t base = PM_A;
+    for (int l = 0; l < 3; ++l) {
+      uint32_t acc = 1;
+      for (int v = 0; v < 2048; ++v) {
+        ht[l * 2048 + v] = acc;
+        acc = pm_mulmod(acc, base);
+      }
+      base = acc;  // base^2048
+    }
+    CK(cudaMalloc(&c.twf, sizeof(float2) * ntw));
+    CK(cudaMalloc(&c.twd, sizeof(double2) * ntw));
+    CK(cudaMalloc(&c.ptab, sizeof(uint32_t) * 3 * 2048));
+    CK(cudaMemcpy(c.twf, hf.data(), sizeof(float2) * ntw, cudaMemcpyHostToDevice));
+    CK(cudaMemcpy(c.twd, hd.data(), sizeof(double2) * ntw, cudaMemcpyHostToDevice));
+    CK(cudaMemcpy(c.ptab, ht.data(), sizeof(uint32_t) * 3 * 2048, cudaMemcpyHostToDevice));
+    c.ready = true;
+  }
+  *out = &c;
+  return SS3D_OK;
+}
+
+bool is_device_ptr(const void* p) {
+  cudaPointerAttributes a;
+  if (cudaPointerGetAttributes(&a, p) != cudaSuccess) {
+    cudaGetLastError();
+    return false;
+  }
+  return a.type == cudaMemoryTypeDevice || a.type == cudaMemoryTypeManaged;
+}
+
+// ---------------------------------------------------------------- model
+const double PI = 3.14159265358979323846;  // f90:92
+
+// setrot, f90:107-139 (same expression order as the reference)
+void setrot_rc(const ss3d_struct& s, double rot[3][3], double axes[3][3]) {
+  double deg = PI / 180.0;
+  double alpha = (s.azimuth >= 0.0 && s.azimuth < 270.0) ? (90.0 - s.azimuth) * deg : (450.0 - s.azimuth) * deg;
+  double beta = -(s.dip * deg);
+  double theta = s.plunge * deg;
+  double sina = sin(alpha), cosa = cos(alpha);
+  double sinb = sin(beta), cosb = cos(beta);
+  double sint = sin(theta), cost = cos(theta);
+  double anis1 = s.ahmin / s.ahmax, anis2 = s.avert / s.ahmax;
+  double afac1 = 1.0 / fmax(anis1, 1.0e-20), afac2 = 1.0 / fmax(anis2, 1.0e-20);
+  rot[0][0] = cosb * cosa;
+  rot[0][1] = cosb * sina;
+  rot[0][2] = -sinb;
+  rot[1][0] = afac1 * (-(cost * sina) + sint * sinb * cosa);
+  rot[1][1] = afac1 * (cost * cosa + sint * sinb * sina);
+  rot[1][2] = afac1 * (sint * cosb);
+  rot[2][0] = afac2 * (sint * sina + cost * sinb * cosa);
+  rot[2][1] = afac2 * (-(sint * cosa) + cost * sinb * sina);
+  rot[2][2] = afac2 * (cost * cosb);
+  for (int c = 0; c < 3; c++) {
+    axes[0][c] = rot[0][c] * s.ahmax;
+    axes[1][c] = rot[1][c] / afac1 * s.ahmin;
+    axes[2][c] = rot[2][c] / afac2 * s.avert;
+  }
+}
+
+int check_structs(const ss3d_struct* st, int nst) {
+  if (!st) return fail(SS3D_EINVAL, "structures pointer is NULL");
+  if (nst < 1 || nst > MAXST) return fail(SS3D_EINVAL, "nstruct out of range");
+  for (int i = 0; i < nst; i++) {
+    if (st[i].ahmax <= 0 || st[i].ahmin <= 0 || st[i].avert <= 0) return fail(SS3D_EINVAL, "ranges must be positive");
+    if (st[i].itype < 1 || st[i].itype > 3) {
+      // the reference treats any other itype as gaussian (select case default, f90:174)
+    }
+  }
+  return SS3D_OK;
+}
+
+void build_model(const ss3d_struct* st, int nst, double nugget, Model& m) {
+  memset(&m, 0, sizeof m);
+  m.nst = nst;
+  m.nugget = nugget;
+  for (int i = 0; i < nst; i++) {
+    double rot[3][3], axes[3][3];
+    setrot_rc(st[i], rot, axes);
+    m.itype[i] = st[i].itype;
+    m.sill[i] = st[i].sill;
+    m.ahmax[i] = st[i].ahmax;
+    for (int r = 0; r < 3; r++)
+      for (int c = 0; c < 3; c++) m.rot[i][3 * r + c] = rot[r][c];
+  }
+}
+
+int nextpow2(int n) {
+  int m = 1;
+  while (m < n) m *= 2;
+  return m;
+}
+
+double cutoff(int itype) { return itype == 1 ? 1.0 : (itype == 2 ? 2.3 : 1.6); }
+
+int grid_size(const ss3d_struct* st, int nst, const double d[3], const int n[3], int ipad, int np[3]) {
+  np[0] = nextpow2(n[0]);
+  np[1] = nextpow2(n[1]);
+  np[2] = nextpow2(n[2]);
+  if (ipad == 1) {
+    double e[3] = {0, 0, 0};
+    for (int s = 0; s < nst; s++) {
+      double rot[3][3], axes[3][3];
+      setrot_rc(st[s], rot, axes);
+      for (int a = 0; a < 3; a++) {
+        double ss = axes[0][a] * axes[0][a];
+        ss = ss + axes[1][a] * axes[1][a];
+        ss = ss + axes[2][a] * axes[2][a];
+        e[a] = fmax(e[a], cutoff(st[s].itype) * sqrt(ss) / d[a]);
+      }
+    }
+    int r[3];
+    for (int a = 0; a < 3; a++) r[a] = (int)ceil(e[a]);
+    np[0] = nextpow2(std::max(n[0] + r[0], 2 * r[0]));
+    np[1] = nextpow2(std::max(n[1] + r[1], 2 * r[1]));
+    np[2] = n[2] > 1 ? nextpow2(std::max(n[2] + r[2], 2 * r[2])) : 1;
+  }
+  if ((double)np[0] * (double)np[1] * (double)np[2] > 134217728.0)
+    return fail(SS3D_ETOOLARGE, "periodic grid too large (>2^27 nodes)");
+  return SS3D_OK;
+}
+
+int ilog2i(int n) {
+  int l = 0;
+  while ((1 << l) < n) ++l;
+  return l;
+}
+}  // namespace
+
+extern "C" int ss3d_setrot(const ss3d_struct* s, double rot[9], double axes[9]) {
+  if (!s || !rot || !axes) return fail(SS3D_EINVAL, "NULL argument");
+  double r[3][3], a[3][3];
+  setrot_rc(*s, r, a);
+  for (int i = 0; i < 3; i++)
+    for (int j = 0; j < 3; j++) {
+      rot[3 * i + j] = r[i][j];
+      axes[3 * i + j] = a[i][j];
+    }
+  return SS3D_OK;
+}
+
+extern "C" int ss3d_covariance(const ss3d_struct* st, int nst, double nugget, double dx, double dy, double dz,
+                               double* c) {
+  int rc = check_structs(st, nst);
+  if (rc) return rc;
+  Model m;
+  build_model(st, nst, nugget, m);
+  *c = covariance(m, dx, dy, dz);
+  return SS3D_OK;
+}
+
+extern "C" int ss3d_grid_size(const ss3d_struct* st, int nst, const double d[3], const int n[3], int ipad,
+                              int np[3]) {
+  int rc = check_structs(st, nst);
+  if (rc) return rc;
+  if (!d || !n || !np) return fail(SS3D_EINVAL, "NULL argument");
+  if (n[0] < 1 || n[1] < 1 || n[2] < 1) return fail(SS3D_EINVAL, "grid sizes must be positive");
+  return grid_size(st, nst, d, n, ipad, np);
+}
+
+// ---------------------------------------------------------------- spectrum handle
+struct ss3d_spectrum {
+  int dev;
+  Geo geo;  // d and D filled per call
+  Model model;
+  double d[3];
+  ss3d_spec_stats stats;
+  double* amp64 = nullptr;
+  float* amp32 = nullptr;
+  // cached workspace of the realization path
+  void* ws = nullptr;
+  size_t ws_bytes = 0;
+};
+
+namespace {
+int supported_axes(const Geo& g, bool dbl, const char** which) {
+  int maxl = dbl ? MAX_LOGN_D : MAX_LOGN_F;
+  if (g.npx > 1 && ilog2i(g.npx) - 1 > maxl) { *which = "x"; return 0; }
+  if (ilog2i(g.npy) > maxl) { *which = "y"; return 0; }
+  if (ilog2i(g.npz) > maxl) { *which = "z"; return 0; }
+  return 1;
+}
+
+int ws_reserve(ss3d_spectrum* sp, size_t bytes) {
+  if (sp->ws_bytes >= bytes) return SS3D_OK;
+  if (sp->ws) {
+    cudaFree(sp->ws);
+    sp->ws = nullptr;
+    sp->ws_bytes = 0;
+  }
+  CK(cudaMalloc(&sp->ws, bytes));
+  sp->ws_bytes = bytes;
+  return SS3D_OK;
+}
+
+size_t align256(size_t x) { return (x + 255) & ~(size_t)255; }
+}  // namespace
+
+extern "C" int ss3d_spectrum_create(const ss3d_struct* st, int nst, double nugget, const double d[3], const int n[3],
+                                    int ipad, ss3d_spectrum** out, ss3d_spec_stats* stats) {
+  if (!out) return fail(SS3D_EINVAL, "out is NULL");
+  *out = nullptr;
+  int rc = check_structs(st, nst);
+  if (rc) return rc;
+  if (!d || !n) return fail(SS3D_EINVAL, "NULL argument");
+  if (n[0] < 1 || n[1] < 1 || n[2] < 1) return fail(SS3D_EINVAL, "grid sizes must be positive");
+  int np[3];
+  rc = grid_size(st, nst, d, n, ipad, np);
+  if (rc) return rc;
+  DevCtx* ctx;
+  if ((rc = get_ctx(&ctx))) return rc;
+  ss3d_spectrum* sp = new ss3d_spectrum();
+  CK(cudaGetDevice(&sp->dev));
+  Geo& g = sp->geo;
+  g.npx = np[0];
+  g.npy = np[1];
+  g.npz = np[2];
+  g.nx = n[0];
+  g.ny = n[1];
+  g.nz = n[2];
+  g.H = np[0] >= 2 ? np[0] / 2 + 1 : 1;
+  g.HP = (g.H + 1) & ~1;
+  g.d = 1;
+  g.D = 0;
+  const char* ax = "";
+  if (!supported_axes(g, true, &ax)) {
+    delete sp;
+    return fail(SS3D_ETOOLARGE, "periodic axis %s longer than the supported FP64 transform length", ax);
+  }
+  memcpy(sp->d, d, sizeof sp->d);
+  build_model(st, nst, nugget, sp->model);
+  const size_t nh = (size_t)g.npz * g.npy * g.HP;
+  cudaStream_t s = g_stream;
+  double2* work = nullptr;
+  SpecPartial* part = nullptr;
+  const int npart = 148 * 8;
+  cudaError_t e = cudaMalloc(&work, sizeof(double2) * nh);
+  if (e == cudaSuccess) e = cudaMalloc(&sp->amp64, sizeof(double) * nh);
+  if (e == cudaSuccess) e = cudaMalloc(&sp->amp32, sizeof(float) * nh);
+  if (e == cudaSuccess) e = cudaMalloc(&part, sizeof(SpecPartial) * (npart + 1));
+  if (e == cudaSuccess)
+    e = launch_spectrum(sp->model, d, g, work, sp->amp64, sp->amp32, part, npart, part + npart, Tw{ctx->twf, ctx->twd},
+                        s);
+  SpecPartial res{};
+  if (e == cudaSuccess) e = cudaMemcpyAsync(&res, part + npart, sizeof res, cudaMemcpyDeviceToHost, s);
+  if (e == cudaSuccess) e = cudaStreamSynchronize(s);
+  if (work) cudaFree(work);
+  if (part) cudaFree(part);
+  if (e != cudaSuccess) {
+    ss3d_spectrum_free(sp);
+    return cuda_fail(e, "spectrum");
+  }
+  sp->stats.np[0] = np[0];
+  sp->stats.np[1] = np[1];
+  sp->stats.np[2] = np[2];
+  sp->stats.c0 = covariance(sp->model, 0.0, 0.0, 0.0);
+  sp->stats.maximag = res.maximag;
+  sp->stats.maxreal = res.maxreal;
+  sp->stats.spos = res.spos;
+  sp->stats.sneg = res.sneg;
+  if (stats) *stats = sp->stats;
+  *out = sp;
+  return SS3D_OK;
+}
+
+extern "C" void ss3d_spectrum_free(ss3d_spectrum* sp) {
+  if (!sp) return;
+  int cur = 0;
+  cudaGetDevice(&cur);
+  cudaSetDevice(sp->dev);
+  if (sp->amp64) cudaFree(sp->amp64);
+  if (sp->amp32) cudaFree(sp->amp32);
+  if (sp->ws) cudaFree(sp->ws);
+  cudaSetDevice(cur);
+  delete sp;
+}
+
+extern "C" int ss3d_spectrum_info(const ss3d_spectrum* sp, int np[3], int n[3], ss3d_spec_stats* stats) {
+  if (!sp) return fail(SS3D_EINVAL, "spectrum is NULL");
+  if (np) {
+    np[0] = sp->geo.npx;
+    np[1] = sp->geo.npy;
+    np[2] = sp->geo.npz;
+  }
+  if (n) {
+    n[0] = sp->geo.nx;
+    n[1] = sp->geo.ny;
+    n[2] = sp->geo.nz;
+  }
+  if (stats) *stats = sp->stats;
+  return SS3D_OK;
+}
+
+extern "C" int64_t ss3d_spectrum_bytes(const ss3d_spectrum* sp) {
+  if (!sp) return 0;
+  const size_t nh = (size_t)sp->geo.npz * sp->geo.npy * sp->geo.HP;
+  return (int64_t)(nh * (sizeof(double) + sizeof(float)) + sp->ws_bytes);
+}
+
+extern "C" int ss3d_spectrum_amp(const ss3d_spectrum* sp, double* amp) {
+  if (!sp || !amp) return fail(SS3D_EINVAL, "NULL argument");
+  const Geo& g = sp->geo;
+  CK(cudaMemcpy2DAsync(amp, sizeof(double) * g.H, sp->amp64, sizeof(double) * g.HP, sizeof(double) * g.H,
+                       (size_t)g.npy * g.npz, cudaMemcpyDeviceToHost, g_stream));
+  CK(cudaStreamSynchronize(g_stream));
+  return SS3D_OK;
+}
+
+// ---------------------------------------------------------------- realizations
+namespace {
+Geo geo_for(const ss3d_spectrum* sp, int igauss) {
+  Geo g = sp->geo;
+  g.d = igauss ? 2 : 1;
+  uint64_t N = (uint64_t)g.npx * g.npy * g.npz;
+  uint64_t nself = (uint64_t)(g.npx >= 2 ? 2 : 1) * (g.npy >= 2 ? 2 : 1) * (g.npz >= 2 ? 2 : 1);
+  g.D = (uint64_t)g.d * ((N + nself) / 2);
+  return g;
+}
+uint32_t seed0(int iseed) {
+  int64_t a = iseed < 0 ? -(int64_t)iseed : (int64_t)iseed;
+  return (uint32_t)(a % 2147483646LL + 1);
+}
+}  // namespace
+
+extern "C" int ss3d_realize(const ss3d_spectrum* csp, int iseed, int64_t r_first, int nreal, int igauss,
+                            int precision, void* out, int out_dtype, double* zstats) {
+  ss3d_spectrum* sp = const_cast<ss3d_spectrum*>(csp);
+  if (!sp) return fail(SS3D_EINVAL, "spectrum is NULL");
+  if (nreal < 0) return fail(SS3D_EINVAL, "nreal must be >= 0");
+  if (r_first < 0) return fail(SS3D_EINVAL, "r_first must be >= 0");
+  if (igauss != 0 && igauss != 1) return fail(SS3D_EINVAL, "igauss must be 0 or 1");
+  if (precision != SS3D_FP64 && precision != SS3D_FP32) return fail(SS3D_EINVAL, "unknown precision %d", precision);
+  if (out_dtype != SS3D_OUT_F32 && out_dtype != SS3D_OUT_F64) return fail(SS3D_EINVAL, "unknown out_dtype %d", out_dtype);
+  if (nreal == 0) return SS3D_OK;
+  if (!out) return fail(SS3D_EINVAL, "out is NULL");
+  const bool dbl = precision == SS3D_FP64;
+  Geo g = geo_for(sp, igauss);
+  const char* ax = "";
+  if (!supported_axes(g, dbl, &ax))
+    return fail(SS3D_ETOOLARGE, "periodic axis %s longer than the supported transform length", ax);
+  DevCtx* ctx;
+  int rc;
+  if ((rc = get_ctx(&ctx))) return rc;
+  CK(cudaSetDevice(sp->dev));
+  cudaStream_t s = g_stream;
+  const bool dev_out = is_device_ptr(out);
+  const size_t M = (size_t)g.nx * g.ny * g.nz;
+  const size_t oel = out_dtype == SS3D_OUT_F32 ? 4 : 8;
+  const size_t cel = dbl ? sizeof(double2) : sizeof(float2);
+  const size_t per_work = (size_t)g.npz * g.npy * g.HP * cel;
+  const int nbx = realize_part_blocks(g, dbl);
+  // batch: at most 16 realizations and about 8 GiB of work space
+  size_t budget = (size_t)8 << 30;
+  size_t per_real = per_work + (dev_out ? 0 : 2 * M * oel) + (size_t)g.npy * g.npz * 4 + (size_t)nbx * 16;
+  int bt = (int)std::min<size_t>((size_t)nreal, std::max<size_t>(1, budget / per_real));
+  bt = std::min(bt, 16);
+  size_t off_work = 0;
+  size_t off_rs = align256(off_work + per_work * bt);
+  size_t off_apow = align256(off_rs + (size_t)g.npy * g.npz * 4 * bt);
+  size_t off_part = align256(off_apow + (size_t)g.npx * 4);
+  size_t off_zs = align256(off_part + (size_t)nbx * 16 * bt);
+  size_t off_stage = align256(off_zs + (size_t)nreal * 16);
+  size_t total = off_stage + (dev_out ? 0 : 2 * align256(M * oel * bt));
+  if ((rc = ws_reserve(sp, total))) return rc;
+  char* base = (char*)sp->ws;
+  void* work = base + off_work;
+  uint32_t* rs = (uint32_t*)(base + off_rs);
+  uint32_t* apow = (uint32_t*)(base + off_apow);
+  double* part = (double*)(base + off_part);
+  double* zs = (double*)(base + off_zs);
+  char* stage[2] = {base + off_stage, base + off_stage + align256(M * oel * bt)};
+  const long long wstride = (long long)g.npz * g.npy * g.HP;
+  const uint32_t s0 = seed0(iseed);
+  Tw tw{ctx->twf, ctx->twd};
+  cudaEvent_t done[2] = {nullptr, nullptr};
+  cudaStream_t cs = nullptr;
+  if (!dev_out) {
+    CK(cudaStreamCreateWithFlags(&cs, cudaStreamNonBlocking));
+    CK(cudaEventCreateWithFlags(&done[0], cudaEventDisableTiming));
+    CK(cudaEventCreateWithFlags(&done[1], cudaEventDisableTiming));
+  }
+  cudaError_t e = cudaSuccess;
+  int ib = 0;
+  for (int r0 = 0; r0 < nreal && e == cudaSuccess; r0 += bt, ++ib) {
+    int nb = std::min(bt, nreal - r0);
+    int slot = ib & 1;
+    void* dst = dev_out ? (void*)((char*)out + (size_t)r0 * M * oel) : (void*)stage[slot];
+    if (!dev_out && ib >= 2) e = cudaStreamWaitEvent(s, done[slot], 0);
+    if (e == cudaSuccess) e = launch_rowstates(g, s0, r_first + r0, nb, ctx->ptab, rs, r0 == 0 ? apow : nullptr, s);
+    int nblk = 0;
+    if (e == cudaSuccess) {
+      if (dbl)
+        e = launch_realize<double>(g, sp->amp64, rs, apow, (double2*)work, wstride, nb, dst, out_dtype, part, &nblk,
+                                   tw, true, s);
+      else
+        e = launch_realize<float>(g, sp->amp32, rs, apow, (float2*)work, wstride, nb, dst, out_dtype, part, &nblk,
+                                  tw, true, s);
+    }
+    if (e == cudaSuccess && zstats) e = launch_reduce_zstats(part, nblk, nb, zs + 2 * (size_t)r0, s);
+    if (e == cudaSuccess && !dev_out) {
+      cudaEvent_t ready;
+      e = cudaEventCreateWithFlags(&ready, cudaEventDisableTiming);
+      if (e == cudaSuccess) e = cudaEventRecord(ready, s);
+      if (e == cudaSuccess) e = cudaStreamWaitEvent(cs, ready, 0);
+      if (e == cudaSuccess)
+        e = cudaMemcpyAsync((char*)out + (size_t)r0 * M * oel, stage[slot], (size_t)nb * M * oel,
+                            cudaMemcpyDeviceToHost, cs);
+      if (e == cudaSuccess) e = cudaEventRecord(done[slot], cs);
+      cudaEventDestroy(ready);
+    }
+  }
+  std::vector<double> hz;
+  if (e == cudaSuccess && zstats) {
+    hz.resize(2 * (size_t)nreal);
+    e = cudaMemcpyAsync(hz.data(), zs, sizeof(double) * 2 * nreal, cudaMemcpyDeviceToHost, s);
+  }
+  if (e == cudaSuccess) e = cudaStreamSynchronize(s);
+  if (e == cudaSuccess && cs) e = cudaStreamSynchronize(cs);
+  if (cs) {
+    cudaStreamDestroy(cs);
+    cudaEventDestroy(done[0]);
+    cudaEventDestroy(done[1]);
+  }
+  if (e != cudaSuccess) return cuda_fail(e, "realize");
+  if (zstats) {
+    for (int r = 0; r < nreal; r++) {
+      double mean = hz[2 * r] / (double)M;
+      zstats[3 * r] = mean;
+      zstats[3 * r + 1] = hz[2 * r + 1] / (double)M - mean * mean;
+      zstats[3 * r + 2] = 0.0;
+    }
+  }
+  return SS3D_OK;
+}
+
+// ---------------------------------------------------------------- debug hooks
+namespace ss3d {
+cudaError_t launch_debug_states(const Geo& g, const uint32_t* rowstates, const uint32_t* apow, uint32_t* out,
+                                cudaStream_t st);
+}
+
+extern "C" int ss3d_debug_states(const ss3d_spectrum* sp, int iseed, int64_t r, int igauss, uint32_t* states) {
+  if (!sp || !states) return fail(SS3D_EINVAL, "NULL argument");
+  if (r < 0) return fail(SS3D_EINVAL, "r must be >= 0");
+  DevCtx* ctx;
+  int rc;
+  if ((rc = get_ctx(&ctx))) return rc;
+  Geo g = geo_for(sp, igauss != 0);
+  cudaStream_t s = g_stream;
+  const size_t nhalf = (size_t)g.npz * g.npy * g.H;
+  uint32_t *rs = nullptr, *apow = nullptr, *o = nullptr;
+  CK(cudaMalloc(&rs, sizeof(uint32_t) * g.npy * g.npz));
+  CK(cudaMalloc(&apow, sizeof(uint32_t) * g.npx));
+  CK(cudaMalloc(&o, sizeof(uint32_t) * nhalf));
+  cudaError_t e = launch_rowstates(g, seed0(iseed), r, 1, ctx->ptab, rs, apow, s);
+  if (e == cudaSuccess) e = launch_debug_states(g, rs, apow, o, s);
+  if (e == cudaSuccess) e = cudaMemcpyAsync(states, o, sizeof(uint32_t) * nhalf, cudaMemcpyDeviceToHost, s);
+  if (e == cudaSuccess) e = cudaStreamSynchronize(s);
+  cudaFree(rs);
+  cudaFree(apow);
+  cudaFree(o);
+  if (e != cudaSuccess) return cuda_fail(e, "debug_states");
+  return SS3D_OK;
+}
+
+extern "C" int ss3d_debug_coefficients(const ss3d_spectrum* sp, int iseed, int64_t r, int igauss, int precision,
+                                       double* coef) {
+  if (!sp || !coef) return fail(SS3D_EINVAL, "NULL argument");
+  if (r < 0) return fail(SS3D_EINVAL, "r must be >= 0");
+  DevCtx* ctx;
+  int rc;
+  if ((rc = get_ctx(&ctx))) return rc;
+  const bool dbl = precision == SS3D_FP64;
+  Geo g = geo_for(sp, igauss != 0);
+  cudaStream_t s = g_stream;
+  const size_t nh = (size_t)g.npz * g.npy * g.HP;
+  uint32_t *rs = nullptr, *apow = nullptr;
+  void* w = nullptr;
+  CK(cudaMalloc(&rs, sizeof(uint32_t) * g.npy * g.npz));
+  CK(cudaMalloc(&apow, sizeof(uint32_t) * g.npx));
+  CK(cudaMalloc(&w, (dbl ? sizeof(double2) : sizeof(float2)) * nh));
+  cudaError_t e = launch_rowstates(g, seed0(iseed), r, 1, ctx->ptab, rs, apow, s);
+  if (e == cudaSuccess) {
+    if (dbl)
+      e = launch_gen<double>(g, sp->amp64, rs, apow, (double2*)w, 0, 1, s);
+    else
+      e = launch_gen<float>(g, sp->amp32, rs, apow, (float2*)w, 0, 1, s);
+  }
+  std::vector<char> h((dbl ? sizeof(double2) : sizeof(float2)) * nh);
+  if (e == cudaSuccess) e = cudaMemcpyAsync(h.data(), w, h.size(), cudaMemcpyDeviceToHost, s);
+  if (e == cudaSuccess) e = cudaStreamSynchronize(s);
+  cudaFree(rs);
+  cudaFree(apow);
+  cudaFree(w);
+  if (e != cudaSuccess) return cuda_fail(e, "debug_coefficients");
+  for (size_t row = 0; row < (size_t)g.npz * g.npy; row++)
+    for (int i = 0; i < g.H; i++) {
+      size_t src = row * g.HP + i, dst = row * g.H + i;
+      if (dbl) {
+        const double2* p = (const double2*)h.data();
+        coef[2 * dst] = p[src].x;
+        coef[2 * dst + 1] = p[src].y;
+      } else {
+        const float2* p = (const float2*)h.data();
+        coef[2 * dst] = p[src].x;
+        coef[2 * dst + 1] = p[src].y;
+      }
+    }
+  return SS3D_OK;
+}

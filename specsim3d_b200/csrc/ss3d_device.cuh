@@ -1,0 +1,304 @@
+// ss3d_device.cuh -- device-side building blocks shared by the SPECSIM3D
+// kernels: complex helpers, the Park-Miller jump-ahead stream, the Hermitian
+// draw-offset arithmetic and the shared-memory Stockham FFT engine.
+//
+// Reference behaviour reproduced here (src/specsim3d.f90):
+//   * urand / gauss_pair  f90:191-205  (Lehmer 16807 mod 2^31-1, Box-Muller)
+//   * seeding             f90:1302-1303 (s0 = mod(|iseed|, 2^31-2) + 1, 10 draws)
+//   * Hermitian fill      f90:1305-1334 (draw order k, j, i over lin <= linp)
+//   * fft1d / fft3d       f90:208-304   (unscaled; isign -1 forward, +1 inverse)
+#pragma once
+#include <cstdint>
+#include <cuda_runtime.h>
+
+namespace ss3d {
+
+constexpr uint32_t PM_M = 2147483647u;  // 2^31 - 1
+constexpr uint32_t PM_A = 16807u;
+
+// ---------------------------------------------------------------- complex
+template <typename R> struct cpx;
+template <> struct cpx<float> { using T = float2; };
+template <> struct cpx<double> { using T = double2; };
+template <typename R> using cpx_t = typename cpx<R>::T;
+
+template <typename C> __device__ __forceinline__ C cmk(decltype(C::x) a, decltype(C::x) b) { C c; c.x = a; c.y = b; return c; }
+template <typename C> __device__ __forceinline__ C cadd(C a, C b) { return cmk<C>(a.x + b.x, a.y + b.y); }
+template <typename C> __device__ __forceinline__ C csub(C a, C b) { return cmk<C>(a.x - b.x, a.y - b.y); }
+template <typename C> __device__ __forceinline__ C cmul(C a, C b) {
+  return cmk<C>(a.x * b.x - a.y * b.y, a.x * b.y + a.y * b.x);
+}
+// a * conj(b) when conjugate is true
+template <typename C> __device__ __forceinline__ C cmul_sgn(C a, C b, bool conjb) {
+  decltype(C::x) by = conjb ? -b.y : b.y;
+  return cmk<C>(a.x * b.x - a.y * by, a.x * by + a.y * b.x);
+}
+// multiply by (sign * i): forward (sign -1) gives -i, inverse gives +i
+template <int SIGN, typename C> __device__ __forceinline__ C cmul_si(C a) {
+  return SIGN > 0 ? cmk<C>(-a.y, a.x) : cmk<C>(a.y, -a.x);
+}
+
+// ---------------------------------------------------------------- Park-Miller
+__host__ __device__ __forceinline__ uint32_t pm_mulmod(uint32_t a, uint32_t b) {
+  uint64_t p = (uint64_t)a * (uint64_t)b;           // < 2^62
+  uint64_t r = (p & PM_M) + (p >> 31);               // < 2^32
+  r = (r & PM_M) + (r >> 31);
+  return (uint32_t)(r >= PM_M ? r - PM_M : r);
+}
+
+// 16807^e mod (2^31-1) from the three 11-bit power tables
+// tab[l*2048 + v] = 16807^(v * 2048^l) mod m, e < 2^31 (reduced mod m-1).
+__device__ __forceinline__ uint32_t pm_pow(const uint32_t* __restrict__ tab, uint64_t e) {
+  e %= (uint64_t)(PM_M - 1);
+  uint32_t r = tab[e & 2047u];
+  r = pm_mulmod(r, tab[2048 + ((e >> 11) & 2047u)]);
+  r = pm_mulmod(r, tab[4096 + ((e >> 22) & 2047u)]);
+  return r;
+}
+
+// ---------------------------------------------------------------- grid geometry
+// Padded periodic grid (npx, npy, npz) and the Hermitian half spectrum
+// i in [0, H), H = npx/2 + 1 (1 when npx = 1), stored with row pitch HP.
+struct Geo {
+  int npx, npy, npz;   // periodic grid
+  int nx, ny, nz;      // output grid
+  int H, HP;           // half-spectrum width and row pitch (elements)
+  int d;               // draws per representative index (1 phases, 2 Gaussian)
+  uint64_t D;          // draws per realization
+};
+
+// number of representative indices (lin <= linp) in the rows of plane k that
+// precede row j, plus all planes before k  (row order k, j as in f90:1306-1308)
+__host__ __device__ __forceinline__ uint64_t row_prefix(const Geo& g, int j, int k) {
+  const uint64_t npx = g.npx, npy = g.npy;
+  const uint64_t Hr = g.npx >= 2 ? (uint64_t)(g.npx / 2 + 1) : 1u;
+  const uint64_t nless_rows = g.npy >= 2 ? (uint64_t)(g.npy / 2 - 1) : 0u;
+  const uint64_t neq_rows = g.npy >= 2 ? 2u : 1u;
+  const uint64_t qeq = nless_rows * npx + neq_rows * Hr;   // count of a self-conjugate plane
+  uint64_t P = 0;
+  if (k > 0) {
+    P = qeq;
+    if (g.npz >= 2) {
+      int half = g.npz / 2;
+      int full = (k < half ? k : half) - 1;
+      if (full > 0) P += (uint64_t)full * npy * npx;
+      if (k > half) P += qeq;
+    }
+  }
+  const int kp = (g.npz - k) % g.npz;
+  if (k < kp) return P + (uint64_t)j * npx;
+  if (k > kp) return P;
+  if (j == 0) return P;
+  uint64_t s = Hr;
+  if (g.npy >= 2) {
+    int half = g.npy / 2;
+    s += (uint64_t)((j < half ? j : half) - 1) * npx;
+    if (j > half) s += Hr;
+  }
+  return P + s;
+}
+
+// class of row (j,k): 0 all indices are representatives, 1 self-conjugate row
+// (i <= npx/2 are representatives), 2 none (conjugates of row (jp,kp))
+__host__ __device__ __forceinline__ int row_class(const Geo& g, int j, int k) {
+  const int jp = (g.npy - j) % g.npy, kp = (g.npz - k) % g.npz;
+  if (k < kp || (k == kp && j < jp)) return 0;
+  if (k > kp || (k == kp && j > jp)) return 2;
+  return 1;
+}
+
+// ---------------------------------------------------------------- coefficient synthesis
+// Unit phasor e^{2 pi i s/m} in float with the quadrant taken exactly in integers.
+__device__ __forceinline__ void phasor_f(uint32_t s, float& c, float& sn) {
+  uint64_t q = 4ull * s;
+  int quad = (q >= 2ull * PM_M) ? ((q >= 3ull * PM_M) ? 3 : 2) : ((q >= PM_M) ? 1 : 0);
+  uint32_t rem = (uint32_t)(q - (uint64_t)quad * PM_M);
+  float x = (float)rem * (1.0f / 2147483647.0f);    // in [0,1): quarter turns
+  float s0, c0;
+  sincospif(0.5f * x, &s0, &c0);
+  switch (quad) {
+    case 0: c = c0; sn = s0; break;
+    case 1: c = -s0; sn = c0; break;
+    case 2: c = -c0; sn = -s0; break;
+    default: c = s0; sn = -c0; break;
+  }
+}
+__device__ __forceinline__ void phasor_d(uint32_t s, double& c, double& sn) {
+  double u = (double)s / 2147483647.0;
+  sincospi(2.0 * u, &sn, &c);
+}
+// -2 ln(s/m) in float, accurate near s = m through log1p of an exact difference
+__device__ __forceinline__ float m2log_f(uint32_t s) {
+  if (s >= (1u << 30)) return -2.0f * log1pf(-(float)(PM_M - s) * (1.0f / 2147483647.0f));
+  return -2.0f * logf((float)s * (1.0f / 2147483647.0f));
+}
+__device__ __forceinline__ double m2log_d(uint32_t s) {
+  double u = (double)s / 2147483647.0;
+  return -2.0 * log(u);
+}
+
+// Park-Miller state right after the first draw that produced coefficient
+// (i, j, k): the index itself for representative rows, its conjugate partner
+// (ip, jp, kp) for rows of class 2 (conj = true).  self marks the
+// self-conjugate indices (lin == linp).
+__device__ __forceinline__ uint32_t first_state(const Geo& g, int i, int j, int k, const uint32_t* __restrict__ rs,
+                                                const uint32_t* __restrict__ apow, bool& conj, bool& self) {
+  int cls = row_class(g, j, k);
+  int si = i, sj = j, sk = k;
+  conj = false;
+  if (cls == 2) {
+    si = (g.npx - i) % g.npx;
+    sj = (g.npy - j) % g.npy;
+    sk = (g.npz - k) % g.npz;
+    conj = true;
+  }
+  self = (cls == 1) && (i == 0 || 2 * i == g.npx);
+  return pm_mulmod(rs[sj + (size_t)g.npy * sk], apow[si]);
+}
+
+// Coefficient of half-spectrum index (i, j, k) for the realization whose row
+// states are rs (state of the first draw of each row of the realization).
+// Reproduces f90:1312-1331 for the half spectrum:
+//   row class 0 (or self-conjugate row, non-self index): amp * (g1 + i g2) sqrt(1/2)
+//     or amp * e^{i phi}
+//   row class 2: conjugate of the partner draw at (ip, jp, kp)
+//   self-conjugate index: amp * g1 (Gaussian) or +/-amp (phases, u < 0.5 -> +)
+template <typename R>
+__device__ __forceinline__ cpx_t<R> coefficient(const Geo& g, int i, int j, int k, R amp,
+                                                 const uint32_t* __restrict__ rs,
+                                                 const uint32_t* __restrict__ apow) {
+  using C = cpx_t<R>;
+  bool conj, self;
+  uint32_t s1 = first_state(g, i, j, k, rs, apow, conj, self);
+  if (g.d == 2) {
+    uint32_t s2 = pm_mulmod(s1, PM_A);
+    if constexpr (sizeof(R) == 4) {
+      float rr = sqrtf(m2log_f(s1));
+      float cs, sn;
+      phasor_f(s2, cs, sn);
+      if (self) return cmk<C>(amp * (rr * cs), 0.f);
+      const float h = 0.70710678118654752f;
+      float a = amp * h;
+      return cmk<C>(a * (rr * cs), (conj ? -a : a) * (rr * sn));
+    } else {
+      double rr = sqrt(m2log_d(s1));
+      double cs, sn;
+      phasor_d(s2, cs, sn);
+      double g1 = rr * cs, g2 = rr * sn;
+      if (self) return cmk<C>(amp * g1, 0.0);
+      const double h = 0.70710678118654757;   // sqrt(0.5d0)
+      return cmk<C>(amp * g1 * h, amp * (conj ? -g2 : g2) * h);
+    }
+  } else {
+    if (self) {
+      // urand() < 0.5  <=>  s/m < 0.5 with s integer  <=>  2 s < m
+      bool pos = (2ull * s1) < (uint64_t)PM_M;
+      return cmk<C>(pos ? amp : -amp, R(0));
+    }
+    R cs, sn;
+    if constexpr (sizeof(R) == 4) phasor_f(s1, cs, sn); else phasor_d(s1, cs, sn);
+    return cmk<C>(amp * cs, conj ? -(amp * sn) : amp * sn);
+  }
+}
+
+// ---------------------------------------------------------------- small DFTs
+template <int SIGN, typename C> __device__ __forceinline__ void dft2(C& a, C& b) {
+  C t = a; a = cadd(t, b); b = csub(t, b);
+}
+template <int SIGN, typename C> __device__ __forceinline__ void dft4(C& v0, C& v1, C& v2, C& v3) {
+  C t0 = cadd(v0, v2), t1 = csub(v0, v2), t2 = cadd(v1, v3), t3 = cmul_si<SIGN>(csub(v1, v3));
+  v0 = cadd(t0, t2); v2 = csub(t0, t2); v1 = cadd(t1, t3); v3 = csub(t1, t3);
+}
+template <int SIGN, typename C> __device__ __forceinline__ void dft8(C* v) {
+  using R = decltype(C::x);
+  C e0 = v[0], e1 = v[2], e2 = v[4], e3 = v[6];
+  C o0 = v[1], o1 = v[3], o2 = v[5], o3 = v[7];
+  dft4<SIGN>(e0, e1, e2, e3);
+  dft4<SIGN>(o0, o1, o2, o3);
+  const R r2 = (R)0.70710678118654752440;
+  // o1 *= w8, o2 *= w8^2 = sign*i, o3 *= w8^3
+  C w1 = cmk<C>(r2, SIGN * r2), w3 = cmk<C>(-r2, SIGN * r2);
+  o1 = cmul(o1, w1);
+  o2 = cmul_si<SIGN>(o2);
+  o3 = cmul(o3, w3);
+  v[0] = cadd(e0, o0); v[4] = csub(e0, o0);
+  v[1] = cadd(e1, o1); v[5] = csub(e1, o1);
+  v[2] = cadd(e2, o2); v[6] = csub(e2, o2);
+  v[3] = cadd(e3, o3); v[7] = csub(e3, o3);
+}
+template <int R, int SIGN, typename C> __device__ __forceinline__ void dftR(C* v) {
+  if constexpr (R == 8) dft8<SIGN>(v);
+  else if constexpr (R == 4) dft4<SIGN>(v[0], v[1], v[2], v[3]);
+  else if constexpr (R == 2) dft2<SIGN>(v[0], v[1]);
+}
+
+// radix of pass number p for a length 2^LOGN transform: radix-8 passes first,
+// then one radix-4 or radix-2 pass for the remaining bits
+template <int LOGN> struct Sched {
+  static constexpr int n8 = LOGN / 3;
+  static constexpr int rem = LOGN % 3;
+  static constexpr int npass = n8 + (rem ? 1 : 0);
+  static constexpr int radix(int p) { return p < n8 ? 8 : (rem == 2 ? 4 : 2); }
+  static constexpr int ns_before(int p) { return p == 0 ? 1 : ns_before(p - 1) * radix(p - 1); }
+};
+
+// One Stockham pass (Ns = sub-transform size already done, R = radix) over a
+// tile stored in shared memory as s[p * PITCH + t], t in [0,TX) columns,
+// p in [0,N) positions.  In place: every item is loaded before the barrier and
+// stored after it.  tw: shared twiddles, tw[m] = e^{-2 pi i m / N}.
+template <int N, int TX, int PITCH, int NT, int R, int NS, int SIGN, int TWS, typename C>
+__device__ __forceinline__ void stockham_pass(C* s, const C* tw) {
+  constexpr int NB = N / R;                 // butterflies per column
+  constexpr int TOTAL = NB * TX;
+  constexpr int ITEMS = (TOTAL + NT - 1) / NT;
+  C v[ITEMS][R];
+#pragma unroll
+  for (int it = 0; it < ITEMS; ++it) {
+    int q = it * NT + (int)threadIdx.x;
+    if (TOTAL % NT == 0 || q < TOTAL) {
+      int t = q % TX, jb = q / TX;
+      int k = jb % NS;
+#pragma unroll
+      for (int r = 0; r < R; ++r) v[it][r] = s[(jb + r * NB) * PITCH + t];
+      if (NS > 1) {
+#pragma unroll
+        for (int r = 1; r < R; ++r) {
+          C w = tw[(k * r) * (N / (NS * R)) * TWS];
+          v[it][r] = cmul_sgn(v[it][r], w, SIGN > 0);
+        }
+      }
+      dftR<R, SIGN>(v[it]);
+    }
+  }
+  __syncthreads();
+#pragma unroll
+  for (int it = 0; it < ITEMS; ++it) {
+    int q = it * NT + (int)threadIdx.x;
+    if (TOTAL % NT == 0 || q < TOTAL) {
+      int t = q % TX, jb = q / TX;
+      int k = jb % NS;
+      int idxD = (jb / NS) * NS * R + k;
+#pragma unroll
+      for (int r = 0; r < R; ++r) s[(idxD + r * NS) * PITCH + t] = v[it][r];
+    }
+  }
+  __syncthreads();
+}
+
+template <int N, int TX, int PITCH, int NT, int SIGN, int TWS, int LOGN, int P, typename C>
+__device__ __forceinline__ void stockham_from(C* s, const C* tw) {
+  if constexpr (P < Sched<LOGN>::npass) {
+    stockham_pass<N, TX, PITCH, NT, Sched<LOGN>::radix(P), Sched<LOGN>::ns_before(P), SIGN, TWS>(s, tw);
+    stockham_from<N, TX, PITCH, NT, SIGN, TWS, LOGN, P + 1>(s, tw);
+  }
+}
+
+// Full length-2^LOGN transform of TX columns in shared memory (unscaled).
+// tw[m * TWS] = e^{-2 pi i m / 2^LOGN}.  Caller must __syncthreads() after
+// filling s and tw; the transform ends with a barrier.
+template <int LOGN, int TX, int PITCH, int NT, int SIGN, int TWS = 1, typename C>
+__device__ __forceinline__ void smem_fft(C* s, const C* tw) {
+  stockham_from<(1 << LOGN), TX, PITCH, NT, SIGN, TWS, LOGN, 0>(s, tw);
+}
+
+}  // namespace ss3d

@@ -1,0 +1,795 @@
+// ss3d_fft.cu -- spectrum construction and realization synthesis kernels.
+//
+// GPU replacement of these reference stages (src/specsim3d.f90):
+//   covariance grid        f90:1256-1270  -> k_spec_rows   (fused with the x R2C pass)
+//   forward fft3d, /ntot   f90:1273-1274  -> k_spec_rows, k_axis_c2c (y, z)
+//   amp = sqrt(max(S,0))   f90:1275-1292  -> k_spec_amp (+ k_reduce_spec)
+//   Hermitian fill         f90:1305-1334  -> k_axis_gen (fused into the first
+//                                            inverse pass) or k_gen
+//   inverse fft3d + crop   f90:1335-1340  -> k_axis_c2c (z, y), k_rows_c2r (x)
+//
+// Data layout in HBM: every complex grid is the Hermitian half spectrum
+// i in [0, H), H = npx/2+1, stored as [k][j][HP] with row pitch HP = H rounded
+// up to an even count (16-byte aligned rows of float2).  A batch of realizations
+// stores its grids back to back, wstride elements apart.
+//
+// Each FFT kernel keeps one tile in shared memory: TX lines of the transformed
+// axis (TX consecutive elements in memory, so that every global access of a
+// warp covers whole 32-byte sectors) and runs the radix-8/4/2 Stockham engine
+// of ss3d_device.cuh on it.  Only the positions that survive the final crop are
+// written back (z pass: k < nz; y pass: j < ny; x pass: i < nx).
+#include <cuda_runtime.h>
+
+#include <algorithm>
+#include <cstdio>
+
+#include "ss3d_internal.h"
+
+namespace ss3d {
+
+constexpr int NT = 256;  // threads per block of every FFT kernel
+
+// tile elements per block: 64 KB of shared memory for the data in both precisions
+template <typename R> struct TileE { static constexpr int E = 8192; };
+template <> struct TileE<double> { static constexpr int E = 4096; };
+
+template <typename R, int LOGN> struct AxisTX {
+  static constexpr int v0 = TileE<R>::E >> LOGN;
+  static constexpr int TX = v0 > 64 ? 64 : (v0 < 2 ? 2 : v0);
+};
+template <typename R, int LOGN> struct RowTX {
+  static constexpr int v0 = TileE<R>::E >> LOGN;
+  static constexpr int TX = v0 > 64 ? 64 : (v0 < 1 ? 1 : v0);
+};
+
+template <typename R> __device__ __forceinline__ const cpx_t<R>* twtab(const Tw& tw);
+template <> __device__ __forceinline__ const float2* twtab<float>(const Tw& tw) { return tw.f; }
+template <> __device__ __forceinline__ const double2* twtab<double>(const Tw& tw) { return tw.d; }
+
+// copy the first cnt entries of the twiddle table of length n into shared memory
+template <typename C>
+__device__ __forceinline__ void load_tw(C* s, const C* g, int n, int cnt) {
+  const C* src = g + (n - 1);
+  for (int q = threadIdx.x; q < cnt; q += blockDim.x) s[q] = src[q];
+}
+
+// ---------------------------------------------------------------- strided axis passes
+// A "line" is one column along the transformed axis.  Lines of one group are
+// contiguous in memory; groups are gstride apart; realizations rstride apart.
+struct AxisArgs {
+  long long S;         // element stride along the axis
+  int nout;            // positions stored (p < nout)
+  int lines;           // lines per group
+  int ngroups;
+  long long gstride;
+  int tpg;             // tiles per group
+  long long rstride;   // realization stride in the complex buffer
+  int nreal;
+  int axis;            // 1 = y, 2 = z (index decoding of the synthesis)
+};
+
+__device__ __forceinline__ bool line_valid(const Geo& g, int line, int lines) {
+  return line < lines && (line % g.HP) < g.H;
+}
+
+// c2c transform along a strided axis; out may alias in (the whole line is read first)
+template <typename R, int LOGN, int SIGN>
+__global__ void __launch_bounds__(NT) k_axis_c2c(AxisArgs a, Geo g, const cpx_t<R>* in, cpx_t<R>* out, Tw tw) {
+  using C = cpx_t<R>;
+  constexpr int N = 1 << LOGN;
+  constexpr int TX = AxisTX<R, LOGN>::TX;
+  extern __shared__ __align__(16) unsigned char smraw[];
+  C* s = reinterpret_cast<C*>(smraw);
+  C* stw = s + N * TX;
+  const int r = blockIdx.x % a.nreal;
+  const int tile = blockIdx.x / a.nreal;
+  const int grp = tile / a.tpg;
+  const int line0 = (tile % a.tpg) * TX;
+  const long long base = (long long)grp * a.gstride + line0 + (long long)r * a.rstride;
+  load_tw(stw, twtab<R>(tw), N, N);
+  for (int q = threadIdx.x; q < N * TX; q += NT) {
+    int t = q % TX, p = q / TX;
+    C v = cmk<C>(R(0), R(0));
+    if (line_valid(g, line0 + t, a.lines)) v = in[base + t + p * a.S];
+    s[p * TX + t] = v;
+  }
+  __syncthreads();
+  smem_fft<LOGN, TX, TX, NT, SIGN>(s, stw);
+  for (int q = threadIdx.x; q < a.nout * TX; q += NT) {
+    int t = q % TX, p = q / TX;
+    if (line_valid(g, line0 + t, a.lines)) out[base + t + p * a.S] = s[p * TX + t];
+  }
+}
+
+// First inverse pass with the coefficient synthesis fused into the load: the
+// coefficients of realization r are generated from amp and the row states,
+// transformed along the axis, and only p < nout is stored.
+template <typename R, int LOGN>
+__global__ void __launch_bounds__(NT) k_axis_gen(AxisArgs a, Geo g, const R* __restrict__ amp,
+                                                 const uint32_t* __restrict__ rowstates,
+                                                 const uint32_t* __restrict__ apow, cpx_t<R>* out, Tw tw) {
+  using C = cpx_t<R>;
+  constexpr int N = 1 << LOGN;
+  constexpr int TX = AxisTX<R, LOGN>::TX;
+  extern __shared__ __align__(16) unsigned char smraw[];
+  C* s = reinterpret_cast<C*>(smraw);
+  C* stw = s + N * TX;
+  const int r = blockIdx.x % a.nreal;
+  const int tile = blockIdx.x / a.nreal;
+  const int grp = tile / a.tpg;
+  const int line0 = (tile % a.tpg) * TX;
+  const long long abase = (long long)grp * a.gstride + line0;
+  const uint32_t* rs = rowstates + (size_t)r * g.npy * g.npz;
+  load_tw(stw, twtab<R>(tw), N, N);
+  for (int q = threadIdx.x; q < N * TX; q += NT) {
+    int t = q % TX, p = q / TX;
+    int line = line0 + t;
+    C v = cmk<C>(R(0), R(0));
+    if (line_valid(g, line, a.lines)) {
+      int i, j, k;
+      if (a.axis == 2) {
+        i = line % g.HP;
+        j = line / g.HP;
+        k = p;
+      } else {
+        i = line;
+        j = p;
+        k = grp;
+      }
+      R am = amp[abase + t + p * a.S];
+      v = coefficient<R>(g, i, j, k, am, rs, apow);
+    }
+    s[p * TX + t] = v;
+  }
+  __syncthreads();
+  smem_fft<LOGN, TX, TX, NT, +1>(s, stw);
+  const long long obase = abase + (long long)r * a.rstride;
+  for (int q = threadIdx.x; q < a.nout * TX; q += NT) {
+    int t = q % TX, p = q / TX;
+    if (line_valid(g, line0 + t, a.lines)) out[obase + t + p * a.S] = s[p * TX + t];
+  }
+}
+
+// Standalone synthesis of the full half spectrum of nreal realizations.
+template <typename R>
+__global__ void k_gen(Geo g, const R* __restrict__ amp, const uint32_t* __restrict__ rowstates,
+                      const uint32_t* __restrict__ apow, cpx_t<R>* out, long long rstride, int nreal) {
+  using C = cpx_t<R>;
+  const long long per = (long long)g.npz * g.npy * g.HP;
+  const long long tot = per * nreal;
+  for (long long q = blockIdx.x * (long long)blockDim.x + threadIdx.x; q < tot;
+       q += (long long)gridDim.x * blockDim.x) {
+    int r = (int)(q / per);
+    long long o = q - r * per;
+    int i = (int)(o % g.HP);
+    long long rest = o / g.HP;
+    int j = (int)(rest % g.npy), k = (int)(rest / g.npy);
+    C v = cmk<C>(R(0), R(0));
+    if (i < g.H) v = coefficient<R>(g, i, j, k, amp[o], rowstates + (size_t)r * g.npy * g.npz, apow);
+    out[o + r * rstride] = v;
+  }
+}
+
+// State of the first draw of every row of every realization of the batch:
+// s = 16807^(11 + (r_first + r) * D + d * prefix(row)) * s0  (mod 2^31-1)
+__global__ void k_rowstates(Geo g, uint32_t s0, long long r_first, int nreal, const uint32_t* __restrict__ ptab,
+                            uint32_t* rowstates) {
+  const int rows = g.npy * g.npz;
+  const long long tot = (long long)rows * nreal;
+  for (long long q = blockIdx.x * (long long)blockDim.x + threadIdx.x; q < tot;
+       q += (long long)gridDim.x * blockDim.x) {
+    int r = (int)(q / rows);
+    int row = (int)(q - (long long)r * rows);
+    int j = row % g.npy, k = row / g.npy;
+    const uint64_t M1 = (uint64_t)(PM_M - 1);
+    uint64_t t = ((uint64_t)(r_first + r) % M1) * (g.D % M1) % M1;
+    t = (t + (uint64_t)g.d * row_prefix(g, j, k)) % M1;
+    rowstates[q] = pm_mulmod(pm_pow(ptab, 11ull + t), s0);
+  }
+}
+
+// a^(d*i) mod m for i in [0, npx): the offset of index i inside a row
+__global__ void k_apow(int npx, int d, const uint32_t* __restrict__ ptab, uint32_t* apow) {
+  for (int i = blockIdx.x * blockDim.x + threadIdx.x; i < npx; i += gridDim.x * blockDim.x)
+    apow[i] = pm_pow(ptab, (uint64_t)d * i);
+}
+
+// First-draw state of every half-spectrum index of one realization (test hook)
+__global__ void k_debug_states(Geo g, const uint32_t* __restrict__ rs, const uint32_t* __restrict__ apow,
+                               uint32_t* out) {
+  const long long tot = (long long)g.npz * g.npy * g.H;
+  for (long long q = blockIdx.x * (long long)blockDim.x + threadIdx.x; q < tot;
+       q += (long long)gridDim.x * blockDim.x) {
+    int i = (int)(q % g.H);
+    long long row = q / g.H;
+    int j = (int)(row % g.npy), k = (int)(row / g.npy);
+    bool conj, self;
+    out[q] = first_state(g, i, j, k, rs, apow, conj, self);
+  }
+}
+
+// ---------------------------------------------------------------- block reduction helpers
+template <int NTH>
+__device__ __forceinline__ void block_sum2(double& a, double& b) {
+  __shared__ double red[2][NTH / 32];
+#pragma unroll
+  for (int off = 16; off > 0; off >>= 1) {
+    a += __shfl_down_sync(0xffffffffu, a, off);
+    b += __shfl_down_sync(0xffffffffu, b, off);
+  }
+  __syncthreads();
+  if ((threadIdx.x & 31) == 0) {
+    red[0][threadIdx.x >> 5] = a;
+    red[1][threadIdx.x >> 5] = b;
+  }
+  __syncthreads();
+  if (threadIdx.x == 0) {
+    double s1 = 0, s2 = 0;
+    for (int w = 0; w < NTH / 32; ++w) {
+      s1 += red[0][w];
+      s2 += red[1][w];
+    }
+    a = s1;
+    b = s2;
+  }
+}
+
+// ---------------------------------------------------------------- x pass: C2R + crop
+// Row (j,k) of the half spectrum (N+1 values) -> npx = 2N reals, of which the
+// first nx go to out[r][k][j][:].  Packing for a length-N inverse FFT:
+//   Z[q] = (X[q] + conj X[N-q]) + i w^q (X[q] - conj X[N-q]),  w = e^{+2 pi i/(2N)}
+// then x[2m] = Re z[m], x[2m+1] = Im z[m].  The imaginary parts of X[0] and
+// X[N] are dropped: the reference keeps the real part of the full complex
+// inverse (f90:1339), which does not see them.
+template <typename R, typename O, int LOGN>
+__global__ void __launch_bounds__(NT) k_rows_c2r(Geo g, const cpx_t<R>* __restrict__ in, long long rstride,
+                                                 O* __restrict__ out, long long ostride, int nreal, int nblk_per_r,
+                                                 double* __restrict__ part, Tw tw) {
+  using C = cpx_t<R>;
+  constexpr int N = 1 << LOGN;
+  constexpr int TX = RowTX<R, LOGN>::TX;
+  constexpr int PITCH = TX + 1;
+  extern __shared__ __align__(16) unsigned char smraw[];
+  C* s = reinterpret_cast<C*>(smraw);   // [N+1][PITCH]
+  C* stw = s + (N + 1) * PITCH;         // 2N entries e^{-2 pi i m/(2N)}
+  const int r = blockIdx.x % nreal;
+  const int blk = blockIdx.x / nreal;
+  const int nrows = g.ny * g.nz;
+  const int row0 = blk * TX;
+  load_tw(stw, twtab<R>(tw), 2 * N, 2 * N);
+  const C* src = in + (long long)r * rstride;
+  for (int q = threadIdx.x; q < (N + 1) * TX; q += NT) {
+    int t = q / (N + 1), p = q % (N + 1);
+    int row = row0 + t;
+    C v = cmk<C>(R(0), R(0));
+    if (row < nrows) {
+      int j = row % g.ny, k = row / g.ny;
+      v = src[((long long)k * g.npy + j) * g.HP + p];
+    }
+    s[p * PITCH + t] = v;
+  }
+  __syncthreads();
+  for (int q = threadIdx.x; q < (N / 2 + 1) * TX; q += NT) {
+    int t = q % TX, k = q / TX;
+    int kc = N - k;
+    C a = s[k * PITCH + t], b = s[kc * PITCH + t];
+    if (k == 0) {
+      a.y = R(0);
+      b.y = R(0);
+    }
+    C w = stw[k];
+    w.y = -w.y;
+    C bc = cmk<C>(b.x, -b.y);
+    C zk = cadd(cadd(a, bc), cmul_si<+1>(cmul(w, csub(a, bc))));
+    if (k != 0 && kc != k) {
+      C w2 = stw[kc];
+      w2.y = -w2.y;
+      C ac = cmk<C>(a.x, -a.y);
+      s[kc * PITCH + t] = cadd(cadd(b, ac), cmul_si<+1>(cmul(w2, csub(b, ac))));
+    }
+    s[k * PITCH + t] = zk;
+  }
+  __syncthreads();
+  smem_fft<LOGN, TX, PITCH, NT, +1, 2>(s, stw);
+  double s1 = 0.0, s2 = 0.0;
+  O* dst = out + (long long)r * ostride;
+  const int nxh = (g.nx + 1) / 2;
+  for (int q = threadIdx.x; q < nxh * TX; q += NT) {
+    int t = q / nxh, m = q % nxh;
+    int row = row0 + t;
+    if (row < nrows) {
+      C z = s[m * PITCH + t];
+      long long o = (long long)row * g.nx + 2 * m;
+      dst[o] = (O)z.x;
+      s1 += (double)z.x;
+      s2 += (double)z.x * (double)z.x;
+      if (2 * m + 1 < g.nx) {
+        dst[o + 1] = (O)z.y;
+        s1 += (double)z.y;
+        s2 += (double)z.y * (double)z.y;
+      }
+    }
+  }
+  if (part) {
+    block_sum2<NT>(s1, s2);
+    if (threadIdx.x == 0) {
+      part[2 * ((long long)r * nblk_per_r + blk)] = s1;
+      part[2 * ((long long)r * nblk_per_r + blk) + 1] = s2;
+    }
+  }
+}
+
+// npx == 1: the x axis is trivial, x[0] = Re X[0]
+template <typename R, typename O>
+__global__ void k_rows_copy(Geo g, const cpx_t<R>* __restrict__ in, long long rstride, O* __restrict__ out,
+                            long long ostride, int nreal, int nblk_per_r, double* __restrict__ part) {
+  const int r = blockIdx.x % nreal;
+  const int blk = blockIdx.x / nreal;
+  const int nrows = g.ny * g.nz;
+  double s1 = 0, s2 = 0;
+  int row = blk * NT + threadIdx.x;
+  if (row < nrows) {
+    int j = row % g.ny, k = row / g.ny;
+    R v = in[(long long)r * rstride + ((long long)k * g.npy + j) * g.HP].x;
+    out[(long long)r * ostride + row] = (O)v;
+    s1 = v;
+    s2 = (double)v * v;
+  }
+  if (part) {
+    block_sum2<NT>(s1, s2);
+    if (threadIdx.x == 0) {
+      part[2 * ((long long)r * nblk_per_r + blk)] = s1;
+      part[2 * ((long long)r * nblk_per_r + blk) + 1] = s2;
+    }
+  }
+}
+
+__global__ void k_reduce_zstats(const double* __restrict__ part, int nblk, double* zsum) {
+  const int r = blockIdx.x;
+  double a = 0, b = 0;
+  for (int q = threadIdx.x; q < nblk; q += NT) {
+    a += part[2 * ((long long)r * nblk + q)];
+    b += part[2 * ((long long)r * nblk + q) + 1];
+  }
+  block_sum2<NT>(a, b);
+  if (threadIdx.x == 0) {
+    zsum[2 * r] = a;
+    zsum[2 * r + 1] = b;
+  }
+}
+
+// ---------------------------------------------------------------- spectrum
+// x pass of the forward transform with the covariance grid generated in place
+// (f90:1256-1270): row (j,k) of c(i,j,k) = C(ip dx, jp dy, kp dz) with minimum
+// image lags, R2C of length npx = 2N through a length-N complex FFT:
+//   X[q] = (Z[q] + conj Z[N-q])/2 - i/2 w^q (Z[q] - conj Z[N-q]),  w = e^{-2 pi i/(2N)}
+template <int LOGN>
+__global__ void __launch_bounds__(NT) k_spec_rows(Model m, double dx, double dy, double dz, Geo g,
+                                                  double2* __restrict__ out, Tw tw) {
+  using C = double2;
+  constexpr int N = 1 << LOGN;
+  constexpr int TX = RowTX<double, LOGN>::TX;
+  constexpr int PITCH = TX + 1;
+  extern __shared__ __align__(16) unsigned char smraw[];
+  C* s = reinterpret_cast<C*>(smraw);
+  C* stw = s + (N + 1) * PITCH;
+  const int nrows = g.npy * g.npz;
+  const int row0 = blockIdx.x * TX;
+  load_tw(stw, tw.d, 2 * N, 2 * N);
+  for (int q = threadIdx.x; q < N * TX; q += NT) {
+    int t = q / N, p = q % N;
+    int row = row0 + t;
+    C v = cmk<C>(0.0, 0.0);
+    if (row < nrows) {
+      int j = row % g.npy, k = row / g.npy;
+      int kp = k > g.npz / 2 ? k - g.npz : k;
+      int jp = j > g.npy / 2 ? j - g.npy : j;
+      int i0 = 2 * p, i1 = 2 * p + 1;
+      int ip0 = i0 > g.npx / 2 ? i0 - g.npx : i0;
+      int ip1 = i1 > g.npx / 2 ? i1 - g.npx : i1;
+      v.x = covariance(m, (double)ip0 * dx, (double)jp * dy, (double)kp * dz);
+      v.y = covariance(m, (double)ip1 * dx, (double)jp * dy, (double)kp * dz);
+    }
+    s[p * PITCH + t] = v;
+  }
+  __syncthreads();
+  smem_fft<LOGN, TX, PITCH, NT, -1, 2>(s, stw);
+  for (int q = threadIdx.x; q < (N / 2 + 1) * TX; q += NT) {
+    int t = q % TX, k = q / TX;
+    int kc = N - k;
+    C zk = s[k * PITCH + t];
+    C zc = s[(kc % N) * PITCH + t];
+    C zcc = cmk<C>(zc.x, -zc.y), zkc = cmk<C>(zk.x, -zk.y);
+    C w = stw[k];
+    C sum = cadd(zk, zcc), dif = csub(zk, zcc);
+    C xk = cmk<C>(0.5 * sum.x, 0.5 * sum.y);
+    C wd = cmul(w, dif);
+    xk = cadd(xk, cmk<C>(0.5 * wd.y, -0.5 * wd.x));   // - i/2 * w * dif
+    if (kc != k) {
+      C w2 = stw[kc];   // kc <= N < 2N entries
+      C sum2 = cadd(zc, zkc), dif2 = csub(zc, zkc);
+      C wd2 = cmul(w2, dif2);
+      C xc = cadd(cmk<C>(0.5 * sum2.x, 0.5 * sum2.y), cmk<C>(0.5 * wd2.y, -0.5 * wd2.x));
+      s[kc * PITCH + t] = xc;
+    }
+    s[k * PITCH + t] = xk;
+  }
+  __syncthreads();
+  for (int q = threadIdx.x; q < (N + 1) * TX; q += NT) {
+    int t = q / (N + 1), p = q % (N + 1);
+    int row = row0 + t;
+    if (row < nrows) {
+      int j = row % g.npy, k = row / g.npy;
+      out[((long long)k * g.npy + j) * g.HP + p] = s[p * PITCH + t];
+    }
+  }
+}
+
+// npx == 1: X[0] = c(0, j, k)
+__global__ void k_spec_rows_n1(Model m, double dx, double dy, double dz, Geo g, double2* __restrict__ out) {
+  const int nrows = g.npy * g.npz;
+  for (int row = blockIdx.x * blockDim.x + threadIdx.x; row < nrows; row += gridDim.x * blockDim.x) {
+    int j = row % g.npy, k = row / g.npy;
+    int kp = k > g.npz / 2 ? k - g.npz : k;
+    int jp = j > g.npy / 2 ? j - g.npy : j;
+    out[(long long)row * g.HP] = make_double2(covariance(m, 0.0 * dx, (double)jp * dy, (double)kp * dz), 0.0);
+  }
+}
+
+// S = X / ntot, amp = sqrt(max(Re S, 0)), diagnostics over the full spectrum
+// (indices 0 < i < npx/2 stand for themselves and their mirror).  f90:1273-1292
+__global__ void k_spec_amp(Geo g, const double2* __restrict__ X, double* __restrict__ amp64,
+                           float* __restrict__ amp32, SpecPartial* part) {
+  const long long tot = (long long)g.npz * g.npy * g.HP;
+  const double rn = (double)g.npx * (double)g.npy * (double)g.npz;
+  double mi = 0, mr = 0, sp = 0, sn = 0;
+  for (long long q = blockIdx.x * (long long)blockDim.x + threadIdx.x; q < tot;
+       q += (long long)gridDim.x * blockDim.x) {
+    int i = (int)(q % g.HP);
+    double a = 0.0;
+    if (i < g.H) {
+      double2 v = X[q];
+      double re = v.x / rn, im = v.y / rn;
+      double w = (i == 0 || 2 * i == g.npx) ? 1.0 : 2.0;
+      mi = fmax(mi, fabs(im));
+      mr = fmax(mr, fabs(re));
+      if (re < 0.0) {
+        sn += w * re;
+      } else {
+        sp += w * re;
+        a = sqrt(re);
+      }
+    }
+    if (amp64) amp64[q] = a;
+    if (amp32) amp32[q] = (float)a;
+  }
+  __shared__ double red[4][NT / 32];
+#pragma unroll
+  for (int off = 16; off > 0; off >>= 1) {
+    mi = fmax(mi, __shfl_down_sync(0xffffffffu, mi, off));
+    mr = fmax(mr, __shfl_down_sync(0xffffffffu, mr, off));
+    sp += __shfl_down_sync(0xffffffffu, sp, off);
+    sn += __shfl_down_sync(0xffffffffu, sn, off);
+  }
+  if ((threadIdx.x & 31) == 0) {
+    int w = threadIdx.x >> 5;
+    red[0][w] = mi;
+    red[1][w] = mr;
+    red[2][w] = sp;
+    red[3][w] = sn;
+  }
+  __syncthreads();
+  if (threadIdx.x == 0) {
+    SpecPartial p{0, 0, 0, 0};
+    for (int w = 0; w < NT / 32; ++w) {
+      p.maximag = fmax(p.maximag, red[0][w]);
+      p.maxreal = fmax(p.maxreal, red[1][w]);
+      p.spos += red[2][w];
+      p.sneg += red[3][w];
+    }
+    part[blockIdx.x] = p;
+  }
+}
+
+__global__ void k_reduce_spec(const SpecPartial* part, int n, SpecPartial* out) {
+  if (threadIdx.x == 0 && blockIdx.x == 0) {
+    SpecPartial p{0, 0, 0, 0};
+    for (int q = 0; q < n; ++q) {
+      p.maximag = fmax(p.maximag, part[q].maximag);
+      p.maxreal = fmax(p.maxreal, part[q].maxreal);
+      p.spos += part[q].spos;
+      p.sneg += part[q].sneg;
+    }
+    *out = p;
+  }
+}
+
+// ---------------------------------------------------------------- launch helpers
+static int ilog2(int n) {
+  int l = 0;
+  while ((1 << l) < n) ++l;
+  return l;
+}
+
+template <typename K>
+static cudaError_t set_smem(K kernel, size_t bytes) {
+  if (bytes <= 48 * 1024) return cudaSuccess;
+  return cudaFuncSetAttribute(kernel, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)bytes);
+}
+
+#define SS3D_LOGN_SWITCH(LOGN_VAR, MAXL, CALL)                  \
+  switch (LOGN_VAR) {                                            \
+    case 0: { constexpr int L = 0; if constexpr (L <= MAXL) { CALL; } break; } \
+    case 1: { constexpr int L = 1; if constexpr (L <= MAXL) { CALL; } break; } \
+    case 2: { constexpr int L = 2; if constexpr (L <= MAXL) { CALL; } break; } \
+    case 3: { constexpr int L = 3; if constexpr (L <= MAXL) { CALL; } break; } \
+    case 4: { constexpr int L = 4; if constexpr (L <= MAXL) { CALL; } break; } \
+    case 5: { constexpr int L = 5; if constexpr (L <= MAXL) { CALL; } break; } \
+    case 6: { constexpr int L = 6; if constexpr (L <= MAXL) { CALL; } break; } \
+    case 7: { constexpr int L = 7; if constexpr (L <= MAXL) { CALL; } break; } \
+    case 8: { constexpr int L = 8; if constexpr (L <= MAXL) { CALL; } break; } \
+    case 9: { constexpr int L = 9; if constexpr (L <= MAXL) { CALL; } break; } \
+    case 10: { constexpr int L = 10; if constexpr (L <= MAXL) { CALL; } break; } \
+    case 11: { constexpr int L = 11; if constexpr (L <= MAXL) { CALL; } break; } \
+    case 12: { constexpr int L = 12; if constexpr (L <= MAXL) { CALL; } break; } \
+    default: return cudaErrorInvalidValue;                       \
+  }
+
+template <typename R> struct MaxL { static constexpr int v = MAX_LOGN_F; };
+template <> struct MaxL<double> { static constexpr int v = MAX_LOGN_D; };
+
+template <typename R, int L, int SIGN>
+static cudaError_t run_axis_c2c(const AxisArgs& a, const Geo& g, const cpx_t<R>* in, cpx_t<R>* out, Tw tw,
+                                cudaStream_t st) {
+  constexpr int TX = AxisTX<R, L>::TX;
+  size_t smem = (size_t)((1 << L) * TX + (1 << L)) * sizeof(cpx_t<R>);
+  cudaError_t e = set_smem(k_axis_c2c<R, L, SIGN>, smem);
+  if (e != cudaSuccess) return e;
+  AxisArgs b = a;
+  b.tpg = (a.lines + TX - 1) / TX;
+  unsigned blocks = (unsigned)((long long)b.tpg * a.ngroups * a.nreal);
+  k_axis_c2c<R, L, SIGN><<<blocks, NT, smem, st>>>(b, g, in, out, tw);
+  return cudaGetLastError();
+}
+
+template <typename R, int L>
+static cudaError_t run_axis_gen(const AxisArgs& a, const Geo& g, const R* amp, const uint32_t* rs,
+                                const uint32_t* apow, cpx_t<R>* out, Tw tw, cudaStream_t st) {
+  constexpr int TX = AxisTX<R, L>::TX;
+  size_t smem = (size_t)((1 << L) * TX + (1 << L)) * sizeof(cpx_t<R>);
+  cudaError_t e = set_smem(k_axis_gen<R, L>, smem);
+  if (e != cudaSuccess) return e;
+  AxisArgs b = a;
+  b.tpg = (a.lines + TX - 1) / TX;
+  unsigned blocks = (unsigned)((long long)b.tpg * a.ngroups * a.nreal);
+  k_axis_gen<R, L><<<blocks, NT, smem, st>>>(b, g, amp, rs, apow, out, tw);
+  return cudaGetLastError();
+}
+
+template <typename R, typename O, int L>
+static cudaError_t run_rows_c2r(const Geo& g, const cpx_t<R>* in, long long rstride, O* out, long long ostride,
+                                int nreal, double* part, int* nblk_out, Tw tw, cudaStream_t st) {
+  constexpr int TX = RowTX<R, L>::TX;
+  constexpr int N = 1 << L;
+  size_t smem = (size_t)((N + 1) * (TX + 1) + 2 * N) * sizeof(cpx_t<R>);
+  cudaError_t e = set_smem(k_rows_c2r<R, O, L>, smem);
+  if (e != cudaSuccess) return e;
+  int nblk = (g.ny * g.nz + TX - 1) / TX;
+  if (nblk_out) *nblk_out = nblk;
+  k_rows_c2r<R, O, L><<<(unsigned)((long long)nblk * nreal), NT, smem, st>>>(g, in, rstride, out, ostride, nreal,
+                                                                            nblk, part, tw);
+  return cudaGetLastError();
+}
+
+template <int L>
+static cudaError_t run_spec_rows(const Model& m, const double d[3], const Geo& g, double2* out, Tw tw,
+                                 cudaStream_t st) {
+  constexpr int TX = RowTX<double, L>::TX;
+  constexpr int N = 1 << L;
+  size_t smem = (size_t)((N + 1) * (TX + 1) + 2 * N) * sizeof(double2);
+  cudaError_t e = set_smem(k_spec_rows<L>, smem);
+  if (e != cudaSuccess) return e;
+  int nblk = (g.npy * g.npz + TX - 1) / TX;
+  k_spec_rows<L><<<nblk, NT, smem, st>>>(m, d[0], d[1], d[2], g, out, tw);
+  return cudaGetLastError();
+}
+
+// x pass rows kernel: number of row blocks per realization (for the partial sums)
+int realize_part_blocks(const Geo& g, bool dbl) {
+  if (g.npx == 1) return (g.ny * g.nz + NT - 1) / NT;
+  int L = ilog2(g.npx) - 1;
+  int E = dbl ? TileE<double>::E : TileE<float>::E;
+  int tx = std::min(64, std::max(1, E >> L));
+  return (g.ny * g.nz + tx - 1) / tx;
+}
+
+// ---------------------------------------------------------------- public launchers
+cudaError_t launch_spectrum(const Model& m, const double d[3], const Geo& g, double2* work, double* amp64,
+                            float* amp32, SpecPartial* part, int npart_max, SpecPartial* result, Tw tw,
+                            cudaStream_t st) {
+  cudaError_t e;
+  if (g.npx == 1) {
+    int nrows = g.npy * g.npz;
+    k_spec_rows_n1<<<(nrows + NT - 1) / NT, NT, 0, st>>>(m, d[0], d[1], d[2], g, work);
+    e = cudaGetLastError();
+  } else {
+    int L = ilog2(g.npx) - 1;
+    e = cudaErrorInvalidValue;
+    SS3D_LOGN_SWITCH(L, MAX_LOGN_D, e = run_spec_rows<L>(m, d, g, work, tw, st));
+  }
+  if (e != cudaSuccess) return e;
+  if (g.npy > 1) {
+    AxisArgs a{};
+    a.S = g.HP;
+    a.nout = g.npy;
+    a.lines = g.H;
+    a.ngroups = g.npz;
+    a.gstride = (long long)g.npy * g.HP;
+    a.rstride = 0;
+    a.nreal = 1;
+    a.axis = 1;
+    int L = ilog2(g.npy);
+    e = cudaErrorInvalidValue;
+    SS3D_LOGN_SWITCH(L, MAX_LOGN_D, e = (run_axis_c2c<double, L, -1>(a, g, work, work, tw, st)));
+    if (e != cudaSuccess) return e;
+  }
+  if (g.npz > 1) {
+    AxisArgs a{};
+    a.S = (long long)g.npy * g.HP;
+    a.nout = g.npz;
+    a.lines = g.npy * g.HP;
+    a.ngroups = 1;
+    a.gstride = 0;
+    a.rstride = 0;
+    a.nreal = 1;
+    a.axis = 2;
+    int L = ilog2(g.npz);
+    e = cudaErrorInvalidValue;
+    SS3D_LOGN_SWITCH(L, MAX_LOGN_D, e = (run_axis_c2c<double, L, -1>(a, g, work, work, tw, st)));
+    if (e != cudaSuccess) return e;
+  }
+  long long tot = (long long)g.npz * g.npy * g.HP;
+  int nb = (int)std::min<long long>(npart_max, (tot + NT - 1) / NT);
+  k_spec_amp<<<nb, NT, 0, st>>>(g, work, amp64, amp32, part);
+  if ((e = cudaGetLastError()) != cudaSuccess) return e;
+  k_reduce_spec<<<1, 32, 0, st>>>(part, nb, result);
+  return cudaGetLastError();
+}
+
+cudaError_t launch_rowstates(const Geo& g, uint32_t s0, long long r_first, int nreal, const uint32_t* ptab,
+                             uint32_t* rowstates, uint32_t* apow, cudaStream_t st) {
+  long long tot = (long long)g.npy * g.npz * nreal;
+  int nb = (int)std::min<long long>(4096, (tot + NT - 1) / NT);
+  k_rowstates<<<nb, NT, 0, st>>>(g, s0, r_first, nreal, ptab, rowstates);
+  cudaError_t e = cudaGetLastError();
+  if (e != cudaSuccess || apow == nullptr) return e;
+  k_apow<<<(g.npx + NT - 1) / NT, NT, 0, st>>>(g.npx, g.d, ptab, apow);
+  return cudaGetLastError();
+}
+
+template <typename R>
+cudaError_t launch_gen(const Geo& g, const R* amp, const uint32_t* rowstates, const uint32_t* apow,
+                       cpx_t<R>* work, long long wstride, int nreal, cudaStream_t st) {
+  long long tot = (long long)g.npz * g.npy * g.HP * nreal;
+  int nb = (int)std::min<long long>(148 * 16, (tot + NT - 1) / NT);
+  k_gen<R><<<nb, NT, 0, st>>>(g, amp, rowstates, apow, work, wstride, nreal);
+  return cudaGetLastError();
+}
+
+template <typename R>
+cudaError_t launch_realize(const Geo& g, const R* amp, const uint32_t* rowstates, const uint32_t* apow,
+                           cpx_t<R>* work, long long wstride, int nreal, void* out, int out_kind, double* part,
+                           int* nblk_per_r, Tw tw, bool fused, cudaStream_t st) {
+  constexpr int ML = MaxL<R>::v;
+  cudaError_t e = cudaSuccess;
+  // first inverse axis: z if present, else y, else only x
+  if (g.npz > 1) {
+    AxisArgs a{};
+    a.S = (long long)g.npy * g.HP;
+    a.nout = g.nz;
+    a.lines = g.npy * g.HP;
+    a.ngroups = 1;
+    a.gstride = 0;
+    a.rstride = wstride;
+    a.nreal = nreal;
+    a.axis = 2;
+    int L = ilog2(g.npz);
+    if (fused) {
+      e = cudaErrorInvalidValue;
+      SS3D_LOGN_SWITCH(L, ML, e = (run_axis_gen<R, L>(a, g, amp, rowstates, apow, work, tw, st)));
+    } else {
+      e = launch_gen<R>(g, amp, rowstates, apow, work, wstride, nreal, st);
+      if (e != cudaSuccess) return e;
+      e = cudaErrorInvalidValue;
+      SS3D_LOGN_SWITCH(L, ML, e = (run_axis_c2c<R, L, +1>(a, g, work, work, tw, st)));
+    }
+    if (e != cudaSuccess) return e;
+    if (g.npy > 1) {
+      AxisArgs b{};
+      b.S = g.HP;
+      b.nout = g.ny;
+      b.lines = g.H;
+      b.ngroups = g.nz;
+      b.gstride = (long long)g.npy * g.HP;
+      b.rstride = wstride;
+      b.nreal = nreal;
+      b.axis = 1;
+      int Ly = ilog2(g.npy);
+      e = cudaErrorInvalidValue;
+      SS3D_LOGN_SWITCH(Ly, ML, e = (run_axis_c2c<R, L, +1>(b, g, work, work, tw, st)));
+      if (e != cudaSuccess) return e;
+    }
+  } else if (g.npy > 1) {
+    AxisArgs b{};
+    b.S = g.HP;
+    b.nout = g.ny;
+    b.lines = g.H;
+    b.ngroups = 1;
+    b.gstride = (long long)g.npy * g.HP;
+    b.rstride = wstride;
+    b.nreal = nreal;
+    b.axis = 1;
+    int Ly = ilog2(g.npy);
+    if (fused) {
+      e = cudaErrorInvalidValue;
+      SS3D_LOGN_SWITCH(Ly, ML, e = (run_axis_gen<R, L>(b, g, amp, rowstates, apow, work, tw, st)));
+    } else {
+      e = launch_gen<R>(g, amp, rowstates, apow, work, wstride, nreal, st);
+      if (e != cudaSuccess) return e;
+      e = cudaErrorInvalidValue;
+      SS3D_LOGN_SWITCH(Ly, ML, e = (run_axis_c2c<R, L, +1>(b, g, work, work, tw, st)));
+    }
+    if (e != cudaSuccess) return e;
+  } else {
+    e = launch_gen<R>(g, amp, rowstates, apow, work, wstride, nreal, st);
+    if (e != cudaSuccess) return e;
+  }
+  // x pass
+  const long long ostride = (long long)g.nx * g.ny * g.nz;
+  if (g.npx == 1) {
+    int nblk = (g.ny * g.nz + NT - 1) / NT;
+    if (nblk_per_r) *nblk_per_r = nblk;
+    if (out_kind == 0)
+      k_rows_copy<R, float><<<nblk * nreal, NT, 0, st>>>(g, work, wstride, (float*)out, ostride, nreal, nblk, part);
+    else
+      k_rows_copy<R, double><<<nblk * nreal, NT, 0, st>>>(g, work, wstride, (double*)out, ostride, nreal, nblk,
+                                                          part);
+    return cudaGetLastError();
+  }
+  int Lx = ilog2(g.npx) - 1;
+  e = cudaErrorInvalidValue;
+  if (out_kind == 0) {
+    SS3D_LOGN_SWITCH(Lx, ML,
+                     e = (run_rows_c2r<R, float, L>(g, work, wstride, (float*)out, ostride, nreal, part,
+                                                     nblk_per_r, tw, st)));
+  } else {
+    SS3D_LOGN_SWITCH(Lx, ML,
+                     e = (run_rows_c2r<R, double, L>(g, work, wstride, (double*)out, ostride, nreal, part,
+                                                      nblk_per_r, tw, st)));
+  }
+  return e;
+}
+
+cudaError_t launch_debug_states(const Geo& g, const uint32_t* rowstates, const uint32_t* apow, uint32_t* out,
+                                cudaStream_t st) {
+  long long tot = (long long)g.npz * g.npy * g.H;
+  int nb = (int)std::min<long long>(4096, (tot + NT - 1) / NT);
+  k_debug_states<<<nb, NT, 0, st>>>(g, rowstates, apow, out);
+  return cudaGetLastError();
+}
+
+cudaError_t launch_reduce_zstats(const double* part, int nblk_per_r, int nreal, double* zsum, cudaStream_t st) {
+  k_reduce_zstats<<<nreal, NT, 0, st>>>(part, nblk_per_r, zsum);
+  return cudaGetLastError();
+}
+
+template cudaError_t launch_realize<float>(const Geo&, const float*, const uint32_t*, const uint32_t*, float2*,
+                                           long long, int, void*, int, double*, int*, Tw, bool, cudaStream_t);
+template cudaError_t launch_realize<double>(const Geo&, const double*, const uint32_t*, const uint32_t*, double2*,
+                                            long long, int, void*, int, double*, int*, Tw, bool, cudaStream_t);
+template cudaError_t launch_gen<float>(const Geo&, const float*, const uint32_t*, const uint32_t*, float2*,
+                                       long long, int, cudaStream_t);
+template cudaError_t launch_gen<double>(const Geo&, const double*, const uint32_t*, const uint32_t*, double2*,
+                                        long long, int, cudaStream_t);
+
+}  // namespace ss3d

@@ -1,0 +1,79 @@
+// ss3d_internal.h -- host/device shared declarations of the CUDA library
+// (not part of the public C ABI in include/specsim3d_gpu.h).
+#pragma once
+#include <cuda_runtime.h>
+
+#include <cmath>
+#include <cstdint>
+#include <string>
+
+#include "ss3d_device.cuh"
+
+namespace ss3d {
+
+constexpr int MAXST = 10;          // f90:93
+constexpr int MAX_LOGN_F = 12;     // longest axis kept in shared memory, float
+constexpr int MAX_LOGN_D = 11;     // longest axis kept in shared memory, double
+constexpr int TW_LOG_MAX = 13;     // twiddle tables for n = 1 .. 2^13
+
+// Twiddle tables: for n = 2^L the table e^{-2 pi i m / n}, m in [0, n), starts
+// at offset n - 1.
+struct Tw {
+  const float2* f;
+  const double2* d;
+};
+
+// Variogram model after setrot (f90:95-139), in kernel-parameter form.
+struct Model {
+  int nst;
+  double nugget;
+  int itype[MAXST];
+  double sill[MAXST], ahmax[MAXST];
+  double rot[MAXST][9];   // row-major rot(r, c) -> rot[s][3*r + c]
+};
+
+// covariance, f90:153-178
+__host__ __device__ inline double covariance(const Model& m, double dx, double dy, double dz) {
+  double c = 0.0;
+  if (dx == 0.0 && dy == 0.0 && dz == 0.0) c = m.nugget;
+  for (int i = 0; i < m.nst; i++) {
+    const double* r = m.rot[i];
+    double rx = r[0] * dx + r[1] * dy + r[2] * dz;
+    double ry = r[3] * dx + r[4] * dy + r[5] * dz;
+    double rz = r[6] * dx + r[7] * dy + r[8] * dz;
+    double h = sqrt(rx * rx + ry * ry + rz * rz);
+    double hr = h / m.ahmax[i];
+    if (m.itype[i] == 1) {
+      if (hr < 1.0) c = c + m.sill[i] * (1.0 - 1.5 * hr + 0.5 * (hr * hr * hr));
+    } else if (m.itype[i] == 2) {
+      c = c + m.sill[i] * exp(-3.0 * hr);
+    } else {
+      c = c + m.sill[i] * exp(-(3.0 * hr * hr));
+    }
+  }
+  return c;
+}
+
+// Spectrum diagnostics, f90:1275-1292, accumulated over the full spectrum
+struct SpecPartial {
+  double maximag, maxreal, spos, sneg;
+};
+
+// ---- launchers (ss3d_fft.cu); all return cudaError_t of the last launch
+cudaError_t launch_spectrum(const Model& m, const double d[3], const Geo& g, double2* work, double* amp64,
+                            float* amp32, SpecPartial* part, int npart_max, SpecPartial* result, Tw tw,
+                            cudaStream_t st);
+cudaError_t launch_rowstates(const Geo& g, uint32_t s0, long long r_first, int nreal, const uint32_t* ptab,
+                             uint32_t* rowstates, uint32_t* apow, cudaStream_t st);
+// out_kind: 0 float output, 1 double output
+template <typename R>
+cudaError_t launch_realize(const Geo& g, const R* amp, const uint32_t* rowstates, const uint32_t* apow,
+                           cpx_t<R>* work, long long wstride, int nreal, void* out, int out_kind,
+                           double* part, int* nblk_per_r, Tw tw, bool fused, cudaStream_t st);
+template <typename R>
+cudaError_t launch_gen(const Geo& g, const R* amp, const uint32_t* rowstates, const uint32_t* apow,
+                       cpx_t<R>* work, long long wstride, int nreal, cudaStream_t st);
+cudaError_t launch_reduce_zstats(const double* part, int nblk_per_r, int nreal, double* zsum, cudaStream_t st);
+int realize_part_blocks(const Geo& g, bool dbl);
+
+}  // namespace ss3d

@@ -1,0 +1,146 @@
+"""GPU parity of the spectrum and the realization path against the CPU oracle.
+
+Bars (stated per test):
+  * Park-Miller states: bit-exact, every coefficient, several realizations.
+  * FP64 spectrum amplitudes: 1e-12 of max amp (different FFT order).
+  * FP64 realizations: max |gpu - oracle| <= 1e-9 * sqrt(C0) (the FFT
+    algorithms differ in rounding order; spectral values that sit at the FP64
+    noise floor of the forward FFT give the remaining difference).
+  * FP32 realizations: max |gpu - oracle| <= 1e-5 * sqrt(C0), the precision-form
+    target.
+"""
+import numpy as np
+import pytest
+
+import oracle_lib as ora
+import recipes
+
+pytestmark = pytest.mark.gpu
+
+CASES = [
+    # (n, structs, nugget, d, ipad)
+    ((64, 64, 16), [(1, 1.0, 20.0, 10.0, 5.0, 45.0, 0.0, 0.0)], 0.0, (1.0, 1.0, 1.0), 1),       # cfg1 model
+    ((30, 20, 9), [(2, 0.7, 12.0, 6.0, 3.0, 30.0, 10.0, 5.0)], 0.3, (1.0, 1.5, 0.5), 1),        # odd, anisotropic
+    ((17, 33, 1), [(3, 1.0, 8.0, 4.0, 4.0, 120.0, 0.0, 0.0)], 0.1, (1.0, 1.0, 1.0), 1),         # 2D
+    ((16, 16, 16), [(2, 1.0, 5.0, 5.0, 5.0, 0.0, 0.0, 0.0)], 0.0, (1.0, 1.0, 1.0), 0),          # compact ipad 0
+    ((12, 7, 5), [(1, 0.5, 6.0, 3.0, 2.0, 300.0, -20.0, 15.0), (2, 0.4, 3.0, 3.0, 1.0, 0, 0, 0)], 0.1,
+     (1.0, 1.0, 1.0), 0),                                                                       # nested, ipad 0
+    ((1, 24, 10), [(2, 1.0, 6.0, 3.0, 2.0, 0.0, 0.0, 0.0)], 0.0, (1.0, 1.0, 1.0), 0),           # npx = 1
+]
+
+
+def _expected_states(full, np3):
+    """First-draw state per half-spectrum index: own draw, or the partner's draw."""
+    npx, npy, npz = np3
+    h = npx // 2 + 1 if npx >= 2 else 1
+    k, j, i = np.meshgrid(np.arange(npz), np.arange(npy), np.arange(h), indexing="ij")
+    own = full[k, j, i]
+    part = full[(npz - k) % npz, (npy - j) % npy, (npx - i) % npx]
+    return np.where(own != 0, own, part)
+
+
+@pytest.mark.parametrize("case", range(len(CASES)))
+@pytest.mark.parametrize("igauss", [0, 1])
+def test_rng_states_bit_exact(gpu, case, igauss):
+    n, sts, nug, d, ipad = CASES[case]
+    sp = gpu.Spectrum(sts, nug, d, n, ipad)
+    iseed = 69069 + 7 * case
+    full = ora.fill_states(sp.np, iseed, 3, igauss)
+    for r in range(3):
+        exp = _expected_states(full[r], sp.np)
+        got = sp.debug_states(iseed, r, igauss).astype(np.int64)
+        assert np.array_equal(got, exp), f"realization {r}: {np.count_nonzero(got != exp)} states differ"
+
+
+@pytest.mark.parametrize("case", range(len(CASES)))
+def test_spectrum_fp64(gpu, case):
+    n, sts, nug, d, ipad = CASES[case]
+    sp = gpu.Spectrum(sts, nug, d, n, ipad)
+    np3, rc = ora.grid(sts, d, n, ipad)
+    assert rc == 0 and tuple(np3) == sp.np
+    amp_o, st_o = ora.spectrum(sts, nug, d, sp.np)
+    amp_g = sp.amp()
+    ref = recipes.half_of_full(amp_o, sp.np[0])
+    assert np.max(np.abs(amp_g - ref)) <= 1e-12 * np.max(ref)
+    assert sp.stats["c0"] == st_o["c0"]
+    assert abs(sp.stats["spos"] - st_o["spos"]) <= 1e-12 * st_o["spos"]
+    assert abs(sp.stats["sneg"] - st_o["sneg"]) <= 1e-12 * st_o["spos"]
+    assert abs(sp.stats["maxreal"] - st_o["maxreal"]) <= 1e-12 * st_o["maxreal"]
+
+
+@pytest.mark.parametrize("case", range(len(CASES)))
+@pytest.mark.parametrize("igauss", [0, 1])
+def test_coefficients_fp64(gpu, case, igauss):
+    n, sts, nug, d, ipad = CASES[case]
+    sp = gpu.Spectrum(sts, nug, d, n, ipad)
+    amp_o, _ = ora.spectrum(sts, nug, d, sp.np)
+    iseed = 4711 + case
+    for r in (0, 1):
+        co = recipes.half_of_full(ora.coefficients(amp_o, sp.np, iseed, r, igauss), sp.np[0])
+        cg = sp.debug_coefficients(iseed, r, igauss, gpu.FP64)
+        scale = max(np.max(np.abs(co)), 1e-300)
+        assert np.max(np.abs(cg - co)) <= 1e-12 * scale
+
+
+@pytest.mark.parametrize("case", range(len(CASES)))
+@pytest.mark.parametrize("igauss", [0, 1])
+def test_realize_fp64_vs_oracle(gpu, case, igauss):
+    n, sts, nug, d, ipad = CASES[case]
+    sp = gpu.Spectrum(sts, nug, d, n, ipad)
+    amp_o, st = ora.spectrum(sts, nug, d, sp.np)
+    iseed, nreal = 1234 + case, 3
+    res_o, zs_o = ora.realize(amp_o, sp.np, n, iseed, nreal, igauss)
+    res_g, zs_g = sp.realize(iseed, nreal, igauss, gpu.FP64, zstats=True)
+    c0 = st["c0"]
+    err = np.max(np.abs(res_g - res_o))
+    assert err <= 1e-9 * np.sqrt(c0), err
+    assert np.allclose(zs_g[:, :2], zs_o[:, :2], rtol=0, atol=1e-9)
+
+
+@pytest.mark.parametrize("case", range(len(CASES)))
+@pytest.mark.parametrize("igauss", [0, 1])
+def test_realize_fp32_vs_oracle(gpu, case, igauss):
+    n, sts, nug, d, ipad = CASES[case]
+    sp = gpu.Spectrum(sts, nug, d, n, ipad)
+    amp_o, st = ora.spectrum(sts, nug, d, sp.np)
+    iseed, nreal = 99 + case, 2
+    res_o, _ = ora.realize(amp_o, sp.np, n, iseed, nreal, igauss)
+    res_g = sp.realize(iseed, nreal, igauss, gpu.FP32, dtype=np.float32)
+    err = np.max(np.abs(res_g.astype(np.float64) - res_o)) / np.sqrt(st["c0"])
+    assert err <= 1e-5, err
+
+
+def test_sharding_is_exact(gpu):
+    n, sts, nug, d, ipad = CASES[1]
+    sp = gpu.Spectrum(sts, nug, d, n, ipad)
+    for prec in (gpu.FP64, gpu.FP32):
+        full = sp.realize(555, 5, 1, prec)
+        for r0, k in ((0, 2), (2, 3), (4, 1), (1, 3)):
+            part = sp.realize(555, k, 1, prec, r_first=r0)
+            assert np.array_equal(part, full[r0:r0 + k])
+
+
+def test_device_output_matches_host(gpu):
+    import torch
+    n, sts, nug, d, ipad = CASES[0]
+    sp = gpu.Spectrum(sts, nug, d, n, ipad)
+    host = sp.realize(31, 2, 0, gpu.FP32, dtype=np.float32)
+    dev = torch.empty((2, n[2], n[1], n[0]), dtype=torch.float32, device="cuda")
+    sp.realize(31, 2, 0, gpu.FP32, out=dev)
+    torch.cuda.synchronize()
+    assert np.array_equal(dev.cpu().numpy(), host)
+
+
+@pytest.mark.parametrize("n", [32, 64])
+def test_golden_scaling_rms(gpu, n):
+    """Reference-published RMS of realization 1 (docs/figures/scaling_cached.json)."""
+    import json
+    import os
+    pins = json.load(open(os.path.join(os.path.dirname(__file__), "golden", "reference_pins.json")))
+    want = [p for p in pins["scaling_rms"] if p["n"] == n][0]
+    c = recipes.scaling_case(n)
+    sp = gpu.Spectrum(c["structs"], c["nugget"], c["d"], c["n"], c["ipad"])
+    assert list(sp.np) == want["periodic"]
+    res = sp.realize(c["seed"], 1, 0, gpu.FP64, dtype=np.float32)
+    rms = recipes.scaling_rms(res[0])
+    assert abs(rms - want["rms"]) <= 1e-9 * want["rms"], (rms, want["rms"])
