@@ -181,6 +181,17 @@ const char *ss3d_last_error(void);
 /* Library version string. */
 const char *ss3d_version(void);
 
+/* Stage timing of the realization path (the reference prints only wall-clock
+ * totals, f90:1299-1300, 1350-1351).  With profiling on, ss3d_realize records
+ * CUDA events around each stage on its stream; ss3d_profile_read returns the
+ * accumulated milliseconds and launch counts per stage since the last reset:
+ *   0 row states, 1 synthesis + first inverse pass, 2 middle inverse pass,
+ *   3 C2R x pass + crop, 4 statistics.
+ * launches_total counts every kernel launched by the library. */
+#define SS3D_NSTAGE 5
+int ss3d_profile(int enable);
+int ss3d_profile_read(double ms[SS3D_NSTAGE], int64_t launches[SS3D_NSTAGE], int64_t *launches_total);
+
 #ifdef __cplusplus
 }
 #endif

@@ -59,6 +59,25 @@ def set_stream(stream):
     L.check(L.lib().ss3d_set_stream(ctypes.c_void_p(h)))
 
 
+NSTAGE = 5
+STAGES = ("rowstates", "synthesis+first_pass", "middle_pass", "x_c2r_crop", "stats")
+
+
+def profile(enable=True):
+    """Switch per-stage CUDA-event timing of the realization path on/off (resets counters)."""
+    L.check(L.lib().ss3d_profile(1 if enable else 0))
+
+
+def profile_read():
+    """{stage: (ms, launches)} accumulated since profile(True), and the total launch count."""
+    ms = np.zeros(NSTAGE)
+    ln = np.zeros(NSTAGE, dtype=np.int64)
+    tot = ctypes.c_int64()
+    L.check(L.lib().ss3d_profile_read(ctypes.c_void_p(ms.ctypes.data), ctypes.c_void_p(ln.ctypes.data),
+                                      ctypes.byref(tot)))
+    return {name: (float(ms[q]), int(ln[q])) for q, name in enumerate(STAGES)}, int(tot.value)
+
+
 def _out_ptr(out):
     """(pointer, dtype code, nbytes) of a numpy array or a torch tensor."""
     if isinstance(out, np.ndarray):

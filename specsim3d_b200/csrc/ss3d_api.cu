@@ -43,6 +43,52 @@ static int cuda_fail(cudaError_t e, const char* what) {
   } while (0)
 
 extern "C" const char* ss3d_last_error(void) { return g_err.c_str(); }
+
+// ---------------------------------------------------------------- stage profiling
+static bool g_prof = false;
+static double g_prof_ms[SS3D_NSTAGE];
+static int64_t g_prof_launch[SS3D_NSTAGE];
+static unsigned long long g_mark_launch[16];
+
+void ss3d::mark(Marks* m, int stage, cudaStream_t st) {
+  if (!m || !m->on || m->n >= 16) return;
+  if (cudaEventCreate(&m->ev[m->n]) != cudaSuccess) return;
+  cudaEventRecord(m->ev[m->n], st);
+  m->stage[m->n] = stage;
+  g_mark_launch[m->n] = g_launch_count;
+  m->n++;
+}
+
+static void marks_collect(Marks& m) {
+  for (int q = 0; q + 1 < m.n; q++) {
+    float ms = 0.f;
+    if (cudaEventElapsedTime(&ms, m.ev[q], m.ev[q + 1]) == cudaSuccess && m.stage[q] >= 0 &&
+        m.stage[q] < SS3D_NSTAGE) {
+      g_prof_ms[m.stage[q]] += ms;
+      g_prof_launch[m.stage[q]] += (int64_t)(g_mark_launch[q + 1] - g_mark_launch[q]);
+    }
+  }
+  for (int q = 0; q < m.n; q++) cudaEventDestroy(m.ev[q]);
+  m.n = 0;
+}
+
+extern "C" int ss3d_profile(int enable) {
+  g_prof = enable != 0;
+  for (int q = 0; q < SS3D_NSTAGE; q++) {
+    g_prof_ms[q] = 0;
+    g_prof_launch[q] = 0;
+  }
+  return SS3D_OK;
+}
+
+extern "C" int ss3d_profile_read(double ms[SS3D_NSTAGE], int64_t launches[SS3D_NSTAGE], int64_t* launches_total) {
+  for (int q = 0; q < SS3D_NSTAGE; q++) {
+    if (ms) ms[q] = g_prof_ms[q];
+    if (launches) launches[q] = g_prof_launch[q];
+  }
+  if (launches_total) *launches_total = (int64_t)g_launch_count;
+  return SS3D_OK;
+}
 extern "C" const char* ss3d_version(void) { return "specsim3d_b200 0.1 (sm_100a)"; }
 extern "C" int ss3d_set_stream(void* stream) {
   g_stream = (cudaStream_t)stream;
@@ -463,23 +509,28 @@ extern "C" int ss3d_realize(const ss3d_spectrum* csp, int iseed, int64_t r_first
     CK(cudaEventCreateWithFlags(&done[1], cudaEventDisableTiming));
   }
   cudaError_t e = cudaSuccess;
+  Marks marks;
+  marks.on = g_prof;
   int ib = 0;
   for (int r0 = 0; r0 < nreal && e == cudaSuccess; r0 += bt, ++ib) {
     int nb = std::min(bt, nreal - r0);
     int slot = ib & 1;
     void* dst = dev_out ? (void*)((char*)out + (size_t)r0 * M * oel) : (void*)stage[slot];
     if (!dev_out && ib >= 2) e = cudaStreamWaitEvent(s, done[slot], 0);
+    mark(&marks, 0, s);
     if (e == cudaSuccess) e = launch_rowstates(g, s0, r_first + r0, nb, ctx->ptab, rs, r0 == 0 ? apow : nullptr, s);
     int nblk = 0;
     if (e == cudaSuccess) {
       if (dbl)
-        e = launch_realize<double>(g, sp->amp64, rs, apow, (double2*)work, wstride, nb, dst, out_dtype, part, &nblk,
-                                   tw, true, s);
+        e = launch_realize<double>(g, sp->amp64, rs, apow, (double2*)work, wstride, nb, dst, out_dtype,
+                                   zstats ? part : nullptr, &nblk, tw, true, s, &marks);
       else
-        e = launch_realize<float>(g, sp->amp32, rs, apow, (float2*)work, wstride, nb, dst, out_dtype, part, &nblk,
-                                  tw, true, s);
+        e = launch_realize<float>(g, sp->amp32, rs, apow, (float2*)work, wstride, nb, dst, out_dtype,
+                                  zstats ? part : nullptr, &nblk, tw, true, s, &marks);
     }
+    mark(&marks, 4, s);
     if (e == cudaSuccess && zstats) e = launch_reduce_zstats(part, nblk, nb, zs + 2 * (size_t)r0, s);
+    mark(&marks, -1, s);
     if (e == cudaSuccess && !dev_out) {
       cudaEvent_t ready;
       e = cudaEventCreateWithFlags(&ready, cudaEventDisableTiming);
@@ -499,6 +550,7 @@ extern "C" int ss3d_realize(const ss3d_spectrum* csp, int iseed, int64_t r_first
   }
   if (e == cudaSuccess) e = cudaStreamSynchronize(s);
   if (e == cudaSuccess && cs) e = cudaStreamSynchronize(cs);
+  if (marks.on) marks_collect(marks);
   if (cs) {
     cudaStreamDestroy(cs);
     cudaEventDestroy(done[0]);

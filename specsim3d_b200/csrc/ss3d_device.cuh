@@ -108,29 +108,49 @@ __host__ __device__ __forceinline__ int row_class(const Geo& g, int j, int k) {
 }
 
 // ---------------------------------------------------------------- coefficient synthesis
-// Unit phasor e^{2 pi i s/m} in float with the quadrant taken exactly in integers.
+// Unit phasor e^{2 pi i s/m} in float.  The nearest quarter turn n is taken
+// in integers (exact), the remainder |x| <= pi/4 goes through Taylor
+// polynomials of sin (to x^9) and cos (to x^8): truncation below 3e-8, argument
+// error below 5e-8 (one float rounding of the exact integer remainder).
 __device__ __forceinline__ void phasor_f(uint32_t s, float& c, float& sn) {
-  uint64_t q = 4ull * s;
-  int quad = (q >= 2ull * PM_M) ? ((q >= 3ull * PM_M) ? 3 : 2) : ((q >= PM_M) ? 1 : 0);
-  uint32_t rem = (uint32_t)(q - (uint64_t)quad * PM_M);
-  float x = (float)rem * (1.0f / 2147483647.0f);    // in [0,1): quarter turns
-  float s0, c0;
-  sincospif(0.5f * x, &s0, &c0);
-  switch (quad) {
-    case 0: c = c0; sn = s0; break;
-    case 1: c = -s0; sn = c0; break;
-    case 2: c = -c0; sn = -s0; break;
-    default: c = s0; sn = -c0; break;
+  const uint64_t q = 4ull * s;
+  int n = __float2int_rn((float)s * (4.0f / 2147483647.0f));   // nearest quarter (off by one at most)
+  const long long rem = (long long)q - (long long)n * (long long)PM_M;
+  const float x = (float)rem * 7.3145904e-10f;                  // (pi/2) / (2^31-1)
+  const float x2 = x * x;
+  const float sp = x * fmaf(x2, fmaf(x2, fmaf(x2, fmaf(x2, 2.7557319e-6f, -1.9841270e-4f), 8.3333333e-3f),
+                                     -1.6666667e-1f), 1.0f);
+  const float cp = fmaf(x2, fmaf(x2, fmaf(x2, fmaf(x2, 2.4801587e-5f, -1.3888889e-3f), 4.1666667e-2f), -0.5f), 1.0f);
+  switch (n & 3) {
+    case 0: c = cp; sn = sp; break;
+    case 1: c = -sp; sn = cp; break;
+    case 2: c = -cp; sn = -sp; break;
+    default: c = sp; sn = -cp; break;
   }
 }
 __device__ __forceinline__ void phasor_d(uint32_t s, double& c, double& sn) {
   double u = (double)s / 2147483647.0;
   sincospi(2.0 * u, &sn, &c);
 }
-// -2 ln(s/m) in float, accurate near s = m through log1p of an exact difference
+// -2 ln(s/m) in float for s in [1, m-1].  For u = s/m >= 1/2 the logarithm is
+// 2 atanh(z), z = (u-1)/(u+1) = -(m-s)/(m+s) with |z| <= 1/3, from the exact
+// integer difference m-s (odd series to z^13, truncation below 2e-8 relative);
+// below 1/2 |ln u| >= ln 2 and the hardware log2 (relative error ~2^-22) is
+// accurate enough.
 __device__ __forceinline__ float m2log_f(uint32_t s) {
-  if (s >= (1u << 30)) return -2.0f * log1pf(-(float)(PM_M - s) * (1.0f / 2147483647.0f));
-  return -2.0f * logf((float)s * (1.0f / 2147483647.0f));
+  if (s >= (1u << 30)) {
+    const float a = (float)(PM_M - s);
+    const float z = -__fdividef(a, 4294967294.0f - a);        // m + s = 2m - (m - s)
+    const float z2 = z * z;
+    float p = fmaf(z2, 1.0f / 13.0f, 1.0f / 11.0f);
+    p = fmaf(z2, p, 1.0f / 9.0f);
+    p = fmaf(z2, p, 1.0f / 7.0f);
+    p = fmaf(z2, p, 1.0f / 5.0f);
+    p = fmaf(z2, p, 1.0f / 3.0f);
+    p = fmaf(z2, p, 1.0f);
+    return -4.0f * (p * z);
+  }
+  return -1.3862944f * __log2f((float)s * (1.0f / 2147483647.0f));   // -2 ln 2 * log2(u)
 }
 __device__ __forceinline__ double m2log_d(uint32_t s) {
   double u = (double)s / 2147483647.0;
@@ -173,7 +193,8 @@ __device__ __forceinline__ cpx_t<R> coefficient(const Geo& g, int i, int j, int 
   if (g.d == 2) {
     uint32_t s2 = pm_mulmod(s1, PM_A);
     if constexpr (sizeof(R) == 4) {
-      float rr = sqrtf(m2log_f(s1));
+      const float L = m2log_f(s1);
+      float rr = L * rsqrtf(L);
       float cs, sn;
       phasor_f(s2, cs, sn);
       if (self) return cmk<C>(amp * (rr * cs), 0.f);
@@ -198,6 +219,46 @@ __device__ __forceinline__ cpx_t<R> coefficient(const Geo& g, int i, int j, int 
     R cs, sn;
     if constexpr (sizeof(R) == 4) phasor_f(s1, cs, sn); else phasor_d(s1, cs, sn);
     return cmk<C>(amp * cs, conj ? -(amp * sn) : amp * sn);
+  }
+}
+
+// Coefficient of index (i, j, k) with the index-i dependent parts precomputed
+// by the caller: ai = 16807^(d i), aip = 16807^(d ((npx - i) mod npx)),
+// iedge = (i == 0 or 2 i == npx).  Same values as coefficient().
+template <typename R>
+__device__ __forceinline__ cpx_t<R> coef_col(const Geo& g, int j, int k, R amp, const uint32_t* __restrict__ rs,
+                                             uint32_t ai, uint32_t aip, bool iedge) {
+  using C = cpx_t<R>;
+  const int jp = (-j) & (g.npy - 1), kp = (-k) & (g.npz - 1);
+  const bool less = k < kp || (k == kp && j < jp);
+  const bool greater = k > kp || (k == kp && j > jp);
+  const int row = greater ? jp + g.npy * kp : j + g.npy * k;
+  const uint32_t s1 = pm_mulmod(__ldg(rs + row), greater ? aip : ai);
+  const bool self = !less && !greater && iedge;
+  if (g.d == 2) {
+    const uint32_t s2 = pm_mulmod(s1, PM_A);
+    if constexpr (sizeof(R) == 4) {
+      const float L = m2log_f(s1);
+      const float rr = L * rsqrtf(L);
+      float cs, sn;
+      phasor_f(s2, cs, sn);
+      if (self) return cmk<C>(amp * (rr * cs), 0.f);
+      const float a = amp * 0.70710678118654752f;
+      return cmk<C>(a * (rr * cs), (greater ? -a : a) * (rr * sn));
+    } else {
+      const double rr = sqrt(m2log_d(s1));
+      double cs, sn;
+      phasor_d(s2, cs, sn);
+      const double g1 = rr * cs, g2 = rr * sn;
+      if (self) return cmk<C>(amp * g1, 0.0);
+      const double h = 0.70710678118654757;
+      return cmk<C>(amp * g1 * h, amp * (greater ? -g2 : g2) * h);
+    }
+  } else {
+    if (self) return cmk<C>((2ull * s1) < (uint64_t)PM_M ? amp : -amp, R(0));
+    R cs, sn;
+    if constexpr (sizeof(R) == 4) phasor_f(s1, cs, sn); else phasor_d(s1, cs, sn);
+    return cmk<C>(amp * cs, greater ? -(amp * sn) : amp * sn);
   }
 }
 

@@ -1,0 +1,121 @@
+// ss3d_engine.cuh -- register-resident Stockham FFT of a tile of TX columns.
+//
+// Thread layout: t = threadIdx.x % TX is the column, c = threadIdx.x / TX its
+// rank among the TPC threads of that column.  Every thread owns ET = N / TPC
+// elements in registers at all times.  The first radix pass reads its inputs
+// straight from the loader (global memory or on-the-fly synthesis), the last
+// pass hands its outputs straight to the storer; only the exchanges between
+// passes go through shared memory (layout s[position * TX + t]).  For
+// N = 512 = 8 * 8 * 8 this is two shared-memory round trips per element.
+//
+// Stockham indexing of pass p (radix R, Ns = product of earlier radices):
+// butterfly jb reads positions jb + r*N/R, multiplies input r by
+// w^(k*r), k = jb mod Ns, w = e^{SIGN 2 pi i/(Ns*R)}, applies the radix-R DFT
+// and writes positions (jb/Ns)*Ns*R + k + r*Ns.  After the last pass the data
+// are in natural order.
+#pragma once
+#include "ss3d_device.cuh"
+
+namespace ss3d {
+
+template <int LOGN, int TX, int TPC, int SIGN, int P, int PITCH, bool STORE_SYNC, typename C, class Store>
+__device__ __forceinline__ void fft_tile_rest(C* __restrict__ s, const C* __restrict__ tw, C* v, int t, int c,
+                                              Store&& store) {
+  constexpr int N = 1 << LOGN;
+  constexpr int NP = Sched<LOGN>::npass;
+  if constexpr (P < NP) {
+    constexpr int ET = N / TPC;
+    constexpr int R = Sched<LOGN>::radix(P);
+    constexpr int NS = Sched<LOGN>::ns_before(P);
+    constexpr int NBT = ET / R;
+#pragma unroll
+    for (int m = 0; m < NBT; ++m) {
+      const int jb = c + TPC * m;
+#pragma unroll
+      for (int r = 0; r < R; ++r) v[m * R + r] = s[(jb + r * (N / R)) * PITCH + t];
+    }
+#pragma unroll
+    for (int m = 0; m < NBT; ++m) {
+      const int jb = c + TPC * m;
+      const int k = jb % NS;
+#pragma unroll
+      for (int r = 1; r < R; ++r) v[m * R + r] = cmul_sgn(v[m * R + r], tw[(k * r) * (N / (NS * R))], SIGN > 0);
+      dftR<R, SIGN>(&v[m * R]);
+    }
+    if constexpr (P == NP - 1) {
+      if constexpr (STORE_SYNC) __syncthreads();
+#pragma unroll
+      for (int m = 0; m < NBT; ++m) {
+        const int jb = c + TPC * m;
+        const int k = jb % NS;
+        const int idxD = (jb / NS) * NS * R + k;
+#pragma unroll
+        for (int r = 0; r < R; ++r) store(idxD + r * NS, v[m * R + r]);
+      }
+    } else {
+      __syncthreads();
+#pragma unroll
+      for (int m = 0; m < NBT; ++m) {
+        const int jb = c + TPC * m;
+        const int k = jb % NS;
+        const int idxD = (jb / NS) * NS * R + k;
+#pragma unroll
+        for (int r = 0; r < R; ++r) s[(idxD + r * NS) * PITCH + t] = v[m * R + r];
+      }
+      __syncthreads();
+      fft_tile_rest<LOGN, TX, TPC, SIGN, P + 1, PITCH, STORE_SYNC>(s, tw, v, t, c, store);
+    }
+  }
+}
+
+
+// PITCH: shared-memory row pitch (>= TX).  LOAD_SYNC: barrier between the
+// pass-0 loads and the pass-0 shared-memory writes (loader reads s).
+// STORE_SYNC: barrier before the final stores (storer writes s).
+template <int LOGN, int TX, int TPC, int SIGN, int PITCH = TX, bool LOAD_SYNC = false, bool STORE_SYNC = false,
+          typename C, class Load, class Store>
+__device__ __forceinline__ void fft_tile(C* __restrict__ s, const C* __restrict__ tw, Load&& load, Store&& store) {
+  constexpr int N = 1 << LOGN;
+  constexpr int ET = N / TPC;
+  constexpr int NP = Sched<LOGN>::npass;
+  static_assert(ET % 8 == 0 || N < 8, "each thread must own whole radix-8 butterflies");
+  const int t = threadIdx.x % TX;
+  const int c = threadIdx.x / TX;
+  C v[ET > 0 ? ET : 1];
+
+  // ---- pass 0 (Ns = 1): inputs from the loader
+  {
+    constexpr int R = Sched<LOGN>::radix(0);
+    constexpr int NBT = ET / R;
+#pragma unroll
+    for (int m = 0; m < NBT; ++m) {
+      const int jb = c + TPC * m;
+#pragma unroll
+      for (int r = 0; r < R; ++r) v[m * R + r] = load(jb + r * (N / R));
+    }
+#pragma unroll
+    for (int m = 0; m < NBT; ++m) dftR<R, SIGN>(&v[m * R]);
+    if constexpr (LOAD_SYNC) __syncthreads();
+    if constexpr (NP == 1) {
+#pragma unroll
+      for (int m = 0; m < NBT; ++m) {
+        const int jb = c + TPC * m;
+#pragma unroll
+        for (int r = 0; r < R; ++r) store(jb * R + r, v[m * R + r]);
+      }
+      return;
+    } else {
+#pragma unroll
+      for (int m = 0; m < NBT; ++m) {
+        const int jb = c + TPC * m;
+#pragma unroll
+        for (int r = 0; r < R; ++r) s[(jb * R + r) * PITCH + t] = v[m * R + r];
+      }
+      __syncthreads();
+    }
+  }
+  // ---- passes 1 .. NP-1
+  fft_tile_rest<LOGN, TX, TPC, SIGN, 1, PITCH, STORE_SYNC>(s, tw, v, t, c, store);
+}
+
+}  // namespace ss3d

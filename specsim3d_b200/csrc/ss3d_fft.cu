@@ -23,9 +23,12 @@
 #include <algorithm>
 #include <cstdio>
 
+#include "ss3d_engine.cuh"
 #include "ss3d_internal.h"
 
 namespace ss3d {
+
+unsigned long long g_launch_count = 0;
 
 constexpr int NT = 256;  // threads per block of every FFT kernel
 
@@ -72,12 +75,27 @@ __device__ __forceinline__ bool line_valid(const Geo& g, int line, int lines) {
   return line < lines && (line % g.HP) < g.H;
 }
 
-// c2c transform along a strided axis; out may alias in (the whole line is read first)
+// ---------------------------------------------------------------- register-resident column passes
+// Tile configuration per transform length: TX columns, TPC threads per column,
+// ET = N / TPC elements per thread (16 in float, 8 in double).
+template <typename R, int LOGN> struct ColCfg {
+  static constexpr int N = 1 << LOGN;
+  static constexpr int ETW = sizeof(R) == 4 ? 16 : 8;
+  static constexpr int ET = N < ETW ? N : ETW;
+  static constexpr int TPC = N / ET;
+  static constexpr int E = sizeof(R) == 4 ? 8192 : 4096;
+  static constexpr int TX0 = E / N;
+  static constexpr int TX = TX0 > 64 ? 64 : (TX0 < 2 ? 2 : TX0);
+  static constexpr int NTH = TX * TPC;
+};
+
+// c2c transform along a strided axis (in place allowed), unscaled, pruned store
 template <typename R, int LOGN, int SIGN>
-__global__ void __launch_bounds__(NT) k_axis_c2c(AxisArgs a, Geo g, const cpx_t<R>* in, cpx_t<R>* out, Tw tw) {
+__global__ void __launch_bounds__(ColCfg<R, LOGN>::NTH) k_col(AxisArgs a, Geo g, const cpx_t<R>* in, cpx_t<R>* out,
+                                                             Tw tw) {
   using C = cpx_t<R>;
-  constexpr int N = 1 << LOGN;
-  constexpr int TX = AxisTX<R, LOGN>::TX;
+  using CF = ColCfg<R, LOGN>;
+  constexpr int N = CF::N, TX = CF::TX;
   extern __shared__ __align__(16) unsigned char smraw[];
   C* s = reinterpret_cast<C*>(smraw);
   C* stw = s + N * TX;
@@ -85,32 +103,32 @@ __global__ void __launch_bounds__(NT) k_axis_c2c(AxisArgs a, Geo g, const cpx_t<
   const int tile = blockIdx.x / a.nreal;
   const int grp = tile / a.tpg;
   const int line0 = (tile % a.tpg) * TX;
-  const long long base = (long long)grp * a.gstride + line0 + (long long)r * a.rstride;
-  load_tw(stw, twtab<R>(tw), N, N);
-  for (int q = threadIdx.x; q < N * TX; q += NT) {
-    int t = q % TX, p = q / TX;
-    C v = cmk<C>(R(0), R(0));
-    if (line_valid(g, line0 + t, a.lines)) v = in[base + t + p * a.S];
-    s[p * TX + t] = v;
-  }
+  const int t = threadIdx.x % TX;
+  const bool valid = line_valid(g, line0 + t, a.lines);
+  const C* src = in + ((long long)grp * a.gstride + line0 + t + (long long)r * a.rstride);
+  C* dst = out + ((long long)grp * a.gstride + line0 + t + (long long)r * a.rstride);
+  const long long S = a.S;
+  const int nout = a.nout;
+  for (int q = threadIdx.x; q < N; q += CF::NTH) stw[q] = twtab<R>(tw)[N - 1 + q];
   __syncthreads();
-  smem_fft<LOGN, TX, TX, NT, SIGN>(s, stw);
-  for (int q = threadIdx.x; q < a.nout * TX; q += NT) {
-    int t = q % TX, p = q / TX;
-    if (line_valid(g, line0 + t, a.lines)) out[base + t + p * a.S] = s[p * TX + t];
-  }
+  fft_tile<LOGN, TX, CF::TPC, SIGN>(
+      s, stw, [&](int pos) { return valid ? src[pos * S] : cmk<C>(R(0), R(0)); },
+      [&](int pos, C v) {
+        if (valid && pos < nout) dst[pos * S] = v;
+      });
 }
 
-// First inverse pass with the coefficient synthesis fused into the load: the
-// coefficients of realization r are generated from amp and the row states,
-// transformed along the axis, and only p < nout is stored.
+// First inverse pass with the coefficient synthesis fused into the loader.
+// axis 2: columns are (i, j) plane offsets, positions k;  axis 1 (npz = 1):
+// columns are i, positions j.
 template <typename R, int LOGN>
-__global__ void __launch_bounds__(NT) k_axis_gen(AxisArgs a, Geo g, const R* __restrict__ amp,
-                                                 const uint32_t* __restrict__ rowstates,
-                                                 const uint32_t* __restrict__ apow, cpx_t<R>* out, Tw tw) {
+__global__ void __launch_bounds__(ColCfg<R, LOGN>::NTH) k_colgen(AxisArgs a, Geo g, const R* __restrict__ amp,
+                                                                const uint32_t* __restrict__ rowstates,
+                                                                const uint32_t* __restrict__ apow, cpx_t<R>* out,
+                                                                Tw tw) {
   using C = cpx_t<R>;
-  constexpr int N = 1 << LOGN;
-  constexpr int TX = AxisTX<R, LOGN>::TX;
+  using CF = ColCfg<R, LOGN>;
+  constexpr int N = CF::N, TX = CF::TX;
   extern __shared__ __align__(16) unsigned char smraw[];
   C* s = reinterpret_cast<C*>(smraw);
   C* stw = s + N * TX;
@@ -118,36 +136,40 @@ __global__ void __launch_bounds__(NT) k_axis_gen(AxisArgs a, Geo g, const R* __r
   const int tile = blockIdx.x / a.nreal;
   const int grp = tile / a.tpg;
   const int line0 = (tile % a.tpg) * TX;
-  const long long abase = (long long)grp * a.gstride + line0;
+  const int t = threadIdx.x % TX;
+  const int line = line0 + t;
+  const bool valid = line_valid(g, line, a.lines);
+  int i, j0;
+  if (a.axis == 2) {
+    i = line % g.HP;
+    j0 = line / g.HP;
+  } else {
+    i = line;
+    j0 = 0;
+  }
+  if (!valid) i = 0;
+  const uint32_t ai = __ldg(apow + i), aip = __ldg(apow + ((g.npx - i) & (g.npx - 1)));
+  const bool iedge = (i == 0) || (2 * i == g.npx);
   const uint32_t* rs = rowstates + (size_t)r * g.npy * g.npz;
-  load_tw(stw, twtab<R>(tw), N, N);
-  for (int q = threadIdx.x; q < N * TX; q += NT) {
-    int t = q % TX, p = q / TX;
-    int line = line0 + t;
-    C v = cmk<C>(R(0), R(0));
-    if (line_valid(g, line, a.lines)) {
-      int i, j, k;
-      if (a.axis == 2) {
-        i = line % g.HP;
-        j = line / g.HP;
-        k = p;
-      } else {
-        i = line;
-        j = p;
-        k = grp;
-      }
-      R am = amp[abase + t + p * a.S];
-      v = coefficient<R>(g, i, j, k, am, rs, apow);
-    }
-    s[p * TX + t] = v;
-  }
+  const long long cbase = (long long)grp * a.gstride + line;
+  const R* ap = amp + cbase;
+  C* dst = out + cbase + (long long)r * a.rstride;
+  const long long S = a.S;
+  const int nout = a.nout;
+  const bool zaxis = a.axis == 2;
+  for (int q = threadIdx.x; q < N; q += CF::NTH) stw[q] = twtab<R>(tw)[N - 1 + q];
   __syncthreads();
-  smem_fft<LOGN, TX, TX, NT, +1>(s, stw);
-  const long long obase = abase + (long long)r * a.rstride;
-  for (int q = threadIdx.x; q < a.nout * TX; q += NT) {
-    int t = q % TX, p = q / TX;
-    if (line_valid(g, line0 + t, a.lines)) out[obase + t + p * a.S] = s[p * TX + t];
-  }
+  fft_tile<LOGN, TX, CF::TPC, +1>(
+      s, stw,
+      [&](int pos) {
+        if (!valid) return cmk<C>(R(0), R(0));
+        const R am = __ldg(ap + pos * S);
+        return zaxis ? coef_col<R>(g, j0, pos, am, rs, ai, aip, iedge)
+                     : coef_col<R>(g, pos, grp, am, rs, ai, aip, iedge);
+      },
+      [&](int pos, C v) {
+        if (valid && pos < nout) dst[pos * S] = v;
+      });
 }
 
 // Standalone synthesis of the full half spectrum of nreal realizations.
@@ -241,37 +263,76 @@ __device__ __forceinline__ void block_sum2(double& a, double& b) {
 // then x[2m] = Re z[m], x[2m+1] = Im z[m].  The imaginary parts of X[0] and
 // X[N] are dropped: the reference keeps the real part of the full complex
 // inverse (f90:1339), which does not see them.
-template <typename R, typename O, int LOGN>
-__global__ void __launch_bounds__(NT) k_rows_c2r(Geo g, const cpx_t<R>* __restrict__ in, long long rstride,
-                                                 O* __restrict__ out, long long ostride, int nreal, int nblk_per_r,
-                                                 double* __restrict__ part, Tw tw) {
+template <typename R, int LOGN> struct RowCfg {
+  using CF = ColCfg<R, LOGN>;
+  static constexpr int N = CF::N, TPC = CF::TPC, ET = CF::ET;
+  static constexpr int TX0 = CF::E / N;
+  static constexpr int TX = TX0 > 64 ? 64 : (TX0 < 1 ? 1 : TX0);
+  static constexpr int NTH0 = TX * TPC;
+  static constexpr int NTH = NTH0 < 32 ? 32 : NTH0;
+  static constexpr int PITCH = TX + 1;
+};
+
+// inverse length-N FFT of the TX rows staged in s (pitch TX+1), in place;
+// twN holds e^{-2 pi i m/N}, m < N
+template <typename R, int LOGN>
+__device__ __forceinline__ void fft_rows_inv(cpx_t<R>* s, const cpx_t<R>* twN) {
   using C = cpx_t<R>;
-  constexpr int N = 1 << LOGN;
-  constexpr int TX = RowTX<R, LOGN>::TX;
-  constexpr int PITCH = TX + 1;
+  using RC = RowCfg<R, LOGN>;
+  static_assert(RC::NTH0 >= 32, "row tile needs at least one warp");
+  if constexpr (LOGN > 0) {
+    const int t = threadIdx.x % RC::TX;
+    fft_tile<LOGN, RC::TX, RC::TPC, +1, RC::PITCH, true, true>(
+        s, twN, [&](int pos) { return s[pos * RC::PITCH + t]; }, [&](int pos, C v) { s[pos * RC::PITCH + t] = v; });
+    __syncthreads();
+  }
+}
+
+template <typename R, typename O, int LOGN>
+__global__ void __launch_bounds__(RowCfg<R, LOGN>::NTH) k_rows_c2r(Geo g, const cpx_t<R>* __restrict__ in,
+                                                                   long long rstride, O* __restrict__ out,
+                                                                   long long ostride, int nreal, int nblk_per_r,
+                                                                   double* __restrict__ part, Tw tw) {
+  using C = cpx_t<R>;
+  using RC = RowCfg<R, LOGN>;
+  constexpr int N = RC::N, TX = RC::TX, PITCH = RC::PITCH, NTH = RC::NTH;
+  constexpr int NW = NTH / 32;
   extern __shared__ __align__(16) unsigned char smraw[];
   C* s = reinterpret_cast<C*>(smraw);   // [N+1][PITCH]
   C* stw = s + (N + 1) * PITCH;         // 2N entries e^{-2 pi i m/(2N)}
+  C* stwN = stw + 2 * N;                // N entries e^{-2 pi i m/N}
   const int r = blockIdx.x % nreal;
   const int blk = blockIdx.x / nreal;
   const int nrows = g.ny * g.nz;
   const int row0 = blk * TX;
-  load_tw(stw, twtab<R>(tw), 2 * N, 2 * N);
+  const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
+  for (int q = threadIdx.x; q < 2 * N; q += NTH) stw[q] = twtab<R>(tw)[2 * N - 1 + q];
+  for (int q = threadIdx.x; q < N; q += NTH) stwN[q] = twtab<R>(tw)[N - 1 + q];
   const C* src = in + (long long)r * rstride;
-  for (int q = threadIdx.x; q < (N + 1) * TX; q += NT) {
-    int t = q / (N + 1), p = q % (N + 1);
-    int row = row0 + t;
-    C v = cmk<C>(R(0), R(0));
-    if (row < nrows) {
-      int j = row % g.ny, k = row / g.ny;
-      v = src[((long long)k * g.npy + j) * g.HP + p];
+  // stage rows: one warp per row, lanes along the row (coalesced)
+  for (int t = warp; t < TX; t += NW) {
+    const int row = row0 + t;
+    const bool ok = row < nrows;
+    const int j = ok ? row % g.ny : 0, k = ok ? row / g.ny : 0;
+    const C* rp = src + ((long long)k * g.npy + j) * g.HP;
+    constexpr int NIT = (N + 1 + 31) / 32;
+    C tmp[NIT];
+#pragma unroll
+    for (int it = 0; it < NIT; ++it) {
+      const int p = lane + 32 * it;
+      tmp[it] = (ok && p <= N) ? rp[p] : cmk<C>(R(0), R(0));
     }
-    s[p * PITCH + t] = v;
+#pragma unroll
+    for (int it = 0; it < NIT; ++it) {
+      const int p = lane + 32 * it;
+      if (p <= N) s[p * PITCH + t] = tmp[it];
+    }
   }
   __syncthreads();
-  for (int q = threadIdx.x; q < (N / 2 + 1) * TX; q += NT) {
-    int t = q % TX, k = q / TX;
-    int kc = N - k;
+  // packing Z[q] from X[q], X[N-q], in place over the pairs (q, N-q)
+  for (int q = threadIdx.x; q < (N / 2 + 1) * TX; q += NTH) {
+    const int t = q % TX, k = q / TX;
+    const int kc = N - k;
     C a = s[k * PITCH + t], b = s[kc * PITCH + t];
     if (k == 0) {
       a.y = R(0);
@@ -279,39 +340,52 @@ __global__ void __launch_bounds__(NT) k_rows_c2r(Geo g, const cpx_t<R>* __restri
     }
     C w = stw[k];
     w.y = -w.y;
-    C bc = cmk<C>(b.x, -b.y);
-    C zk = cadd(cadd(a, bc), cmul_si<+1>(cmul(w, csub(a, bc))));
+    const C bc = cmk<C>(b.x, -b.y);
+    const C zk = cadd(cadd(a, bc), cmul_si<+1>(cmul(w, csub(a, bc))));
     if (k != 0 && kc != k) {
       C w2 = stw[kc];
       w2.y = -w2.y;
-      C ac = cmk<C>(a.x, -a.y);
+      const C ac = cmk<C>(a.x, -a.y);
       s[kc * PITCH + t] = cadd(cadd(b, ac), cmul_si<+1>(cmul(w2, csub(b, ac))));
     }
     s[k * PITCH + t] = zk;
   }
   __syncthreads();
-  smem_fft<LOGN, TX, PITCH, NT, +1, 2>(s, stw);
+  fft_rows_inv<R, LOGN>(s, stwN);
+  // write x[0..nx) of each row: one warp per row, lanes along m; sums for the stats
   double s1 = 0.0, s2 = 0.0;
   O* dst = out + (long long)r * ostride;
   const int nxh = (g.nx + 1) / 2;
-  for (int q = threadIdx.x; q < nxh * TX; q += NT) {
-    int t = q / nxh, m = q % nxh;
-    int row = row0 + t;
-    if (row < nrows) {
-      C z = s[m * PITCH + t];
-      long long o = (long long)row * g.nx + 2 * m;
-      dst[o] = (O)z.x;
+  const bool even = (g.nx & 1) == 0;
+  for (int t = warp; t < TX; t += NW) {
+    const int row = row0 + t;
+    if (row >= nrows) break;
+    O* rp = dst + (long long)row * g.nx;
+    for (int m = lane; m < nxh; m += 32) {
+      const C z = s[m * PITCH + t];
+      const O a0 = (O)z.x, a1 = (O)z.y;
       s1 += (double)z.x;
       s2 += (double)z.x * (double)z.x;
-      if (2 * m + 1 < g.nx) {
-        dst[o + 1] = (O)z.y;
+      if (even) {
+        if constexpr (sizeof(O) == 4) {
+          reinterpret_cast<float2*>(rp)[m] = make_float2((float)a0, (float)a1);
+        } else {
+          reinterpret_cast<double2*>(rp)[m] = make_double2((double)a0, (double)a1);
+        }
         s1 += (double)z.y;
         s2 += (double)z.y * (double)z.y;
+      } else {
+        rp[2 * m] = a0;
+        if (2 * m + 1 < g.nx) {
+          rp[2 * m + 1] = a1;
+          s1 += (double)z.y;
+          s2 += (double)z.y * (double)z.y;
+        }
       }
     }
   }
   if (part) {
-    block_sum2<NT>(s1, s2);
+    block_sum2<NTH>(s1, s2);
     if (threadIdx.x == 0) {
       part[2 * ((long long)r * nblk_per_r + blk)] = s1;
       part[2 * ((long long)r * nblk_per_r + blk) + 1] = s2;
@@ -541,43 +615,56 @@ template <> struct MaxL<double> { static constexpr int v = MAX_LOGN_D; };
 template <typename R, int L, int SIGN>
 static cudaError_t run_axis_c2c(const AxisArgs& a, const Geo& g, const cpx_t<R>* in, cpx_t<R>* out, Tw tw,
                                 cudaStream_t st) {
-  constexpr int TX = AxisTX<R, L>::TX;
-  size_t smem = (size_t)((1 << L) * TX + (1 << L)) * sizeof(cpx_t<R>);
-  cudaError_t e = set_smem(k_axis_c2c<R, L, SIGN>, smem);
-  if (e != cudaSuccess) return e;
-  AxisArgs b = a;
-  b.tpg = (a.lines + TX - 1) / TX;
-  unsigned blocks = (unsigned)((long long)b.tpg * a.ngroups * a.nreal);
-  k_axis_c2c<R, L, SIGN><<<blocks, NT, smem, st>>>(b, g, in, out, tw);
-  return cudaGetLastError();
+  using CF = ColCfg<R, L>;
+  if constexpr (L == 0) {
+    // length-1 transform: identity; copy when out-of-place
+    if (in != out) return cudaErrorInvalidValue;
+    return cudaSuccess;
+  } else {
+    size_t smem = (size_t)(CF::N * CF::TX + CF::N) * sizeof(cpx_t<R>);
+    cudaError_t e = set_smem(k_col<R, L, SIGN>, smem);
+    if (e != cudaSuccess) return e;
+    AxisArgs b = a;
+    b.tpg = (a.lines + CF::TX - 1) / CF::TX;
+    unsigned blocks = (unsigned)((long long)b.tpg * a.ngroups * a.nreal);
+    k_col<R, L, SIGN><<<blocks, CF::NTH, smem, st>>>(b, g, in, out, tw);
+    ++g_launch_count;
+    return cudaGetLastError();
+  }
 }
 
 template <typename R, int L>
 static cudaError_t run_axis_gen(const AxisArgs& a, const Geo& g, const R* amp, const uint32_t* rs,
                                 const uint32_t* apow, cpx_t<R>* out, Tw tw, cudaStream_t st) {
-  constexpr int TX = AxisTX<R, L>::TX;
-  size_t smem = (size_t)((1 << L) * TX + (1 << L)) * sizeof(cpx_t<R>);
-  cudaError_t e = set_smem(k_axis_gen<R, L>, smem);
-  if (e != cudaSuccess) return e;
-  AxisArgs b = a;
-  b.tpg = (a.lines + TX - 1) / TX;
-  unsigned blocks = (unsigned)((long long)b.tpg * a.ngroups * a.nreal);
-  k_axis_gen<R, L><<<blocks, NT, smem, st>>>(b, g, amp, rs, apow, out, tw);
-  return cudaGetLastError();
+  using CF = ColCfg<R, L>;
+  if constexpr (L == 0) {
+    return cudaErrorInvalidValue;
+  } else {
+    size_t smem = (size_t)(CF::N * CF::TX + CF::N) * sizeof(cpx_t<R>);
+    cudaError_t e = set_smem(k_colgen<R, L>, smem);
+    if (e != cudaSuccess) return e;
+    AxisArgs b = a;
+    b.tpg = (a.lines + CF::TX - 1) / CF::TX;
+    unsigned blocks = (unsigned)((long long)b.tpg * a.ngroups * a.nreal);
+    k_colgen<R, L><<<blocks, CF::NTH, smem, st>>>(b, g, amp, rs, apow, out, tw);
+    ++g_launch_count;
+    return cudaGetLastError();
+  }
 }
 
 template <typename R, typename O, int L>
 static cudaError_t run_rows_c2r(const Geo& g, const cpx_t<R>* in, long long rstride, O* out, long long ostride,
                                 int nreal, double* part, int* nblk_out, Tw tw, cudaStream_t st) {
-  constexpr int TX = RowTX<R, L>::TX;
-  constexpr int N = 1 << L;
-  size_t smem = (size_t)((N + 1) * (TX + 1) + 2 * N) * sizeof(cpx_t<R>);
+  using RC = RowCfg<R, L>;
+  constexpr int N = RC::N;
+  size_t smem = (size_t)((N + 1) * RC::PITCH + 3 * N) * sizeof(cpx_t<R>);
   cudaError_t e = set_smem(k_rows_c2r<R, O, L>, smem);
   if (e != cudaSuccess) return e;
-  int nblk = (g.ny * g.nz + TX - 1) / TX;
+  int nblk = (g.ny * g.nz + RC::TX - 1) / RC::TX;
   if (nblk_out) *nblk_out = nblk;
-  k_rows_c2r<R, O, L><<<(unsigned)((long long)nblk * nreal), NT, smem, st>>>(g, in, rstride, out, ostride, nreal,
-                                                                            nblk, part, tw);
+  k_rows_c2r<R, O, L><<<(unsigned)((long long)nblk * nreal), RC::NTH, smem, st>>>(g, in, rstride, out, ostride,
+                                                                                  nreal, nblk, part, tw);
+  ++g_launch_count;
   return cudaGetLastError();
 }
 
@@ -591,6 +678,7 @@ static cudaError_t run_spec_rows(const Model& m, const double d[3], const Geo& g
   if (e != cudaSuccess) return e;
   int nblk = (g.npy * g.npz + TX - 1) / TX;
   k_spec_rows<L><<<nblk, NT, smem, st>>>(m, d[0], d[1], d[2], g, out, tw);
+  ++g_launch_count;
   return cudaGetLastError();
 }
 
@@ -598,7 +686,7 @@ static cudaError_t run_spec_rows(const Model& m, const double d[3], const Geo& g
 int realize_part_blocks(const Geo& g, bool dbl) {
   if (g.npx == 1) return (g.ny * g.nz + NT - 1) / NT;
   int L = ilog2(g.npx) - 1;
-  int E = dbl ? TileE<double>::E : TileE<float>::E;
+  int E = dbl ? 4096 : 8192;
   int tx = std::min(64, std::max(1, E >> L));
   return (g.ny * g.nz + tx - 1) / tx;
 }
@@ -611,6 +699,7 @@ cudaError_t launch_spectrum(const Model& m, const double d[3], const Geo& g, dou
   if (g.npx == 1) {
     int nrows = g.npy * g.npz;
     k_spec_rows_n1<<<(nrows + NT - 1) / NT, NT, 0, st>>>(m, d[0], d[1], d[2], g, work);
+    ++g_launch_count;
     e = cudaGetLastError();
   } else {
     int L = ilog2(g.npx) - 1;
@@ -651,8 +740,10 @@ cudaError_t launch_spectrum(const Model& m, const double d[3], const Geo& g, dou
   long long tot = (long long)g.npz * g.npy * g.HP;
   int nb = (int)std::min<long long>(npart_max, (tot + NT - 1) / NT);
   k_spec_amp<<<nb, NT, 0, st>>>(g, work, amp64, amp32, part);
+  ++g_launch_count;
   if ((e = cudaGetLastError()) != cudaSuccess) return e;
   k_reduce_spec<<<1, 32, 0, st>>>(part, nb, result);
+  ++g_launch_count;
   return cudaGetLastError();
 }
 
@@ -661,9 +752,11 @@ cudaError_t launch_rowstates(const Geo& g, uint32_t s0, long long r_first, int n
   long long tot = (long long)g.npy * g.npz * nreal;
   int nb = (int)std::min<long long>(4096, (tot + NT - 1) / NT);
   k_rowstates<<<nb, NT, 0, st>>>(g, s0, r_first, nreal, ptab, rowstates);
+  ++g_launch_count;
   cudaError_t e = cudaGetLastError();
   if (e != cudaSuccess || apow == nullptr) return e;
   k_apow<<<(g.npx + NT - 1) / NT, NT, 0, st>>>(g.npx, g.d, ptab, apow);
+  ++g_launch_count;
   return cudaGetLastError();
 }
 
@@ -673,15 +766,17 @@ cudaError_t launch_gen(const Geo& g, const R* amp, const uint32_t* rowstates, co
   long long tot = (long long)g.npz * g.npy * g.HP * nreal;
   int nb = (int)std::min<long long>(148 * 16, (tot + NT - 1) / NT);
   k_gen<R><<<nb, NT, 0, st>>>(g, amp, rowstates, apow, work, wstride, nreal);
+  ++g_launch_count;
   return cudaGetLastError();
 }
 
 template <typename R>
 cudaError_t launch_realize(const Geo& g, const R* amp, const uint32_t* rowstates, const uint32_t* apow,
                            cpx_t<R>* work, long long wstride, int nreal, void* out, int out_kind, double* part,
-                           int* nblk_per_r, Tw tw, bool fused, cudaStream_t st) {
+                           int* nblk_per_r, Tw tw, bool fused, cudaStream_t st, Marks* marks) {
   constexpr int ML = MaxL<R>::v;
   cudaError_t e = cudaSuccess;
+  mark(marks, 1, st);
   // first inverse axis: z if present, else y, else only x
   if (g.npz > 1) {
     AxisArgs a{};
@@ -705,6 +800,7 @@ cudaError_t launch_realize(const Geo& g, const R* amp, const uint32_t* rowstates
     }
     if (e != cudaSuccess) return e;
     if (g.npy > 1) {
+      mark(marks, 2, st);
       AxisArgs b{};
       b.S = g.HP;
       b.nout = g.ny;
@@ -745,6 +841,7 @@ cudaError_t launch_realize(const Geo& g, const R* amp, const uint32_t* rowstates
     if (e != cudaSuccess) return e;
   }
   // x pass
+  mark(marks, 3, st);
   const long long ostride = (long long)g.nx * g.ny * g.nz;
   if (g.npx == 1) {
     int nblk = (g.ny * g.nz + NT - 1) / NT;
@@ -754,6 +851,7 @@ cudaError_t launch_realize(const Geo& g, const R* amp, const uint32_t* rowstates
     else
       k_rows_copy<R, double><<<nblk * nreal, NT, 0, st>>>(g, work, wstride, (double*)out, ostride, nreal, nblk,
                                                           part);
+    ++g_launch_count;
     return cudaGetLastError();
   }
   int Lx = ilog2(g.npx) - 1;
@@ -775,18 +873,22 @@ cudaError_t launch_debug_states(const Geo& g, const uint32_t* rowstates, const u
   long long tot = (long long)g.npz * g.npy * g.H;
   int nb = (int)std::min<long long>(4096, (tot + NT - 1) / NT);
   k_debug_states<<<nb, NT, 0, st>>>(g, rowstates, apow, out);
+  ++g_launch_count;
   return cudaGetLastError();
 }
 
 cudaError_t launch_reduce_zstats(const double* part, int nblk_per_r, int nreal, double* zsum, cudaStream_t st) {
   k_reduce_zstats<<<nreal, NT, 0, st>>>(part, nblk_per_r, zsum);
+  ++g_launch_count;
   return cudaGetLastError();
 }
 
 template cudaError_t launch_realize<float>(const Geo&, const float*, const uint32_t*, const uint32_t*, float2*,
-                                           long long, int, void*, int, double*, int*, Tw, bool, cudaStream_t);
+                                           long long, int, void*, int, double*, int*, Tw, bool, cudaStream_t,
+                                           Marks*);
 template cudaError_t launch_realize<double>(const Geo&, const double*, const uint32_t*, const uint32_t*, double2*,
-                                            long long, int, void*, int, double*, int*, Tw, bool, cudaStream_t);
+                                            long long, int, void*, int, double*, int*, Tw, bool, cudaStream_t,
+                                            Marks*);
 template cudaError_t launch_gen<float>(const Geo&, const float*, const uint32_t*, const uint32_t*, float2*,
                                        long long, int, cudaStream_t);
 template cudaError_t launch_gen<double>(const Geo&, const double*, const uint32_t*, const uint32_t*, double2*,

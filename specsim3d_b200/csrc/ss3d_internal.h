@@ -59,6 +59,16 @@ struct SpecPartial {
   double maximag, maxreal, spos, sneg;
 };
 
+// Stage markers of one realize call (CUDA events recorded between stages)
+struct Marks {
+  bool on = false;
+  int n = 0;
+  int stage[16];
+  cudaEvent_t ev[16];
+};
+void mark(Marks* m, int stage, cudaStream_t st);   // records an event opening `stage`
+extern unsigned long long g_launch_count;          // kernels launched by the library
+
 // ---- launchers (ss3d_fft.cu); all return cudaError_t of the last launch
 cudaError_t launch_spectrum(const Model& m, const double d[3], const Geo& g, double2* work, double* amp64,
                             float* amp32, SpecPartial* part, int npart_max, SpecPartial* result, Tw tw,
@@ -69,7 +79,8 @@ cudaError_t launch_rowstates(const Geo& g, uint32_t s0, long long r_first, int n
 template <typename R>
 cudaError_t launch_realize(const Geo& g, const R* amp, const uint32_t* rowstates, const uint32_t* apow,
                            cpx_t<R>* work, long long wstride, int nreal, void* out, int out_kind,
-                           double* part, int* nblk_per_r, Tw tw, bool fused, cudaStream_t st);
+                           double* part, int* nblk_per_r, Tw tw, bool fused, cudaStream_t st,
+                           Marks* marks = nullptr);
 template <typename R>
 cudaError_t launch_gen(const Geo& g, const R* amp, const uint32_t* rowstates, const uint32_t* apow,
                        cpx_t<R>* work, long long wstride, int nreal, cudaStream_t st);
