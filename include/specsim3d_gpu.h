@@ -120,6 +120,24 @@ int ss3d_realize(const ss3d_spectrum *sp, int iseed, int64_t r_first, int nreal,
 int ss3d_debug_states(const ss3d_spectrum *sp, int iseed, int64_t r, int igauss, uint32_t *states);
 int ss3d_debug_coefficients(const ss3d_spectrum *sp, int iseed, int64_t r, int igauss, int precision, double *coef);
 
+/* Realizations like ss3d_realize, but without allocating device memory.  No
+ * counterpart in the reference (the Fortran program allocates its own arrays).
+ * For callers that cannot call cudaMalloc when they need realizations: an
+ * application that has handed the GPU's memory to its own pool (a serving
+ * process that reserves HBM up front), or a latency-bound loop that cannot
+ * afford the device-wide synchronisation of cudaMalloc/cudaFree.  All scratch
+ * lives in one fixed array of SS3D_NOALLOC_SCRATCH_BYTES that every GPU loading
+ * the library holds until exit.  A call needs about nz * npy * (npx/2 + 2) * 8
+ * bytes (FP32; 16 for FP64; nz is replaced by 1 when npz = 1) plus 0.5 MB of
+ * tables: a 128^3 grid on its 256^3 periodic grid fits, the 256^3 grid on 512^3
+ * does not.  Larger grids are rejected with SS3D_ETOOLARGE and a message giving
+ * the bytes needed.  out must be device memory.  The first call on a device copies the
+ * constant tables into the array: make it before any stream capture.  Every call
+ * shares and overwrites the one array, so calls that overlap on the GPU race. */
+#define SS3D_NOALLOC_SCRATCH_BYTES (64u << 20)
+int ss3d_realize_noalloc(const ss3d_spectrum *sp, int iseed, int64_t r_first, int nreal, int igauss, int precision,
+                         void *out, int out_dtype);
+
 /* ---------------------------------------------------------------- variogram */
 
 /* Experimental semivariograms of nreal fields res(nx,ny,nz,nreal) (FP64, host or

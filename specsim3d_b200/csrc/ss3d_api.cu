@@ -643,3 +643,14 @@ extern "C" int ss3d_debug_coefficients(const ss3d_spectrum* sp, int iseed, int64
     }
   return SS3D_OK;
 }
+
+// ---------------------------------------------------------------- helpers of the allocation-free entry point
+int ss3d::set_error(int code, const char* msg) { return fail(code, "%s", msg); }
+cudaStream_t ss3d::current_stream() { return g_stream; }
+int ss3d::spectrum_view(const ss3d_spectrum* sp, NoallocView* v) {
+  if (!sp || !sp->amp32 || !sp->amp64) return 1;
+  v->geo = sp->geo;
+  v->amp64 = sp->amp64;
+  v->amp32 = sp->amp32;
+  return 0;
+}

@@ -87,4 +87,18 @@ cudaError_t launch_gen(const Geo& g, const R* amp, const uint32_t* rowstates, co
 cudaError_t launch_reduce_zstats(const double* part, int nblk_per_r, int nreal, double* zsum, cudaStream_t st);
 int realize_part_blocks(const Geo& g, bool dbl);
 
+// ---- helpers of the allocation-free entry point (ss3d_api.cu)
+struct NoallocView {
+  Geo geo;
+  const double* amp64;
+  const float* amp32;
+};
+int set_error(int code, const char* msg);     // sets the message returned by ss3d_last_error
+cudaStream_t current_stream();                // stream selected with ss3d_set_stream
+
+}  // namespace ss3d
+
+struct ss3d_spectrum;
+namespace ss3d {
+int spectrum_view(const ss3d_spectrum* sp, NoallocView* v);
 }  // namespace ss3d
