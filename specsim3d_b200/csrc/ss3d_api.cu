@@ -654,3 +654,7 @@ int ss3d::spectrum_view(const ss3d_spectrum* sp, NoallocView* v) {
   v->amp32 = sp->amp32;
   return 0;
 }
+
+// model helpers shared with the conditioning module
+void ss3d::setrot_public(const ss3d_struct& s, double rot[3][3], double axes[3][3]) { setrot_rc(s, rot, axes); }
+void ss3d::model_public(const ss3d_struct* st, int nst, double nugget, Model& m) { build_model(st, nst, nugget, m); }

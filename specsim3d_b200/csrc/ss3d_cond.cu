@@ -1,0 +1,718 @@
+// ss3d_cond.cu -- conditioning by kriging of the residual
+// (reference: condition_field f90:700-1081, nscore/backtr/gauinv f90:557-697).
+//
+//   z_c(x) = z*_SK(x; data) + [ z_s(x) - z*_SK(x; z_s at the data nodes) ]
+//
+// Host (small, serial in the reference too): data snapping and trimming,
+// merging of data that share a node (heapsort order, weighted mean), normal
+// scores, super-block tables.  GPU: the neighbour search of every node
+// (thread per node), the simple-kriging solve of every node (warp per node,
+// matrix in shared memory), the back transform (thread per cell).
+//
+// The search reproduces the reference's neighbour set exactly: squared scaled
+// distances are formed with round-to-nearest intrinsics in the reference's
+// expression order (no FMA contraction), blocks are visited in the same
+// kb, jb, ib order, data inside a block in index order, and the list keeps
+// the ndmax smallest with the same insertion rules (strict < to replace the
+// last entry when full, insertion after equal distances).
+#include <cuda_runtime.h>
+
+#include <algorithm>
+#include <cmath>
+#include <cstdint>
+#include <cstdio>
+#include <cstring>
+#include <string>
+#include <vector>
+
+#include "../../include/specsim3d_gpu.h"
+#include "ss3d_internal.h"
+
+namespace ss3d {
+
+// shared memory of one kriging warp: A and L (ndmax^2 doubles each), four
+// ndmax vectors of doubles and the neighbour ids, rounded up to 16 bytes
+__host__ __device__ inline size_t cond_warp_bytes(int ndmax) {
+  const size_t b = (size_t)ndmax * ndmax * 16 + (size_t)ndmax * 32 + (size_t)ndmax * 4;
+  return (b + 15) & ~(size_t)15;
+}
+
+struct CondGeo {
+  int nx, ny, nz, nreal, nd, ndmax;
+  double xmin, ymin, zmin, dx, dy, dz;
+  int nsbx, nsby, nsbz, mbx, mby, mbz;
+  double bsx, bsy, bsz;
+  double rot[9];       // search ellipsoid rotation (setrot of the search "structure")
+  double rmax2;        // rmax * rmax
+  double c0;           // C(0)
+};
+
+__device__ __forceinline__ int clampi(int v, int lo, int hi) { return v < lo ? lo : (v > hi ? hi : v); }
+
+// neighbour search of nodes [node0, node0 + count): writes nn and the
+// neighbour ids (0-based data index) and flags the exact data nodes
+__global__ void k_cond_search(CondGeo G, long long node0, int count, const double* __restrict__ dxs,
+                              const double* __restrict__ dys, const double* __restrict__ dzs,
+                              const int* __restrict__ sbstart, const int* __restrict__ sbidx,
+                              const int* __restrict__ ix, const int* __restrict__ iy, const int* __restrict__ iz,
+                              int* __restrict__ nbr, int* __restrict__ nnb) {
+  const int q = blockIdx.x * blockDim.x + threadIdx.x;
+  if (q >= count) return;
+  const long long node = node0 + q;
+  const int i = (int)(node % G.nx) + 1;
+  const int j = (int)((node / G.nx) % G.ny) + 1;
+  const int k = (int)(node / ((long long)G.nx * G.ny)) + 1;
+  const double x = __dadd_rn(G.xmin, __dmul_rn((double)(i - 1), G.dx));
+  const double y = __dadd_rn(G.ymin, __dmul_rn((double)(j - 1), G.dy));
+  const double z = __dadd_rn(G.zmin, __dmul_rn((double)(k - 1), G.dz));
+  const int bx = clampi((int)__ddiv_rn(__dadd_rn(__dsub_rn(x, G.xmin), __dmul_rn(0.5, G.dx)), G.bsx) + 1, 1, G.nsbx);
+  const int by = clampi((int)__ddiv_rn(__dadd_rn(__dsub_rn(y, G.ymin), __dmul_rn(0.5, G.dy)), G.bsy) + 1, 1, G.nsby);
+  const int bz = clampi((int)__ddiv_rn(__dadd_rn(__dsub_rn(z, G.zmin), __dmul_rn(0.5, G.dz)), G.bsz) + 1, 1, G.nsbz);
+  double cd[100];
+  int cid[100];
+  int nn = 0;
+  const int ndmax = G.ndmax;
+  for (int kb = max(1, bz - G.mbz); kb <= min(G.nsbz, bz + G.mbz); ++kb)
+    for (int jb = max(1, by - G.mby); jb <= min(G.nsby, by + G.mby); ++jb)
+      for (int ib = max(1, bx - G.mbx); ib <= min(G.nsbx, bx + G.mbx); ++ib) {
+        const int blk = ib + G.nsbx * (jb - 1 + G.nsby * (kb - 1));
+        const int p1 = __ldg(sbstart + blk) - 1;
+        for (int p = __ldg(sbstart + blk - 1); p <= p1; ++p) {
+          const int d = __ldg(sbidx + p - 1) - 1;
+          const double hx = __dsub_rn(__ldg(dxs + d), x), hy = __dsub_rn(__ldg(dys + d), y),
+                       hz = __dsub_rn(__ldg(dzs + d), z);
+          const double rx = __dadd_rn(__dadd_rn(__dmul_rn(G.rot[0], hx), __dmul_rn(G.rot[1], hy)), __dmul_rn(G.rot[2], hz));
+          const double ry = __dadd_rn(__dadd_rn(__dmul_rn(G.rot[3], hx), __dmul_rn(G.rot[4], hy)), __dmul_rn(G.rot[5], hz));
+          const double rz = __dadd_rn(__dadd_rn(__dmul_rn(G.rot[6], hx), __dmul_rn(G.rot[7], hy)), __dmul_rn(G.rot[8], hz));
+          const double d2 = __ddiv_rn(__dadd_rn(__dadd_rn(__dmul_rn(rx, rx), __dmul_rn(ry, ry)), __dmul_rn(rz, rz)), G.rmax2);
+          if (d2 > 1.0) continue;
+          int m;
+          if (nn < ndmax) {
+            nn = nn + 1;
+            m = nn;
+          } else if (d2 < cd[nn - 1]) {
+            m = nn;
+          } else {
+            continue;
+          }
+          while (m > 1) {
+            if (cd[m - 2] <= d2) break;
+            cd[m - 1] = cd[m - 2];
+            cid[m - 1] = cid[m - 2];
+            m = m - 1;
+          }
+          cd[m - 1] = d2;
+          cid[m - 1] = d;
+        }
+      }
+  int* out = nbr + (long long)q * ndmax;
+  for (int m = 0; m < nn; ++m) out[m] = cid[m];
+  // exact data node: nearest at distance 0 and on this very node
+  int flag = 0;
+  if (nn > 0 && cd[0] == 0.0) {
+    const int d = cid[0];
+    if (__ldg(ix + d) == i && __ldg(iy + d) == j && __ldg(iz + d) == k) flag = 1;
+  }
+  nnb[q] = nn | (flag << 16);
+}
+
+// Cholesky factor of A + ridge I (lower, in place in L = A copy), solve L L^T w = b.
+// Warp-cooperative, right-looking.  Returns false on a non-positive pivot.
+template <typename T>
+__device__ bool warp_chol_solve(T* L, const T* A, int ld, int n, T ridge, T* w, const T* b, int lane) {
+  for (int q = lane; q < n * ld; q += 32) L[q] = A[q];
+  __syncwarp();
+  if (lane == 0)
+    for (int p = 0; p < n; ++p) L[p * ld + p] += ridge;
+  __syncwarp();
+  bool ok = true;
+  for (int c = 0; c < n; ++c) {
+    const T piv = L[c * ld + c];
+    if (!(piv > T(0))) {
+      ok = false;
+      break;
+    }
+    const T dgl = sqrt(piv);
+    __syncwarp();
+    for (int r = c + 1 + lane; r < n; r += 32) L[r * ld + c] = L[r * ld + c] / dgl;
+    if (lane == 0) L[c * ld + c] = dgl;
+    __syncwarp();
+    for (int r = c + 1 + lane; r < n; r += 32) {
+      const T lrc = L[r * ld + c];
+      for (int cc = c + 1; cc <= r; ++cc) L[r * ld + cc] -= lrc * L[cc * ld + c];
+    }
+    __syncwarp();
+  }
+  ok = __shfl_sync(0xffffffffu, ok ? 1 : 0, 0) != 0;
+  if (!ok) return false;
+  if (lane == 0) {
+    for (int p = 0; p < n; ++p) {
+      T s = b[p];
+      for (int m = 0; m < p; ++m) s -= L[p * ld + m] * w[m];
+      w[p] = s / L[p * ld + p];
+    }
+    for (int p = n - 1; p >= 0; --p) {
+      T s = w[p];
+      for (int m = p + 1; m < n; ++m) s -= L[m * ld + p] * w[m];
+      w[p] = s / L[p * ld + p];
+    }
+  }
+  __syncwarp();
+  return true;
+}
+
+// triangular solves with an existing factor (lane 0)
+template <typename T>
+__device__ void chol_resolve(const T* L, int ld, int n, T* w, const T* b) {
+  for (int p = 0; p < n; ++p) {
+    T s = b[p];
+    for (int m = 0; m < p; ++m) s -= L[p * ld + m] * w[m];
+    w[p] = s / L[p * ld + p];
+  }
+  for (int p = n - 1; p >= 0; --p) {
+    T s = w[p];
+    for (int m = p + 1; m < n; ++m) s -= L[m * ld + p] * w[m];
+    w[p] = s / L[p * ld + p];
+  }
+}
+
+// kriging of the residual at nodes [node0, node0+count): warp per node.
+// precision 0: FP64 factor and solve; 1: FP32 factor and solve plus one
+// refinement step with the residual b - A w formed in FP64.
+template <int PREC>
+__global__ void k_cond_krige(CondGeo G, Model mdl, long long node0, int count, const int* __restrict__ nbr,
+                             const int* __restrict__ nnb, const double* __restrict__ dxs,
+                             const double* __restrict__ dys, const double* __restrict__ dzs,
+                             const double* __restrict__ dg, const double* __restrict__ simd, double* __restrict__ res,
+                             unsigned long long* __restrict__ counters) {
+  extern __shared__ __align__(16) unsigned char smc[];
+  const int lane = threadIdx.x & 31, wib = threadIdx.x >> 5;
+  const int nwb = blockDim.x >> 5;
+  const int ndmax = G.ndmax;
+  const int ld = ndmax;
+  // per warp: A (double), L (double or float), b, w (double), bf, wf (float), id (int)
+  const size_t per = cond_warp_bytes(ndmax);
+  unsigned char* mine = smc + per * wib;
+  double* A = (double*)mine;
+  double* Ld = A + ndmax * ndmax;
+  double* b = Ld + ndmax * ndmax;
+  double* w = b + ndmax;
+  double* r = w + ndmax;
+  double* tmp = r + ndmax;
+  int* id = (int*)(tmp + ndmax);
+  float* Lf = (float*)Ld;
+  float* bf = (float*)r;
+  float* wf = (float*)tmp;
+  const long long M = (long long)G.nx * G.ny * G.nz;
+  for (int q = blockIdx.x * nwb + wib; q < count; q += gridDim.x * nwb) {
+    const long long node = node0 + q;
+    const int code = nnb[q];
+    const int nn = code & 0xffff, exact = code >> 16;
+    if (lane == 0) atomicAdd(&counters[0], (unsigned long long)nn);
+    if (nn == 0) {
+      if (lane == 0) atomicAdd(&counters[2], 1ull);
+      continue;
+    }
+    const int* nl = nbr + (long long)q * ndmax;
+    if (exact) {
+      const double v = dg[nl[0]];
+      for (int l = lane; l < G.nreal; l += 32) res[node + M * l] = v;
+      if (lane == 0) atomicAdd(&counters[3], 1ull);
+      continue;
+    }
+    const int i = (int)(node % G.nx), j = (int)((node / G.nx) % G.ny), k = (int)(node / ((long long)G.nx * G.ny));
+    const double x = G.xmin + (double)i * G.dx, y = G.ymin + (double)j * G.dy, z = G.zmin + (double)k * G.dz;
+    for (int p = lane; p < nn; p += 32) id[p] = nl[p];
+    __syncwarp();
+    for (int e = lane; e < nn * nn; e += 32) {
+      const int p = e / nn, qq = e % nn;
+      if (qq <= p) {
+        const int cp = id[p], cq = id[qq];
+        const double v = covariance(mdl, dxs[cp] - dxs[cq], dys[cp] - dys[cq], dzs[cp] - dzs[cq]);
+        A[p * ld + qq] = v;
+        A[qq * ld + p] = v;
+      }
+    }
+    for (int p = lane; p < nn; p += 32) {
+      const int cp = id[p];
+      b[p] = covariance(mdl, dxs[cp] - x, dys[cp] - y, dzs[cp] - z);
+    }
+    __syncwarp();
+    double ridge = 1.0e-10 * G.c0;
+    bool ok = false;
+    int tries = 0;
+    for (tries = 1; tries <= 3; ++tries) {
+      if (PREC == 0) {
+        ok = warp_chol_solve<double>(Ld, A, ld, nn, ridge, w, b, lane);
+      } else {
+        // FP32 copies of A and b; the factor is built in place in Lf
+        for (int p = lane; p < nn; p += 32) bf[p] = (float)b[p];
+        for (int e = lane; e < nn * ld; e += 32) Lf[e] = (float)A[e];
+        __syncwarp();
+        ok = warp_chol_solve<float>(Lf, Lf, ld, nn, (float)ridge, wf, bf, lane);
+        if (ok) {
+          // one refinement: r = b - (A + ridge I) w in FP64, solve L L^T d = r in FP32, w += d
+          if (lane == 0) {
+            for (int p = 0; p < nn; ++p) w[p] = (double)wf[p];
+          }
+          __syncwarp();
+          for (int p = lane; p < nn; p += 32) {
+            double s = b[p] - ridge * w[p];
+            for (int m = 0; m < nn; ++m) s -= A[p * ld + m] * w[m];
+            r[p] = s;
+          }
+          __syncwarp();
+          if (lane == 0) {
+            float dtmp[100], rtmp[100];
+            for (int p = 0; p < nn; ++p) rtmp[p] = (float)r[p];
+            chol_resolve<float>(Lf, ld, nn, dtmp, rtmp);
+            for (int p = 0; p < nn; ++p) w[p] += (double)dtmp[p];
+          }
+          __syncwarp();
+        }
+      }
+      if (ok) break;
+      ridge = ridge * 1.0e3;
+    }
+    if (!ok) {
+      if (lane == 0) atomicAdd(&counters[1], 1ull);
+      continue;
+    }
+    if (tries > 1 && lane == 0) atomicAdd(&counters[1], 1ull);
+    double zk = 0.0;
+    for (int p = 0; p < nn; ++p) zk += w[p] * dg[id[p]];
+    for (int l = lane; l < G.nreal; l += 32) {
+      double sks = 0.0;
+      for (int p = 0; p < nn; ++p) sks += w[p] * simd[id[p] + (long long)G.nd * l];
+      res[node + M * l] = zk + res[node + M * l] - sks;
+    }
+    __syncwarp();
+  }
+}
+
+__global__ void k_gather_simd(const double* __restrict__ res, long long M, const int* __restrict__ ix,
+                              const int* __restrict__ iy, const int* __restrict__ iz, int nd, int nreal, int nx, int ny,
+                              double* __restrict__ simd) {
+  const long long tot = (long long)nd * nreal;
+  for (long long q = blockIdx.x * (long long)blockDim.x + threadIdx.x; q < tot; q += (long long)gridDim.x * blockDim.x) {
+    const int d = (int)(q % nd), l = (int)(q / nd);
+    simd[q] = res[(ix[d] - 1) + (long long)nx * ((iy[d] - 1) + (long long)ny * (iz[d] - 1)) + M * l];
+  }
+}
+
+// GSLIB back transform (backtr, powint, gcum), f90:628-697
+__device__ __forceinline__ double powint_d(double xlow, double xhigh, double ylow, double yhigh, double xval, double pw) {
+  if (xhigh - xlow < 1.0e-20) return 0.5 * (ylow + yhigh);
+  return ylow + (yhigh - ylow) * pow((xval - xlow) / (xhigh - xlow), pw);
+}
+__device__ __forceinline__ double gcum_d(double x) { return 0.5 * erfc(-x / 1.4142135623730951); }
+
+__global__ void k_backtr(double* __restrict__ res, long long tot, int nt, const double* __restrict__ vr,
+                         const double* __restrict__ gt, double zmin, double zmax, int lt, double ltp, int ut,
+                         double utp) {
+  for (long long q = blockIdx.x * (long long)blockDim.x + threadIdx.x; q < tot; q += (long long)gridDim.x * blockDim.x) {
+    const double y = res[q];
+    double z;
+    if (y <= gt[0]) {
+      const double cdflo = gcum_d(gt[0]), cdfbt = gcum_d(y);
+      z = powint_d(0.0, cdflo, zmin, vr[0], cdfbt, lt == 2 ? ltp : 1.0);
+      if (nt == 1) z = vr[0];
+    } else if (y >= gt[nt - 1]) {
+      const double cdfhi = gcum_d(gt[nt - 1]), cdfbt = gcum_d(y);
+      if (ut == 2) {
+        z = powint_d(cdfhi, 1.0, vr[nt - 1], zmax, cdfbt, utp);
+      } else if (ut == 4) {
+        const double lam = pow(vr[nt - 1], utp) * (1.0 - cdfhi);
+        z = pow(lam / fmax(1.0 - cdfbt, 1.0e-300), 1.0 / utp);
+      } else {
+        z = powint_d(cdfhi, 1.0, vr[nt - 1], zmax, cdfbt, 1.0);
+      }
+    } else {
+      int lo = 1, hi = nt;
+      while (hi - lo > 1) {
+        const int mid = (lo + hi) / 2;
+        if (gt[mid - 1] <= y) lo = mid;
+        else hi = mid;
+      }
+      z = powint_d(gt[lo - 1], gt[hi - 1], vr[lo - 1], vr[hi - 1], y, 1.0);
+    }
+    res[q] = z;
+  }
+}
+
+__global__ void k_add(double* __restrict__ res, long long tot, double v) {
+  for (long long q = blockIdx.x * (long long)blockDim.x + threadIdx.x; q < tot; q += (long long)gridDim.x * blockDim.x)
+    res[q] += v;
+}
+
+}  // namespace ss3d
+
+using namespace ss3d;
+
+// ---------------------------------------------------------------- host helpers
+namespace {
+
+int fnint(double x) { return (int)lround(x); }   // Fortran nint: half away from zero
+
+// GSLIB-style heapsort of an index array by key (sift-down heap, ascending);
+// the same algorithm as the reference so that ties end in the same order
+void heapsort_idx(const double* key, int* idx, int n) {
+  auto sift = [&](int root, int last) {
+    int parent = root;
+    int v = idx[parent - 1];
+    for (;;) {
+      int child = 2 * parent;
+      if (child > last) break;
+      if (child < last && key[idx[child] - 1] > key[idx[child - 1] - 1]) child = child + 1;
+      if (key[idx[child - 1] - 1] > key[v - 1]) {
+        idx[parent - 1] = idx[child - 1];
+        parent = child;
+      } else {
+        break;
+      }
+    }
+    idx[parent - 1] = v;
+  };
+  for (int i = n / 2; i >= 1; i--) sift(i, n);
+  for (int i = n; i >= 2; i--) {
+    std::swap(idx[0], idx[i - 1]);
+    sift(1, i - 1);
+  }
+}
+
+// inverse standard normal cdf: Acklam's rational approximation refined by one
+// Halley step on erfc (as the reference's gauinv)
+double gauinv(double p0) {
+  static const double a[6] = {-3.969683028665376e+01, 2.209460984245205e+02, -2.759285104469687e+02,
+                              1.383577518672690e+02, -3.066479806614716e+01, 2.506628277459239e+00};
+  static const double b[5] = {-5.447609879822406e+01, 1.615858368580409e+02, -1.556989798598866e+02,
+                              6.680131188771972e+01, -1.328068155288572e+01};
+  static const double c[6] = {-7.784894002430293e-03, -3.223964580411365e-01, -2.400758277161838e+00,
+                              -2.549732539343734e+00, 4.374664141464968e+00, 2.938163982698783e+00};
+  static const double d[4] = {7.784695709041462e-03, 3.224671290700398e-01, 2.445134137142996e+00,
+                              3.754408661907416e+00};
+  const double p = std::min(std::max(p0, 1.0e-15), 1.0 - 1.0e-15);
+  double x;
+  if (p < 0.02425) {
+    const double q = sqrt(-2.0 * log(p));
+    x = (((((c[0] * q + c[1]) * q + c[2]) * q + c[3]) * q + c[4]) * q + c[5]) /
+        ((((d[0] * q + d[1]) * q + d[2]) * q + d[3]) * q + 1.0);
+  } else if (p <= 1.0 - 0.02425) {
+    const double q = p - 0.5, r = q * q;
+    x = (((((a[0] * r + a[1]) * r + a[2]) * r + a[3]) * r + a[4]) * r + a[5]) * q /
+        (((((b[0] * r + b[1]) * r + b[2]) * r + b[3]) * r + b[4]) * r + 1.0);
+  } else {
+    const double q = sqrt(-2.0 * log(1.0 - p));
+    x = -((((((c[0] * q + c[1]) * q + c[2]) * q + c[3]) * q + c[4]) * q + c[5]) /
+          ((((d[0] * q + d[1]) * q + d[2]) * q + d[3]) * q + 1.0));
+  }
+  const double e = 0.5 * erfc(-x / 1.4142135623730951) - p;
+  const double u = e * 2.5066282746310002 * exp(0.5 * x * x);
+  return x - u / (1.0 + 0.5 * x * u);
+}
+
+struct DevBuf {
+  std::vector<void*> ptrs;
+  ~DevBuf() {
+    for (void* p : ptrs) cudaFree(p);
+  }
+  template <typename T>
+  cudaError_t alloc(T** p, size_t n) {
+    cudaError_t e = cudaMalloc((void**)p, sizeof(T) * std::max<size_t>(n, 1));
+    if (e == cudaSuccess) ptrs.push_back(*p);
+    return e;
+  }
+};
+
+}  // namespace
+
+extern "C" int ss3d_condition(double* res, const int n[3], int nreal, const double xmin3[3], const double d3[3],
+                              const ss3d_struct* st, int nst, double nugget, const ss3d_cond_params* cp,
+                              const double* rows, int nrows, int nvar, int precision, ss3d_cond_stats* cs,
+                              double* vrt_out, double* gtt_out, double* dxs_out, double* dys_out, double* dzs_out,
+                              double* dval_out, double* dg_out) {
+  if (!res || !n || !xmin3 || !d3 || !st || !cp || (!rows && nrows > 0))
+    return set_error(SS3D_EINVAL, "NULL argument");
+  if (nst < 1 || nst > MAXST) return set_error(SS3D_EINVAL, "nstruct out of range");
+  if (cp->ndmax < 1 || cp->ndmax > 100) return set_error(SS3D_EINVAL, "cond: ndmax must be in 1..100");
+  if (cp->radius[0] <= 0 || cp->radius[1] <= 0 || cp->radius[2] <= 0)
+    return set_error(SS3D_EINVAL, "cond: search radii must be positive");
+  if (precision != SS3D_FP64 && precision != SS3D_FP32) return set_error(SS3D_EINVAL, "unknown precision");
+  auto colok = [&](int c, bool opt) { return (opt && c == 0) || (c >= 1 && c <= nvar); };
+  if (!colok(cp->ixc, false) || !colok(cp->iyc, false) || !colok(cp->ivc, false) || !colok(cp->izc, true) ||
+      !colok(cp->iwc, true))
+    return set_error(SS3D_EINVAL, "cond: data column out of range");
+  const int nx = n[0], ny = n[1], nz = n[2];
+  const double xmin = xmin3[0], ymin = xmin3[1], zmin = xmin3[2];
+  const double dx = d3[0], dy = d3[1], dz = d3[2];
+  // search ellipsoid as a unit-sill spherical structure (f90:754-758)
+  ss3d_struct srch{1, 1.0, cp->radius[0], cp->radius[1], cp->radius[2], cp->angles[0], cp->angles[1], cp->angles[2]};
+  double srot[3][3], saxes[3][3];
+  setrot_public(srch, srot, saxes);
+  const double ex = sqrt(saxes[0][0] * saxes[0][0] + saxes[1][0] * saxes[1][0] + saxes[2][0] * saxes[2][0]);
+  const double ey = sqrt(saxes[0][1] * saxes[0][1] + saxes[1][1] * saxes[1][1] + saxes[2][1] * saxes[2][1]);
+  const double ez = sqrt(saxes[0][2] * saxes[0][2] + saxes[1][2] * saxes[1][2] + saxes[2][2] * saxes[2][2]);
+  // ---- snap to nodes, trim, drop data outside the grid (f90:782-804)
+  std::vector<double> raw;
+  std::vector<double> key;
+  raw.reserve((size_t)nrows * 5);
+  int nn = 0, nout = 0;
+  for (int q = 0; q < nrows; q++) {
+    const double* row = rows + (size_t)q * nvar;
+    const double v = row[cp->ivc - 1];
+    if (v < cp->tmin || v >= cp->tmax) continue;
+    const int j = fnint((row[cp->ixc - 1] - xmin) / dx) + 1;
+    const int k = fnint((row[cp->iyc - 1] - ymin) / dy) + 1;
+    int r = 1;
+    if (cp->izc > 0 && nz > 1) r = fnint((row[cp->izc - 1] - zmin) / dz) + 1;
+    if (j < 1 || j > nx || k < 1 || k > ny || r < 1 || r > nz) {
+      nout++;
+      continue;
+    }
+    raw.push_back(j);
+    raw.push_back(k);
+    raw.push_back(r);
+    raw.push_back(v);
+    raw.push_back(cp->iwc > 0 ? row[cp->iwc - 1] : 1.0);
+    key.push_back((double)j + (double)nx * ((double)(k - 1) + (double)ny * (double)(r - 1)));
+    nn++;
+  }
+  if (nn == 0) return set_error(SS3D_ENODATA, "cond: no conditioning data inside the grid");
+  // ---- merge data of the same node (f90:805-828)
+  std::vector<int> ord(nn);
+  for (int q = 0; q < nn; q++) ord[q] = q + 1;
+  heapsort_idx(key.data(), ord.data(), nn);
+  std::vector<int> ix, iy, iz;
+  std::vector<double> dval, dwt;
+  for (int i = 1; i <= nn;) {
+    int j = i;
+    while (j < nn && key[ord[j] - 1] == key[ord[i - 1] - 1]) j++;
+    const double* r0 = &raw[5 * (size_t)(ord[i - 1] - 1)];
+    ix.push_back(fnint(r0[0]));
+    iy.push_back(fnint(r0[1]));
+    iz.push_back(fnint(r0[2]));
+    double sw = 0.0, svw = 0.0;
+    for (int q = i; q <= j; q++) sw = sw + raw[5 * (size_t)(ord[q - 1] - 1) + 4];
+    for (int q = i; q <= j; q++) svw = svw + raw[5 * (size_t)(ord[q - 1] - 1) + 3] * raw[5 * (size_t)(ord[q - 1] - 1) + 4];
+    dwt.push_back(sw);
+    dval.push_back(svw / sw);
+    i = j + 1;
+  }
+  const int nd = (int)ix.size();
+  std::vector<double> dxs(nd), dys(nd), dzs(nd), dg(nd), vrt(nd), gtt(nd);
+  for (int q = 0; q < nd; q++) {
+    dxs[q] = xmin + (double)(ix[q] - 1) * dx;
+    dys[q] = ymin + (double)(iy[q] - 1) * dy;
+    dzs[q] = zmin + (double)(iz[q] - 1) * dz;
+  }
+  // ---- normal scores (f90:830-847, nscore f90:639-658)
+  double dmean = 0.0, dvar = 0.0;
+  int nt = nd;
+  if (cp->itrans == 1) {
+    std::vector<int> idx(nd);
+    for (int q = 0; q < nd; q++) idx[q] = q + 1;
+    heapsort_idx(dval.data(), idx.data(), nd);
+    double sw = 0.0;
+    for (int q = 0; q < nd; q++) sw = sw + dwt[q];
+    double cpv = 0.0, oldcp = 0.0;
+    for (int q = 0; q < nd; q++) {
+      cpv = cpv + dwt[idx[q] - 1] / sw;
+      gtt[q] = gauinv(0.5 * (cpv + oldcp));
+      vrt[q] = dval[idx[q] - 1];
+      dg[idx[q] - 1] = gtt[q];
+      oldcp = cpv;
+    }
+    double s = 0.0;
+    for (int q = 0; q < nd; q++) s = s + dg[q];
+    dmean = s / nd;
+    double v = 0.0;
+    for (int q = 0; q < nd; q++) v = v + (dg[q] - s / nd) * (dg[q] - s / nd);
+    dvar = v / nd;
+  } else {
+    for (int q = 0; q < nd; q++) dg[q] = dval[q] - cp->skmean;
+  }
+  // ---- super blocks (f90:866-892)
+  int nsbx = std::max(1, std::min(100, (int)ceil((double)nx * dx / (0.5 * ex))));
+  int nsby = std::max(1, std::min(100, (int)ceil((double)ny * dy / (0.5 * ey))));
+  int nsbz = std::max(1, std::min(100, (int)ceil((double)nz * dz / (0.5 * ez))));
+  if (nz == 1) nsbz = 1;
+  while ((double)nsbx * nsby * nsbz > 2.0e6) {
+    nsbx = std::max(1, nsbx * 3 / 4);
+    nsby = std::max(1, nsby * 3 / 4);
+    nsbz = std::max(1, nsbz * 3 / 4);
+  }
+  const int nsb = nsbx * nsby * nsbz;
+  const double bsx = (double)nx * dx / (double)nsbx, bsy = (double)ny * dy / (double)nsby,
+               bsz = (double)nz * dz / (double)nsbz;
+  const int mbx = (int)ceil(ex / bsx), mby = (int)ceil(ey / bsy), mbz = (int)ceil(ez / bsz);
+  std::vector<int> sbstart(nsb + 1), sbcount(nsb, 0), sbidx(nd), sbof(nd);
+  for (int q = 0; q < nd; q++) {
+    const int b1 = std::min(nsbx, std::max(1, (int)((dxs[q] - xmin + 0.5 * dx) / bsx) + 1));
+    const int b2 = std::min(nsby, std::max(1, (int)((dys[q] - ymin + 0.5 * dy) / bsy) + 1));
+    const int b3 = std::min(nsbz, std::max(1, (int)((dzs[q] - zmin + 0.5 * dz) / bsz) + 1));
+    sbof[q] = b1 + nsbx * (b2 - 1 + nsby * (b3 - 1));
+    sbcount[sbof[q] - 1]++;
+  }
+  sbstart[0] = 1;
+  for (int q = 1; q <= nsb; q++) sbstart[q] = sbstart[q - 1] + sbcount[q - 1];
+  std::fill(sbcount.begin(), sbcount.end(), 0);
+  for (int q = 0; q < nd; q++) {
+    const int b = sbof[q];
+    sbidx[sbstart[b - 1] + sbcount[b - 1] - 1] = q + 1;
+    sbcount[b - 1]++;
+  }
+  Model mdl;
+  model_public(st, nst, nugget, mdl);
+  CondGeo G{};
+  G.nx = nx;
+  G.ny = ny;
+  G.nz = nz;
+  G.nreal = nreal;
+  G.nd = nd;
+  G.ndmax = cp->ndmax;
+  G.xmin = xmin;
+  G.ymin = ymin;
+  G.zmin = zmin;
+  G.dx = dx;
+  G.dy = dy;
+  G.dz = dz;
+  G.nsbx = nsbx;
+  G.nsby = nsby;
+  G.nsbz = nsbz;
+  G.mbx = mbx;
+  G.mby = mby;
+  G.mbz = mbz;
+  G.bsx = bsx;
+  G.bsy = bsy;
+  G.bsz = bsz;
+  for (int r = 0; r < 3; r++)
+    for (int c = 0; c < 3; c++) G.rot[3 * r + c] = srot[r][c];
+  G.rmax2 = cp->radius[0] * cp->radius[0];
+  G.c0 = covariance(mdl, 0.0, 0.0, 0.0);
+  // ---- device work
+  cudaStream_t stm = current_stream();
+  const long long M = (long long)nx * ny * nz;
+  cudaPointerAttributes pa;
+  const bool dev_res = cudaPointerGetAttributes(&pa, res) == cudaSuccess &&
+                       (pa.type == cudaMemoryTypeDevice || pa.type == cudaMemoryTypeManaged);
+  cudaGetLastError();
+  DevBuf bufs;
+  double* dres = res;
+  cudaError_t e = cudaSuccess;
+  if (!dev_res) {
+    e = bufs.alloc(&dres, (size_t)M * nreal);
+    if (e == cudaSuccess) e = cudaMemcpyAsync(dres, res, sizeof(double) * M * nreal, cudaMemcpyHostToDevice, stm);
+  }
+  double *ddx = nullptr, *ddy = nullptr, *ddz = nullptr, *ddg = nullptr, *dsimd = nullptr, *dvr = nullptr,
+         *dgt = nullptr;
+  int *dix = nullptr, *diy = nullptr, *diz = nullptr, *dsbs = nullptr, *dsbi = nullptr, *dnbr = nullptr,
+      *dnnb = nullptr;
+  unsigned long long* dcnt = nullptr;
+  const int chunk = (int)std::min<long long>(M, std::max<long long>(1, ((long long)1 << 30) / (4LL * cp->ndmax + 4)));
+  if (e == cudaSuccess) e = bufs.alloc(&ddx, nd);
+  if (e == cudaSuccess) e = bufs.alloc(&ddy, nd);
+  if (e == cudaSuccess) e = bufs.alloc(&ddz, nd);
+  if (e == cudaSuccess) e = bufs.alloc(&ddg, nd);
+  if (e == cudaSuccess) e = bufs.alloc(&dsimd, (size_t)nd * nreal);
+  if (e == cudaSuccess) e = bufs.alloc(&dix, nd);
+  if (e == cudaSuccess) e = bufs.alloc(&diy, nd);
+  if (e == cudaSuccess) e = bufs.alloc(&diz, nd);
+  if (e == cudaSuccess) e = bufs.alloc(&dsbs, nsb + 1);
+  if (e == cudaSuccess) e = bufs.alloc(&dsbi, nd);
+  if (e == cudaSuccess) e = bufs.alloc(&dnbr, (size_t)chunk * cp->ndmax);
+  if (e == cudaSuccess) e = bufs.alloc(&dnnb, chunk);
+  if (e == cudaSuccess) e = bufs.alloc(&dcnt, 4);
+  if (e == cudaSuccess) e = bufs.alloc(&dvr, nd);
+  if (e == cudaSuccess) e = bufs.alloc(&dgt, nd);
+  auto h2d = [&](void* dst, const void* src, size_t bytes) {
+    if (e == cudaSuccess) e = cudaMemcpyAsync(dst, src, bytes, cudaMemcpyHostToDevice, stm);
+  };
+  h2d(ddx, dxs.data(), sizeof(double) * nd);
+  h2d(ddy, dys.data(), sizeof(double) * nd);
+  h2d(ddz, dzs.data(), sizeof(double) * nd);
+  h2d(ddg, dg.data(), sizeof(double) * nd);
+  h2d(dix, ix.data(), sizeof(int) * nd);
+  h2d(diy, iy.data(), sizeof(int) * nd);
+  h2d(diz, iz.data(), sizeof(int) * nd);
+  h2d(dsbs, sbstart.data(), sizeof(int) * (nsb + 1));
+  h2d(dsbi, sbidx.data(), sizeof(int) * nd);
+  h2d(dvr, vrt.data(), sizeof(double) * nd);
+  h2d(dgt, gtt.data(), sizeof(double) * nd);
+  if (e == cudaSuccess) e = cudaMemsetAsync(dcnt, 0, sizeof(unsigned long long) * 4, stm);
+  if (e == cudaSuccess) {
+    k_gather_simd<<<std::max(1, std::min(1024, (int)(((long long)nd * nreal + 255) / 256))), 256, 0, stm>>>(
+        dres, M, dix, diy, diz, nd, nreal, nx, ny, dsimd);
+    ++g_launch_count;
+    e = cudaGetLastError();
+  }
+  // kriging CTAs: warps per block limited by the shared memory of one warp
+  const size_t per = cond_warp_bytes(cp->ndmax);
+  const int wpb = (int)std::max<size_t>(1, std::min<size_t>(8, (size_t)(96 * 1024) / per));
+  if (e == cudaSuccess) {
+    if (precision == SS3D_FP64)
+      e = cudaFuncSetAttribute(k_cond_krige<0>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)(per * wpb));
+    else
+      e = cudaFuncSetAttribute(k_cond_krige<1>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)(per * wpb));
+  }
+  for (long long node0 = 0; node0 < M && e == cudaSuccess; node0 += chunk) {
+    const int count = (int)std::min<long long>(chunk, M - node0);
+    k_cond_search<<<(count + 127) / 128, 128, 0, stm>>>(G, node0, count, ddx, ddy, ddz, dsbs, dsbi, dix, diy, diz,
+                                                       dnbr, dnnb);
+    ++g_launch_count;
+    e = cudaGetLastError();
+    if (e != cudaSuccess) break;
+    const int nblk = (int)std::min<long long>(148 * 16, ((long long)count + wpb - 1) / wpb);
+    if (precision == SS3D_FP64)
+      k_cond_krige<0><<<nblk, 32 * wpb, per * wpb, stm>>>(G, mdl, node0, count, dnbr, dnnb, ddx, ddy, ddz, ddg,
+                                                          dsimd, dres, dcnt);
+    else
+      k_cond_krige<1><<<nblk, 32 * wpb, per * wpb, stm>>>(G, mdl, node0, count, dnbr, dnnb, ddx, ddy, ddz, ddg,
+                                                          dsimd, dres, dcnt);
+    ++g_launch_count;
+    e = cudaGetLastError();
+  }
+  const long long tot = M * nreal;
+  if (e == cudaSuccess && cp->itrans == 1) {
+    k_backtr<<<(int)std::min<long long>(148 * 32, (tot + 255) / 256), 256, 0, stm>>>(
+        dres, tot, nt, dvr, dgt, cp->zmin, cp->zmax, cp->ltail, cp->ltpar, cp->utail, cp->utpar);
+    ++g_launch_count;
+    e = cudaGetLastError();
+  } else if (e == cudaSuccess && cp->skmean != 0.0) {
+    k_add<<<(int)std::min<long long>(148 * 32, (tot + 255) / 256), 256, 0, stm>>>(dres, tot, cp->skmean);
+    ++g_launch_count;
+    e = cudaGetLastError();
+  }
+  unsigned long long cnt[4] = {0, 0, 0, 0};
+  if (e == cudaSuccess) e = cudaMemcpyAsync(cnt, dcnt, sizeof cnt, cudaMemcpyDeviceToHost, stm);
+  if (e == cudaSuccess && !dev_res)
+    e = cudaMemcpyAsync(res, dres, sizeof(double) * M * nreal, cudaMemcpyDeviceToHost, stm);
+  if (e == cudaSuccess) e = cudaStreamSynchronize(stm);
+  if (e != cudaSuccess) {
+    cudaGetLastError();
+    return set_error(SS3D_ECUDA, (std::string("condition: ") + cudaGetErrorString(e)).c_str());
+  }
+  if (cs) {
+    cs->nd = nd;
+    cs->nmerged = nn - nd;
+    cs->nout = nout;
+    cs->nsb[0] = nsbx;
+    cs->nsb[1] = nsby;
+    cs->nsb[2] = nsbz;
+    cs->nsum = (int64_t)cnt[0];
+    cs->nfail = (int)cnt[1];
+    cs->nnone = (int)cnt[2];
+    cs->nexact = (int)cnt[3];
+    cs->data_mean = dmean;
+    cs->data_var = dvar;
+  }
+  for (int q = 0; q < nd; q++) {
+    if (vrt_out) vrt_out[q] = vrt[q];
+    if (gtt_out) gtt_out[q] = gtt[q];
+    if (dxs_out) dxs_out[q] = dxs[q];
+    if (dys_out) dys_out[q] = dys[q];
+    if (dzs_out) dzs_out[q] = dzs[q];
+    if (dval_out) dval_out[q] = dval[q];
+    if (dg_out) dg_out[q] = dg[q];
+  }
+  return SS3D_OK;
+}

@@ -8,6 +8,7 @@
 #include <string>
 
 #include "ss3d_device.cuh"
+#include "../../include/specsim3d_gpu.h"
 
 namespace ss3d {
 
@@ -94,6 +95,8 @@ struct NoallocView {
   const float* amp32;
 };
 int set_error(int code, const char* msg);     // sets the message returned by ss3d_last_error
+void setrot_public(const ss3d_struct& s, double rot[3][3], double axes[3][3]);
+void model_public(const ss3d_struct* st, int nst, double nugget, Model& m);
 cudaStream_t current_stream();                // stream selected with ss3d_set_stream
 
 }  // namespace ss3d

@@ -1,0 +1,119 @@
+"""GPU conditioning (kriging of the residual) against the oracle's condition_field.
+
+The neighbour search reproduces the reference's sets exactly (same FP64
+expression order without FMA, same visit order and insertion rules), so the
+search statistics must match exactly.  The FP64 kriging solve differs from the
+reference only in the order of the Cholesky sums: conditioned values agree to
+1e-9.  The FP32 form (FP32 factor and solve, one FP64-residual refinement)
+agrees to 1e-5 of the field's standard deviation.
+"""
+import numpy as np
+import pytest
+
+import oracle_lib as ora
+
+pytestmark = pytest.mark.gpu
+
+
+def _params(**kw):
+    p = dict(ixc=1, iyc=2, izc=3, ivc=4, iwc=0, tmin=-1e21, tmax=1e21, itrans=0, skmean=0.0, zlo=-5.0, zhi=5.0,
+             ltail=1, ltpar=0.0, utail=1, utpar=0.0, rmax=100.0, rmed=100.0, rvert=100.0, sa1=0.0, sa2=0.0, sa3=0.0,
+             ndmax=100)
+    p.update(kw)
+    return p
+
+
+def _gpu_params(p):
+    return dict(ixc=p["ixc"], iyc=p["iyc"], izc=p["izc"], ivc=p["ivc"], iwc=p["iwc"], tmin=p["tmin"], tmax=p["tmax"],
+                itrans=p["itrans"], skmean=p["skmean"], zmin=p["zlo"], zmax=p["zhi"], ltail=p["ltail"],
+                ltpar=p["ltpar"], utail=p["utail"], utpar=p["utpar"], radius=(p["rmax"], p["rmed"], p["rvert"]),
+                angles=(p["sa1"], p["sa2"], p["sa3"]), ndmax=p["ndmax"])
+
+
+def _run_both(gpu, sts, nug, n, xmin, d, p, rows, nreal, seed, precision):
+    sp = gpu.Spectrum(sts, nug, d, n, 1)
+    res = sp.realize(seed, nreal, 0, gpu.FP64)
+    a = res.copy()
+    b = res.copy()
+    st_o, ex_o = ora.condition(a, xmin, d, sts, nug, p, rows)
+    st_g, ex_g = gpu.condition(b, xmin, d, sts, nug, _gpu_params(p), rows, precision=precision)
+    return a, b, st_o, st_g, ex_o, ex_g
+
+
+def _check_stats(st_o, st_g):
+    for k in ("nd", "nmerged", "nout", "nsb", "nsum", "nnone", "nexact", "nfail"):
+        assert st_o[k] == st_g[k], (k, st_o[k], st_g[k])
+
+
+def test_gaussian_all_data_in_neighbourhood(gpu):
+    """Reference tests/test_conditional.py:test_gaussian setting (30x30x10, 40 data, radii 100, ndmax 100)."""
+    rng = np.random.default_rng(3)
+    n = (30, 30, 10)
+    idx = rng.choice(n[0] * n[1] * n[2], 40, replace=False)
+    i, j, k = np.unravel_index(idx, n)
+    rows = np.c_[i, j, k, rng.normal(size=40)].astype(float)
+    sts = [(1, 1.0, 12.0, 8.0, 6.0, 30.0, 0.0, 0.0)]
+    p = _params()
+    a, b, so, sg, eo, eg = _run_both(gpu, sts, 0.0, n, (0, 0, 0), (1, 1, 1), p, rows, 6, 12345, gpu.FP64)
+    _check_stats(so, sg)
+    assert np.max(np.abs(a - b)) <= 1e-9
+    # data reproduced at their nodes
+    assert np.max(np.abs(b[:, k, j, i] - rows[:, 3][:, None].T)) < 1e-9
+
+
+def test_nscore_backtransform_2d(gpu):
+    """Reference test_nscore setting: 64x64 2D, 200 lognormal data, itrans 1, linear tails."""
+    rng = np.random.default_rng(5)
+    idx = rng.choice(64 * 64, 200, replace=False)
+    x, y = (idx % 64).astype(float), (idx // 64).astype(float)
+    v = np.exp(rng.normal(1.0, 0.8, 200))
+    rows = np.c_[x, y, v]
+    sts = [(2, 1.0, 15.0, 15.0, 15.0, 0.0, 0.0, 0.0)]
+    p = _params(ixc=1, iyc=2, izc=0, ivc=3, tmin=0.0, itrans=1, zlo=0.0, zhi=200.0, rmax=30.0, rmed=30.0,
+                rvert=30.0, ndmax=16)
+    a, b, so, sg, eo, eg = _run_both(gpu, sts, 0.0, (64, 64, 1), (0, 0, 0), (1, 1, 1), p, rows, 4, 777, gpu.FP64)
+    _check_stats(so, sg)
+    assert np.array_equal(eo["gtt"], eg["gtt"]) or np.max(np.abs(eo["gtt"] - eg["gtt"])) < 1e-14
+    assert np.array_equal(eo["vrt"], eg["vrt"])
+    assert np.max(np.abs(a - b) / np.maximum(1.0, np.abs(a))) <= 1e-9
+
+
+@pytest.mark.parametrize("precision,tol", [(0, 1e-9), (1, 1e-5)])
+def test_conditional_config_small(gpu, precision, tol):
+    """Configuration-4-like case: exponential 40/20/8 N60E, nugget 0.05, ndmax 24, skewed data through nscore."""
+    rng = np.random.default_rng(99)
+    n = (48, 40, 16)
+    sts = [(2, 1.0, 40.0, 20.0, 8.0, 60.0, 0.0, 0.0)]
+    sp = gpu.Spectrum(sts, 0.05, (1, 1, 1), n, 1)
+    truth = sp.realize(4242, 1, 0, gpu.FP64)[0]
+    pts = rng.uniform(0, np.array(n) - 1, size=(300, 3))
+    ii = np.rint(pts).astype(int)
+    val = np.exp(0.5 * truth[ii[:, 2], ii[:, 1], ii[:, 0]])
+    rows = np.c_[pts, val]
+    p = _params(tmin=0.0, itrans=1, zlo=0.0, zhi=2 * val.max(), rmax=40.0, rmed=20.0, rvert=8.0, sa1=60.0, ndmax=24)
+    a, b, so, sg, eo, eg = _run_both(gpu, sts, 0.05, n, (0, 0, 0), (1, 1, 1), p, rows, 4, 4243, precision)
+    _check_stats(so, sg)
+    err = np.max(np.abs(a - b)) / max(1e-12, float(np.std(a)))
+    assert err <= tol, err
+
+
+def test_condition_device_array(gpu):
+    import torch
+    rng = np.random.default_rng(8)
+    n = (20, 16, 8)
+    sts = [(1, 1.0, 10.0, 8.0, 4.0, 0.0, 0.0, 0.0)]
+    rows = np.c_[rng.uniform(0, 19, 30), rng.uniform(0, 15, 30), rng.uniform(0, 7, 30), rng.normal(size=30)]
+    sp = gpu.Spectrum(sts, 0.0, (1, 1, 1), n, 1)
+    res = sp.realize(5, 3, 0, gpu.FP64)
+    h = res.copy()
+    gpu.condition(h, (0, 0, 0), (1, 1, 1), sts, 0.0, _gpu_params(_params(rmax=10, rmed=10, rvert=10, ndmax=12)), rows)
+    t = torch.from_numpy(res.copy()).cuda()
+    gpu.condition(t, (0, 0, 0), (1, 1, 1), sts, 0.0, _gpu_params(_params(rmax=10, rmed=10, rvert=10, ndmax=12)), rows)
+    assert np.array_equal(t.cpu().numpy(), h)
+
+
+def test_no_data_inside_grid(gpu):
+    rows = np.array([[100.0, 100.0, 100.0, 1.0]])
+    res = np.zeros((1, 4, 4, 4))
+    with pytest.raises(gpu.SpecsimError, match="no conditioning data"):
+        gpu.condition(res, (0, 0, 0), (1, 1, 1), [(1, 1.0, 5, 5, 5, 0, 0, 0)], 0.0, _gpu_params(_params()), rows)
