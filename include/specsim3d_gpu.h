@@ -138,6 +138,19 @@ int ss3d_debug_coefficients(const ss3d_spectrum *sp, int iseed, int64_t r, int i
 int ss3d_realize_noalloc(const ss3d_spectrum *sp, int iseed, int64_t r_first, int nreal, int igauss, int precision,
                          void *out, int out_dtype);
 
+/* Autotuner of the realization kernels (no counterpart in the reference, whose
+ * FFT has a single code path).  For the grid of sp, times each compiled tile
+ * variant of the synthesis pass, the middle column pass and the C2R row pass
+ * on nreal realizations and keeps the fastest for later calls in this process
+ * (per precision and transform length).  chosen (may be NULL) receives the
+ * variants picked for {middle pass, synthesis pass, row pass}. */
+int ss3d_autotune(const ss3d_spectrum *sp, int igauss, int precision, int nreal, int chosen[3]);
+
+/* Explicit variant (0..3) of kernel kind 0 middle pass, 1 synthesis pass,
+ * 2 row pass, for one precision and transform length 2^logn.  Every variant
+ * computes the same values; they differ in tile shape only. */
+int ss3d_set_variant(int kind, int precision, int logn, int variant);
+
 /* ---------------------------------------------------------------- variogram */
 
 /* Experimental semivariograms of nreal fields res(nx,ny,nz,nreal) (FP64, host or

@@ -78,6 +78,14 @@ def profile_read():
     return {name: (float(ms[q]), int(ln[q])) for q, name in enumerate(STAGES)}, int(tot.value)
 
 
+def autotune(spectrum, igauss=1, precision=FP32, nreal=2):
+    """Pick the fastest tile variant of each realization kernel for this grid (kept for the process)."""
+    ch = np.zeros(3, dtype=np.int32)
+    L.check(L.lib().ss3d_autotune(spectrum.handle, int(igauss), int(precision), int(nreal),
+                                  ctypes.c_void_p(ch.ctypes.data)))
+    return {"middle_pass": int(ch[0]), "synthesis_pass": int(ch[1]), "row_pass": int(ch[2])}
+
+
 def _out_ptr(out):
     """(pointer, dtype code, nbytes) of a numpy array or a torch tensor."""
     if isinstance(out, np.ndarray):

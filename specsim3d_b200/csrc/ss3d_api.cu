@@ -658,3 +658,66 @@ int ss3d::spectrum_view(const ss3d_spectrum* sp, NoallocView* v) {
 // model helpers shared with the conditioning module
 void ss3d::setrot_public(const ss3d_struct& s, double rot[3][3], double axes[3][3]) { setrot_rc(s, rot, axes); }
 void ss3d::model_public(const ss3d_struct* st, int nst, double nugget, Model& m) { build_model(st, nst, nugget, m); }
+
+// ---------------------------------------------------------------- autotuner
+namespace ss3d {
+extern int g_variant[3][2][16];
+}
+
+extern "C" int ss3d_autotune(const ss3d_spectrum* sp, int igauss, int precision, int nreal, int chosen[3]) {
+  if (!sp) return fail(SS3D_EINVAL, "spectrum is NULL");
+  if (precision != SS3D_FP64 && precision != SS3D_FP32) return fail(SS3D_EINVAL, "unknown precision");
+  if (nreal < 1) return fail(SS3D_EINVAL, "nreal must be >= 1");
+  const Geo& g = sp->geo;
+  const int p = precision == SS3D_FP32 ? 1 : 0;
+  // the transform length each kernel kind runs at for this grid
+  int L[3] = {-1, -1, -1};
+  if (g.npz > 1) {
+    L[1] = ilog2i(g.npz);
+    if (g.npy > 1) L[0] = ilog2i(g.npy);
+  } else if (g.npy > 1) {
+    L[1] = ilog2i(g.npy);
+  }
+  if (g.npx > 1) L[2] = ilog2i(g.npx) - 1;
+  // the middle pass and the synthesis pass may share a length: tune them jointly then
+  const size_t M = (size_t)g.nx * g.ny * g.nz;
+  float* out = nullptr;
+  CK(cudaMalloc(&out, sizeof(float) * M * nreal));
+  const bool prof_was = g_prof;
+  double best[3] = {1e30, 1e30, 1e30};
+  int bestv[3] = {0, 0, 0};
+  int rc = SS3D_OK;
+  for (int v = 0; v < 4 && rc == SS3D_OK; v++) {
+    for (int k = 0; k < 3; k++)
+      if (L[k] >= 0) g_variant[k][p][L[k]] = v;
+    rc = ss3d_realize(sp, 1, 0, nreal, igauss, precision, out, SS3D_OUT_F32, nullptr);   // warm up
+    if (rc) break;
+    g_prof = true;
+    for (int q = 0; q < SS3D_NSTAGE; q++) g_prof_ms[q] = 0;
+    for (int rep = 0; rep < 2 && rc == SS3D_OK; rep++)
+      rc = ss3d_realize(sp, 1, 0, nreal, igauss, precision, out, SS3D_OUT_F32, nullptr);
+    g_prof = prof_was;
+    if (rc) break;
+    const double ms[3] = {g_prof_ms[2], g_prof_ms[1], g_prof_ms[3]};   // stage 2 middle, 1 synthesis, 3 rows
+    for (int k = 0; k < 3; k++)
+      if (L[k] >= 0 && ms[k] < best[k]) {
+        best[k] = ms[k];
+        bestv[k] = v;
+      }
+  }
+  for (int k = 0; k < 3; k++)
+    if (L[k] >= 0) g_variant[k][p][L[k]] = bestv[k];
+  for (int q = 0; q < SS3D_NSTAGE; q++) g_prof_ms[q] = 0;
+  cudaFree(out);
+  if (chosen)
+    for (int k = 0; k < 3; k++) chosen[k] = bestv[k];
+  return rc;
+}
+
+extern "C" int ss3d_set_variant(int kind, int precision, int logn, int variant) {
+  if (kind < 0 || kind > 2 || (precision != SS3D_FP64 && precision != SS3D_FP32) || logn < 0 || logn > 15 ||
+      variant < 0 || variant > 3)
+    return fail(SS3D_EINVAL, "invalid variant selection");
+  g_variant[kind][precision == SS3D_FP32 ? 1 : 0][logn] = variant;
+  return SS3D_OK;
+}

@@ -40,10 +40,15 @@ template <int SIGN, typename C> __device__ __forceinline__ C cmul_si(C a) {
 
 // ---------------------------------------------------------------- Park-Miller
 __host__ __device__ __forceinline__ uint32_t pm_mulmod(uint32_t a, uint32_t b) {
-  uint64_t p = (uint64_t)a * (uint64_t)b;           // < 2^62
-  uint64_t r = (p & PM_M) + (p >> 31);               // < 2^32
-  r = (r & PM_M) + (r >> 31);
-  return (uint32_t)(r >= PM_M ? r - PM_M : r);
+  // a, b < 2^31: p = a b < 2^62 = hi 2^32 + lo;  p mod (2^31 - 1) = (p & m) + (p >> 31) folded once
+#ifdef __CUDA_ARCH__
+  const uint32_t lo = a * b, hi = __umulhi(a, b);
+#else
+  const uint64_t p = (uint64_t)a * (uint64_t)b;
+  const uint32_t lo = (uint32_t)p, hi = (uint32_t)(p >> 32);
+#endif
+  uint32_t r = (lo & PM_M) + ((hi << 1) | (lo >> 31));   // <= 2m - 2 for a, b < m
+  return r >= PM_M ? r - PM_M : r;
 }
 
 // 16807^e mod (2^31-1) from the three 11-bit power tables
@@ -113,20 +118,18 @@ __host__ __device__ __forceinline__ int row_class(const Geo& g, int j, int k) {
 // polynomials of sin (to x^9) and cos (to x^8): truncation below 3e-8, argument
 // error below 5e-8 (one float rounding of the exact integer remainder).
 __device__ __forceinline__ void phasor_f(uint32_t s, float& c, float& sn) {
-  const uint64_t q = 4ull * s;
-  int n = __float2int_rn((float)s * (4.0f / 2147483647.0f));   // nearest quarter (off by one at most)
-  const long long rem = (long long)q - (long long)n * (long long)PM_M;
-  const float x = (float)rem * 7.3145904e-10f;                  // (pi/2) / (2^31-1)
+  const int n = __float2int_rn((float)s * (4.0f / 2147483647.0f));   // nearest quarter (off by one at most)
+  const int rem = (int)(4u * s - (uint32_t)n * PM_M);                // exact 4s - n m, |.| <= m/2 + 2^11
+  const float x = (float)rem * 7.3145904e-10f;                         // (pi/2) / (2^31-1)
   const float x2 = x * x;
   const float sp = x * fmaf(x2, fmaf(x2, fmaf(x2, fmaf(x2, 2.7557319e-6f, -1.9841270e-4f), 8.3333333e-3f),
                                      -1.6666667e-1f), 1.0f);
   const float cp = fmaf(x2, fmaf(x2, fmaf(x2, fmaf(x2, 2.4801587e-5f, -1.3888889e-3f), 4.1666667e-2f), -0.5f), 1.0f);
-  switch (n & 3) {
-    case 0: c = cp; sn = sp; break;
-    case 1: c = -sp; sn = cp; break;
-    case 2: c = -cp; sn = -sp; break;
-    default: c = sp; sn = -cp; break;
-  }
+  // rotate by n quarter turns: (c, s) -> (cp, sp), (-sp, cp), (-cp, -sp), (sp, -cp)
+  const bool odd = n & 1;
+  const float c0 = odd ? sp : cp, s0 = odd ? cp : sp;
+  c = ((n + 1) & 2) ? -c0 : c0;
+  sn = (n & 2) ? -s0 : s0;
 }
 __device__ __forceinline__ void phasor_d(uint32_t s, double& c, double& sn) {
   double u = (double)s / 2147483647.0;
@@ -138,19 +141,18 @@ __device__ __forceinline__ void phasor_d(uint32_t s, double& c, double& sn) {
 // below 1/2 |ln u| >= ln 2 and the hardware log2 (relative error ~2^-22) is
 // accurate enough.
 __device__ __forceinline__ float m2log_f(uint32_t s) {
-  if (s >= (1u << 30)) {
-    const float a = (float)(PM_M - s);
-    const float z = -__fdividef(a, 4294967294.0f - a);        // m + s = 2m - (m - s)
-    const float z2 = z * z;
-    float p = fmaf(z2, 1.0f / 13.0f, 1.0f / 11.0f);
-    p = fmaf(z2, p, 1.0f / 9.0f);
-    p = fmaf(z2, p, 1.0f / 7.0f);
-    p = fmaf(z2, p, 1.0f / 5.0f);
-    p = fmaf(z2, p, 1.0f / 3.0f);
-    p = fmaf(z2, p, 1.0f);
-    return -4.0f * (p * z);
-  }
-  return -1.3862944f * __log2f((float)s * (1.0f / 2147483647.0f));   // -2 ln 2 * log2(u)
+  const float a = (float)(PM_M - s);
+  const float z = -__fdividef(a, 4294967294.0f - a);        // (u-1)/(u+1), m + s = 2m - (m - s)
+  const float z2 = z * z;
+  float p = fmaf(z2, 1.0f / 13.0f, 1.0f / 11.0f);
+  p = fmaf(z2, p, 1.0f / 9.0f);
+  p = fmaf(z2, p, 1.0f / 7.0f);
+  p = fmaf(z2, p, 1.0f / 5.0f);
+  p = fmaf(z2, p, 1.0f / 3.0f);
+  p = fmaf(z2, p, 1.0f);
+  const float near1 = -4.0f * (p * z);
+  const float far = -1.3862944f * __log2f((float)s * (1.0f / 2147483647.0f));   // -2 ln 2 * log2(u)
+  return s >= (1u << 30) ? near1 : far;
 }
 __device__ __forceinline__ double m2log_d(uint32_t s) {
   double u = (double)s / 2147483647.0;

@@ -78,23 +78,31 @@ __device__ __forceinline__ bool line_valid(const Geo& g, int line, int lines) {
 // ---------------------------------------------------------------- register-resident column passes
 // Tile configuration per transform length: TX columns, TPC threads per column,
 // ET = N / TPC elements per thread (16 in float, 8 in double).
-template <typename R, int LOGN> struct ColCfg {
+// Variant V (tuned at run time): bit 0 halves the elements per thread
+// (more threads, fewer registers), bit 1 halves the tile (fewer columns).
+template <typename R, int LOGN, int V = 0> struct ColCfg {
   static constexpr int N = 1 << LOGN;
-  static constexpr int ETW = sizeof(R) == 4 ? 16 : 8;
+  static constexpr int ETW0 = sizeof(R) == 4 ? 16 : 8;
+  static constexpr int ETW = (V & 1) ? (ETW0 / 2 < 8 ? 8 : ETW0 / 2) : ETW0;
   static constexpr int ET = N < ETW ? N : ETW;
   static constexpr int TPC = N / ET;
-  static constexpr int E = sizeof(R) == 4 ? 8192 : 4096;
+  static constexpr int E = (sizeof(R) == 4 ? 8192 : 4096) >> ((V >> 1) & 1);
   static constexpr int TX0 = E / N;
   static constexpr int TX = TX0 > 64 ? 64 : (TX0 < 2 ? 2 : TX0);
   static constexpr int NTH = TX * TPC;
+  static_assert(NTH <= 1024, "tile too large");
 };
 
+// run-time choice of the variant per kernel kind, precision and length
+// (kind 0: column pass, 1: column pass with synthesis, 2: C2R rows)
+int g_variant[3][2][16] = {};
+
 // c2c transform along a strided axis (in place allowed), unscaled, pruned store
-template <typename R, int LOGN, int SIGN>
-__global__ void __launch_bounds__(ColCfg<R, LOGN>::NTH) k_col(AxisArgs a, Geo g, const cpx_t<R>* in, cpx_t<R>* out,
-                                                             Tw tw) {
+template <typename R, int LOGN, int SIGN, int V>
+__global__ void __launch_bounds__(ColCfg<R, LOGN, V>::NTH) k_col(AxisArgs a, Geo g, const cpx_t<R>* in,
+                                                                cpx_t<R>* out, Tw tw) {
   using C = cpx_t<R>;
-  using CF = ColCfg<R, LOGN>;
+  using CF = ColCfg<R, LOGN, V>;
   constexpr int N = CF::N, TX = CF::TX;
   extern __shared__ __align__(16) unsigned char smraw[];
   C* s = reinterpret_cast<C*>(smraw);
@@ -107,7 +115,7 @@ __global__ void __launch_bounds__(ColCfg<R, LOGN>::NTH) k_col(AxisArgs a, Geo g,
   const bool valid = line_valid(g, line0 + t, a.lines);
   const C* src = in + ((long long)grp * a.gstride + line0 + t + (long long)r * a.rstride);
   C* dst = out + ((long long)grp * a.gstride + line0 + t + (long long)r * a.rstride);
-  const long long S = a.S;
+  const int S = (int)a.S;   // offsets inside one realization's grid fit in 32 bits
   const int nout = a.nout;
   for (int q = threadIdx.x; q < N; q += CF::NTH) stw[q] = twtab<R>(tw)[N - 1 + q];
   __syncthreads();
@@ -121,13 +129,13 @@ __global__ void __launch_bounds__(ColCfg<R, LOGN>::NTH) k_col(AxisArgs a, Geo g,
 // First inverse pass with the coefficient synthesis fused into the loader.
 // axis 2: columns are (i, j) plane offsets, positions k;  axis 1 (npz = 1):
 // columns are i, positions j.
-template <typename R, int LOGN>
-__global__ void __launch_bounds__(ColCfg<R, LOGN>::NTH) k_colgen(AxisArgs a, Geo g, const R* __restrict__ amp,
-                                                                const uint32_t* __restrict__ rowstates,
-                                                                const uint32_t* __restrict__ apow, cpx_t<R>* out,
-                                                                Tw tw) {
+template <typename R, int LOGN, int V>
+__global__ void __launch_bounds__(ColCfg<R, LOGN, V>::NTH) k_colgen(AxisArgs a, Geo g, const R* __restrict__ amp,
+                                                                   const uint32_t* __restrict__ rowstates,
+                                                                   const uint32_t* __restrict__ apow, cpx_t<R>* out,
+                                                                   Tw tw) {
   using C = cpx_t<R>;
-  using CF = ColCfg<R, LOGN>;
+  using CF = ColCfg<R, LOGN, V>;
   constexpr int N = CF::N, TX = CF::TX;
   extern __shared__ __align__(16) unsigned char smraw[];
   C* s = reinterpret_cast<C*>(smraw);
@@ -154,7 +162,7 @@ __global__ void __launch_bounds__(ColCfg<R, LOGN>::NTH) k_colgen(AxisArgs a, Geo
   const long long cbase = (long long)grp * a.gstride + line;
   const R* ap = amp + cbase;
   C* dst = out + cbase + (long long)r * a.rstride;
-  const long long S = a.S;
+  const int S = (int)a.S;   // offsets inside one realization's grid fit in 32 bits
   const int nout = a.nout;
   const bool zaxis = a.axis == 2;
   for (int q = threadIdx.x; q < N; q += CF::NTH) stw[q] = twtab<R>(tw)[N - 1 + q];
@@ -263,8 +271,8 @@ __device__ __forceinline__ void block_sum2(double& a, double& b) {
 // then x[2m] = Re z[m], x[2m+1] = Im z[m].  The imaginary parts of X[0] and
 // X[N] are dropped: the reference keeps the real part of the full complex
 // inverse (f90:1339), which does not see them.
-template <typename R, int LOGN> struct RowCfg {
-  using CF = ColCfg<R, LOGN>;
+template <typename R, int LOGN, int V = 0> struct RowCfg {
+  using CF = ColCfg<R, LOGN, V>;
   static constexpr int N = CF::N, TPC = CF::TPC, ET = CF::ET;
   static constexpr int TX0 = CF::E / N;
   static constexpr int TX = TX0 > 64 ? 64 : (TX0 < 1 ? 1 : TX0);
@@ -275,10 +283,10 @@ template <typename R, int LOGN> struct RowCfg {
 
 // inverse length-N FFT of the TX rows staged in s (pitch TX+1), in place;
 // twN holds e^{-2 pi i m/N}, m < N
-template <typename R, int LOGN>
+template <typename R, int LOGN, int V>
 __device__ __forceinline__ void fft_rows_inv(cpx_t<R>* s, const cpx_t<R>* twN) {
   using C = cpx_t<R>;
-  using RC = RowCfg<R, LOGN>;
+  using RC = RowCfg<R, LOGN, V>;
   static_assert(RC::NTH0 >= 32, "row tile needs at least one warp");
   if constexpr (LOGN > 0) {
     const int t = threadIdx.x % RC::TX;
@@ -288,13 +296,13 @@ __device__ __forceinline__ void fft_rows_inv(cpx_t<R>* s, const cpx_t<R>* twN) {
   }
 }
 
-template <typename R, typename O, int LOGN>
-__global__ void __launch_bounds__(RowCfg<R, LOGN>::NTH) k_rows_c2r(Geo g, const cpx_t<R>* __restrict__ in,
-                                                                   long long rstride, O* __restrict__ out,
-                                                                   long long ostride, int nreal, int nblk_per_r,
-                                                                   double* __restrict__ part, Tw tw) {
+template <typename R, typename O, int LOGN, int V>
+__global__ void __launch_bounds__(RowCfg<R, LOGN, V>::NTH) k_rows_c2r(Geo g, const cpx_t<R>* __restrict__ in,
+                                                                      long long rstride, O* __restrict__ out,
+                                                                      long long ostride, int nreal, int nblk_per_r,
+                                                                      double* __restrict__ part, Tw tw) {
   using C = cpx_t<R>;
-  using RC = RowCfg<R, LOGN>;
+  using RC = RowCfg<R, LOGN, V>;
   constexpr int N = RC::N, TX = RC::TX, PITCH = RC::PITCH, NTH = RC::NTH;
   constexpr int NW = NTH / 32;
   extern __shared__ __align__(16) unsigned char smraw[];
@@ -351,7 +359,7 @@ __global__ void __launch_bounds__(RowCfg<R, LOGN>::NTH) k_rows_c2r(Geo g, const 
     s[k * PITCH + t] = zk;
   }
   __syncthreads();
-  fft_rows_inv<R, LOGN>(s, stwN);
+  fft_rows_inv<R, LOGN, V>(s, stwN);
   // write x[0..nx) of each row: one warp per row, lanes along m; sums for the stats
   double s1 = 0.0, s2 = 0.0;
   O* dst = out + (long long)r * ostride;
@@ -612,60 +620,106 @@ static cudaError_t set_smem(K kernel, size_t bytes) {
 template <typename R> struct MaxL { static constexpr int v = MAX_LOGN_F; };
 template <> struct MaxL<double> { static constexpr int v = MAX_LOGN_D; };
 
-template <typename R, int L, int SIGN>
-static cudaError_t run_axis_c2c(const AxisArgs& a, const Geo& g, const cpx_t<R>* in, cpx_t<R>* out, Tw tw,
-                                cudaStream_t st) {
-  using CF = ColCfg<R, L>;
+template <typename R, int L, int SIGN, int V>
+static cudaError_t run_axis_c2c_v(const AxisArgs& a, const Geo& g, const cpx_t<R>* in, cpx_t<R>* out, Tw tw,
+                                  cudaStream_t st) {
+  using CF = ColCfg<R, L, V>;
   if constexpr (L == 0) {
     // length-1 transform: identity; copy when out-of-place
     if (in != out) return cudaErrorInvalidValue;
     return cudaSuccess;
   } else {
     size_t smem = (size_t)(CF::N * CF::TX + CF::N) * sizeof(cpx_t<R>);
-    cudaError_t e = set_smem(k_col<R, L, SIGN>, smem);
+    cudaError_t e = set_smem(k_col<R, L, SIGN, V>, smem);
     if (e != cudaSuccess) return e;
     AxisArgs b = a;
     b.tpg = (a.lines + CF::TX - 1) / CF::TX;
     unsigned blocks = (unsigned)((long long)b.tpg * a.ngroups * a.nreal);
-    k_col<R, L, SIGN><<<blocks, CF::NTH, smem, st>>>(b, g, in, out, tw);
+    k_col<R, L, SIGN, V><<<blocks, CF::NTH, smem, st>>>(b, g, in, out, tw);
     ++g_launch_count;
     return cudaGetLastError();
   }
+}
+
+template <typename R, int L, int V>
+static cudaError_t run_axis_gen_v(const AxisArgs& a, const Geo& g, const R* amp, const uint32_t* rs,
+                                  const uint32_t* apow, cpx_t<R>* out, Tw tw, cudaStream_t st) {
+  using CF = ColCfg<R, L, V>;
+  if constexpr (L == 0) {
+    return cudaErrorInvalidValue;
+  } else {
+    size_t smem = (size_t)(CF::N * CF::TX + CF::N) * sizeof(cpx_t<R>);
+    cudaError_t e = set_smem(k_colgen<R, L, V>, smem);
+    if (e != cudaSuccess) return e;
+    AxisArgs b = a;
+    b.tpg = (a.lines + CF::TX - 1) / CF::TX;
+    unsigned blocks = (unsigned)((long long)b.tpg * a.ngroups * a.nreal);
+    k_colgen<R, L, V><<<blocks, CF::NTH, smem, st>>>(b, g, amp, rs, apow, out, tw);
+    ++g_launch_count;
+    return cudaGetLastError();
+  }
+}
+
+template <typename R, typename O, int L, int V>
+static cudaError_t run_rows_c2r_v(const Geo& g, const cpx_t<R>* in, long long rstride, O* out, long long ostride,
+                                  int nreal, double* part, int* nblk_out, Tw tw, cudaStream_t st) {
+  using RC = RowCfg<R, L, V>;
+  constexpr int N = RC::N;
+  size_t smem = (size_t)((N + 1) * RC::PITCH + 3 * N) * sizeof(cpx_t<R>);
+  cudaError_t e = set_smem(k_rows_c2r<R, O, L, V>, smem);
+  if (e != cudaSuccess) return e;
+  int nblk = (g.ny * g.nz + RC::TX - 1) / RC::TX;
+  if (nblk_out) *nblk_out = nblk;
+  k_rows_c2r<R, O, L, V><<<(unsigned)((long long)nblk * nreal), RC::NTH, smem, st>>>(g, in, rstride, out, ostride,
+                                                                                     nreal, nblk, part, tw);
+  ++g_launch_count;
+  return cudaGetLastError();
+}
+
+// variants are compiled for transform lengths 32..1024; other lengths use variant 0
+constexpr bool tuned_len(int L) { return L >= 5 && L <= 10; }
+template <typename R> constexpr int prec_index() { return sizeof(R) == 4 ? 1 : 0; }
+
+template <typename R, int L, int SIGN>
+static cudaError_t run_axis_c2c(const AxisArgs& a, const Geo& g, const cpx_t<R>* in, cpx_t<R>* out, Tw tw,
+                                cudaStream_t st) {
+  if constexpr (tuned_len(L)) {
+    switch (g_variant[0][prec_index<R>()][L]) {
+      case 1: return run_axis_c2c_v<R, L, SIGN, 1>(a, g, in, out, tw, st);
+      case 2: return run_axis_c2c_v<R, L, SIGN, 2>(a, g, in, out, tw, st);
+      case 3: return run_axis_c2c_v<R, L, SIGN, 3>(a, g, in, out, tw, st);
+      default: break;
+    }
+  }
+  return run_axis_c2c_v<R, L, SIGN, 0>(a, g, in, out, tw, st);
 }
 
 template <typename R, int L>
 static cudaError_t run_axis_gen(const AxisArgs& a, const Geo& g, const R* amp, const uint32_t* rs,
                                 const uint32_t* apow, cpx_t<R>* out, Tw tw, cudaStream_t st) {
-  using CF = ColCfg<R, L>;
-  if constexpr (L == 0) {
-    return cudaErrorInvalidValue;
-  } else {
-    size_t smem = (size_t)(CF::N * CF::TX + CF::N) * sizeof(cpx_t<R>);
-    cudaError_t e = set_smem(k_colgen<R, L>, smem);
-    if (e != cudaSuccess) return e;
-    AxisArgs b = a;
-    b.tpg = (a.lines + CF::TX - 1) / CF::TX;
-    unsigned blocks = (unsigned)((long long)b.tpg * a.ngroups * a.nreal);
-    k_colgen<R, L><<<blocks, CF::NTH, smem, st>>>(b, g, amp, rs, apow, out, tw);
-    ++g_launch_count;
-    return cudaGetLastError();
+  if constexpr (tuned_len(L)) {
+    switch (g_variant[1][prec_index<R>()][L]) {
+      case 1: return run_axis_gen_v<R, L, 1>(a, g, amp, rs, apow, out, tw, st);
+      case 2: return run_axis_gen_v<R, L, 2>(a, g, amp, rs, apow, out, tw, st);
+      case 3: return run_axis_gen_v<R, L, 3>(a, g, amp, rs, apow, out, tw, st);
+      default: break;
+    }
   }
+  return run_axis_gen_v<R, L, 0>(a, g, amp, rs, apow, out, tw, st);
 }
 
 template <typename R, typename O, int L>
 static cudaError_t run_rows_c2r(const Geo& g, const cpx_t<R>* in, long long rstride, O* out, long long ostride,
                                 int nreal, double* part, int* nblk_out, Tw tw, cudaStream_t st) {
-  using RC = RowCfg<R, L>;
-  constexpr int N = RC::N;
-  size_t smem = (size_t)((N + 1) * RC::PITCH + 3 * N) * sizeof(cpx_t<R>);
-  cudaError_t e = set_smem(k_rows_c2r<R, O, L>, smem);
-  if (e != cudaSuccess) return e;
-  int nblk = (g.ny * g.nz + RC::TX - 1) / RC::TX;
-  if (nblk_out) *nblk_out = nblk;
-  k_rows_c2r<R, O, L><<<(unsigned)((long long)nblk * nreal), RC::NTH, smem, st>>>(g, in, rstride, out, ostride,
-                                                                                  nreal, nblk, part, tw);
-  ++g_launch_count;
-  return cudaGetLastError();
+  if constexpr (tuned_len(L)) {
+    switch (g_variant[2][prec_index<R>()][L]) {
+      case 1: return run_rows_c2r_v<R, O, L, 1>(g, in, rstride, out, ostride, nreal, part, nblk_out, tw, st);
+      case 2: return run_rows_c2r_v<R, O, L, 2>(g, in, rstride, out, ostride, nreal, part, nblk_out, tw, st);
+      case 3: return run_rows_c2r_v<R, O, L, 3>(g, in, rstride, out, ostride, nreal, part, nblk_out, tw, st);
+      default: break;
+    }
+  }
+  return run_rows_c2r_v<R, O, L, 0>(g, in, rstride, out, ostride, nreal, part, nblk_out, tw, st);
 }
 
 template <int L>
@@ -686,7 +740,8 @@ static cudaError_t run_spec_rows(const Model& m, const double d[3], const Geo& g
 int realize_part_blocks(const Geo& g, bool dbl) {
   if (g.npx == 1) return (g.ny * g.nz + NT - 1) / NT;
   int L = ilog2(g.npx) - 1;
-  int E = dbl ? 4096 : 8192;
+  int v = tuned_len(L) ? g_variant[2][dbl ? 0 : 1][L] : 0;
+  int E = (dbl ? 4096 : 8192) >> ((v >> 1) & 1);
   int tx = std::min(64, std::max(1, E >> L));
   return (g.ny * g.nz + tx - 1) / tx;
 }

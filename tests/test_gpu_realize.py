@@ -144,3 +144,22 @@ def test_golden_scaling_rms(gpu, n):
     res = sp.realize(c["seed"], 1, 0, gpu.FP64, dtype=np.float32)
     rms = recipes.scaling_rms(res[0])
     assert abs(rms - want["rms"]) <= 1e-9 * want["rms"], (rms, want["rms"])
+
+
+def test_tile_variants_give_identical_results(gpu):
+    """All tile variants run the same butterflies: outputs are bitwise identical."""
+    from specsim3d_b200 import _lib
+    L = _lib.lib()
+    n, sts, nug, d, ipad = CASES[0]                   # periodic 128 x 128 x 32
+    sp = gpu.Spectrum(sts, nug, d, n, ipad)
+    for prec in (gpu.FP32, gpu.FP64):
+        ref = sp.realize(77, 2, 1, prec)
+        for v in (1, 2, 3):
+            for kind, logn in ((0, 7), (1, 5), (2, 6)):
+                assert L.ss3d_set_variant(kind, prec, logn, v) == 0
+            assert np.array_equal(sp.realize(77, 2, 1, prec), ref)
+        for kind, logn in ((0, 7), (1, 5), (2, 6)):
+            L.ss3d_set_variant(kind, prec, logn, 0)
+    chosen = gpu.autotune(sp, 1, gpu.FP32, 2)
+    assert set(chosen.values()) <= {0, 1, 2, 3}
+    assert np.array_equal(sp.realize(77, 2, 1, gpu.FP32), sp.realize(77, 2, 1, gpu.FP32))
