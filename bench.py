@@ -221,9 +221,13 @@ def run_ours(args):
     k, w = max(1, args.steps), max(3, args.warmup)
     clk = ClockSampler(local)
     clk.start()
-    ms32, stages, launches = timed(ss.FP32, out32, k, w, prof=True)
+    ms32, _, launches = timed(ss.FP32, out32, k, w)
     clocks = clk.stop()
     ms64, _, _ = timed(ss.FP64, out64, max(1, k // 2), 3)
+    # per-kernel durations for the roofline: a separate pass with stage events
+    # (stages then run back to back instead of overlapped across realizations)
+    _, stages, _ = timed(ss.FP32, out32, max(1, k // 2), 1, prof=True)
+    kprof = max(1, k // 2)
     # precision-form error against the FP64 path on the same realizations
     step(ss.FP64, out64)
     step(ss.FP32, out32)
@@ -293,7 +297,7 @@ def run_ours(args):
                 "h2d_bytes_per_step": 0, "d2h_bytes_per_step": int(M * nreal * 4),
                 "includes": "spectrum build + realizations + D2H into pinned host memory"},
         "gpu_launches": int(launches),
-        "stages_ms_per_step": {kk: round(v[0] / k, 4) for kk, v in stages.items()},
+        "stages_ms_per_step_serialized": {kk: round(v[0] / kprof, 4) for kk, v in stages.items()},
         "roofline": {"bound": "hbm", "achieved": round(achieved, 1), "peak": peak, "unit": "GB/s",
                      "frac": round(achieved / peak, 4), "traffic": traffic,
                      "kernel": "k_colgen<float,9> (synthesis + z inverse pass)",
