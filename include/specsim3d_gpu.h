@@ -16,9 +16,10 @@
  *     C order [nreal][nz][ny][nx].
  *   - Output and in/out arrays may be host or device pointers; the library
  *     detects which.  The library owns device memory behind opaque handles.
- *   - Handles are thread-compatible, not thread-safe.  Work is issued on the
- *     stream set with ss3d_set_stream (default: the legacy default stream) and
- *     every call returns after its results are complete.
+ *   - A spectrum handle is read-only after creation: several host threads may
+ *     call ss3d_realize on it at once, each on its own stream (set per thread
+ *     with ss3d_set_stream; default: the legacy default stream).  Every call
+ *     returns after its results are complete.
  */
 #ifndef SPECSIM3D_GPU_H
 #define SPECSIM3D_GPU_H
@@ -202,9 +203,17 @@ int ss3d_condition(double *res, const int n[3], int nreal, const double xmin[3],
 
 /* ---------------------------------------------------------------- runtime */
 
-/* Stream (a cudaStream_t passed as void*) on which later calls issue work;
- * NULL selects the legacy default stream. */
+/* Stream (a cudaStream_t passed as void*) on which later calls from the
+ * calling host thread issue work; NULL selects the legacy default stream. */
 int ss3d_set_stream(void *stream);
+
+/* The realization work space is kept per host thread and device and grows on
+ * demand.  ss3d_realize_workspace_bytes gives the device bytes a call of nreal
+ * realizations needs (host_out: 1 for a host output array), for admission
+ * control; -1 on invalid arguments.  ss3d_release_workspace frees the calling
+ * thread's work space. */
+int64_t ss3d_realize_workspace_bytes(const ss3d_spectrum *sp, int nreal, int precision, int host_out);
+int ss3d_release_workspace(void);
 
 /* Message of the last failing call on this thread ("" if none). */
 const char *ss3d_last_error(void);

@@ -24,6 +24,7 @@ EXPORTS = (
     "ss3d_realize", "ss3d_debug_states", "ss3d_debug_coefficients",
     "ss3d_vario", "ss3d_condition",
     "ss3d_set_stream", "ss3d_last_error", "ss3d_version", "ss3d_profile", "ss3d_profile_read", "ss3d_autotune", "ss3d_set_variant",
+    "ss3d_realize_workspace_bytes", "ss3d_release_workspace",
 )
 
 
@@ -98,6 +99,8 @@ def lib():
         "ss3d_profile_read": (I, [P, P, P]),
         "ss3d_autotune": (I, [P, I, I, I, P]),
         "ss3d_set_variant": (I, [I, I, I, I]),
+        "ss3d_realize_workspace_bytes": (I64, [P, I, I, I]),
+        "ss3d_release_workspace": (I, []),
     }
     for name, (res, args) in sig.items():
         f = getattr(L, name)

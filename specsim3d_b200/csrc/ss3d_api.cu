@@ -3,6 +3,7 @@
 // tables), spectrum handles, realization batching with host/device output.
 #include <cuda_runtime.h>
 
+#include <algorithm>
 #include <cmath>
 #include <cstdarg>
 #include <cstdio>
@@ -19,7 +20,8 @@ using namespace ss3d;
 
 // ---------------------------------------------------------------- errors and stream
 static thread_local std::string g_err;
-static cudaStream_t g_stream = 0;
+// stream of the calling host thread (ss3d_set_stream)
+static thread_local cudaStream_t g_stream = 0;
 
 static int fail(int code, const char* fmt, ...) {
   char buf[1024];
@@ -296,9 +298,6 @@ struct ss3d_spectrum {
   ss3d_spec_stats stats;
   double* amp64 = nullptr;
   float* amp32 = nullptr;
-  // cached workspace of the realization path
-  void* ws = nullptr;
-  size_t ws_bytes = 0;
 };
 
 namespace {
@@ -310,15 +309,38 @@ int supported_axes(const Geo& g, bool dbl, const char** which) {
   return 1;
 }
 
-int ws_reserve(ss3d_spectrum* sp, size_t bytes) {
-  if (sp->ws_bytes >= bytes) return SS3D_OK;
-  if (sp->ws) {
-    cudaFree(sp->ws);
-    sp->ws = nullptr;
-    sp->ws_bytes = 0;
+// Work space of the realization path, kept per host thread and device so that
+// threads realizing at the same time on their own streams never share it.
+// It grows on demand; every call finishes its work before it returns.
+struct Workspace {
+  void* p = nullptr;
+  size_t bytes = 0;
+  int dev = 0;
+  void release() {
+    if (p) {
+      int cur = 0;
+      cudaGetDevice(&cur);
+      cudaSetDevice(dev);
+      cudaFree(p);
+      cudaSetDevice(cur);
+    }
+    p = nullptr;
+    bytes = 0;
   }
-  CK(cudaMalloc(&sp->ws, bytes));
-  sp->ws_bytes = bytes;
+  ~Workspace() { release(); }
+};
+thread_local Workspace g_ws[64];
+
+int ws_reserve(int dev, size_t bytes, void** ptr) {
+  if (dev < 0 || dev >= 64) return fail(SS3D_EINVAL, "device ordinal %d out of range", dev);
+  Workspace& w = g_ws[dev];
+  if (w.bytes < bytes) {
+    w.release();
+    CK(cudaMalloc(&w.p, bytes));
+    w.bytes = bytes;
+    w.dev = dev;
+  }
+  *ptr = w.p;
   return SS3D_OK;
 }
 
@@ -399,7 +421,6 @@ extern "C" void ss3d_spectrum_free(ss3d_spectrum* sp) {
   cudaSetDevice(sp->dev);
   if (sp->amp64) cudaFree(sp->amp64);
   if (sp->amp32) cudaFree(sp->amp32);
-  if (sp->ws) cudaFree(sp->ws);
   cudaSetDevice(cur);
   delete sp;
 }
@@ -423,7 +444,7 @@ extern "C" int ss3d_spectrum_info(const ss3d_spectrum* sp, int np[3], int n[3], 
 extern "C" int64_t ss3d_spectrum_bytes(const ss3d_spectrum* sp) {
   if (!sp) return 0;
   const size_t nh = (size_t)sp->geo.npz * sp->geo.npy * sp->geo.HP;
-  return (int64_t)(nh * (sizeof(double) + sizeof(float)) + sp->ws_bytes);
+  return (int64_t)(nh * (sizeof(double) + sizeof(float)));
 }
 
 extern "C" int ss3d_spectrum_amp(const ss3d_spectrum* sp, double* amp) {
@@ -451,6 +472,46 @@ uint32_t seed0(int iseed) {
 }
 }  // namespace
 
+namespace {
+// Work-space layout of one realize call: batches of at most 16 realizations
+// and about 8 GiB; host output goes through two staging buffers.
+struct RealizeLayout {
+  int bt;
+  size_t per_work, off_work, off_rs, off_apow, off_part, off_zs, off_stage, stage_bytes, total;
+};
+RealizeLayout realize_layout(const Geo& g, bool dbl, bool dev_out, int nreal, size_t oel) {
+  RealizeLayout L{};
+  const size_t M = (size_t)g.nx * g.ny * g.nz;
+  const size_t cel = dbl ? sizeof(double2) : sizeof(float2);
+  L.per_work = (size_t)g.npz * g.npy * g.HP * cel;
+  const int nbx = realize_part_blocks(g, dbl);
+  const size_t budget = (size_t)8 << 30;
+  const size_t per_real = L.per_work + (dev_out ? 0 : 2 * M * oel) + (size_t)g.npy * g.npz * 4 + (size_t)nbx * 16;
+  L.bt = (int)std::min<size_t>((size_t)std::max(nreal, 1), std::max<size_t>(1, budget / per_real));
+  L.bt = std::min(L.bt, 16);
+  L.off_work = 0;
+  L.off_rs = align256(L.off_work + L.per_work * L.bt);
+  L.off_apow = align256(L.off_rs + (size_t)g.npy * g.npz * 4 * L.bt);
+  L.off_part = align256(L.off_apow + (size_t)g.npx * 4);
+  L.off_zs = align256(L.off_part + (size_t)nbx * 16 * L.bt);
+  L.off_stage = align256(L.off_zs + (size_t)std::max(nreal, 1) * 16);
+  L.stage_bytes = dev_out ? 0 : align256(M * oel * L.bt);
+  L.total = L.off_stage + 2 * L.stage_bytes;
+  return L;
+}
+}  // namespace
+
+extern "C" int64_t ss3d_realize_workspace_bytes(const ss3d_spectrum* sp, int nreal, int precision, int host_out) {
+  if (!sp || nreal < 0 || (precision != SS3D_FP64 && precision != SS3D_FP32)) return -1;
+  const bool dbl = precision == SS3D_FP64;
+  return (int64_t)realize_layout(sp->geo, dbl, host_out == 0, nreal, dbl ? 8 : 4).total;
+}
+
+extern "C" int ss3d_release_workspace(void) {
+  for (Workspace& w : g_ws) w.release();
+  return SS3D_OK;
+}
+
 extern "C" int ss3d_realize(const ss3d_spectrum* csp, int iseed, int64_t r_first, int nreal, int igauss,
                             int precision, void* out, int out_dtype, double* zstats) {
   ss3d_spectrum* sp = const_cast<ss3d_spectrum*>(csp);
@@ -475,29 +536,17 @@ extern "C" int ss3d_realize(const ss3d_spectrum* csp, int iseed, int64_t r_first
   const bool dev_out = is_device_ptr(out);
   const size_t M = (size_t)g.nx * g.ny * g.nz;
   const size_t oel = out_dtype == SS3D_OUT_F32 ? 4 : 8;
-  const size_t cel = dbl ? sizeof(double2) : sizeof(float2);
-  const size_t per_work = (size_t)g.npz * g.npy * g.HP * cel;
-  const int nbx = realize_part_blocks(g, dbl);
-  // batch: at most 16 realizations and about 8 GiB of work space
-  size_t budget = (size_t)8 << 30;
-  size_t per_real = per_work + (dev_out ? 0 : 2 * M * oel) + (size_t)g.npy * g.npz * 4 + (size_t)nbx * 16;
-  int bt = (int)std::min<size_t>((size_t)nreal, std::max<size_t>(1, budget / per_real));
-  bt = std::min(bt, 16);
-  size_t off_work = 0;
-  size_t off_rs = align256(off_work + per_work * bt);
-  size_t off_apow = align256(off_rs + (size_t)g.npy * g.npz * 4 * bt);
-  size_t off_part = align256(off_apow + (size_t)g.npx * 4);
-  size_t off_zs = align256(off_part + (size_t)nbx * 16 * bt);
-  size_t off_stage = align256(off_zs + (size_t)nreal * 16);
-  size_t total = off_stage + (dev_out ? 0 : 2 * align256(M * oel * bt));
-  if ((rc = ws_reserve(sp, total))) return rc;
-  char* base = (char*)sp->ws;
-  void* work = base + off_work;
-  uint32_t* rs = (uint32_t*)(base + off_rs);
-  uint32_t* apow = (uint32_t*)(base + off_apow);
-  double* part = (double*)(base + off_part);
-  double* zs = (double*)(base + off_zs);
-  char* stage[2] = {base + off_stage, base + off_stage + align256(M * oel * bt)};
+  const RealizeLayout lay = realize_layout(g, dbl, dev_out, nreal, oel);
+  const int bt = lay.bt;
+  void* wsp = nullptr;
+  if ((rc = ws_reserve(sp->dev, lay.total, &wsp))) return rc;
+  char* base = (char*)wsp;
+  void* work = base + lay.off_work;
+  uint32_t* rs = (uint32_t*)(base + lay.off_rs);
+  uint32_t* apow = (uint32_t*)(base + lay.off_apow);
+  double* part = (double*)(base + lay.off_part);
+  double* zs = (double*)(base + lay.off_zs);
+  char* stage[2] = {base + lay.off_stage, base + lay.off_stage + lay.stage_bytes};
   const long long wstride = (long long)g.npz * g.npy * g.HP;
   const uint32_t s0 = seed0(iseed);
   Tw tw{ctx->twf, ctx->twd};

@@ -1,0 +1,299 @@
+// ss3d_bodies.cuh -- bodies of the three realization passes as device
+// functions of a work-item index, shared by the per-pass kernels (one CTA per
+// item, ss3d_fft.cu) and the batch kernels (CTAs over the items of many grids,
+// ss3d_batch.cu).
+//
+//   colgen_body  synthesis of the Hermitian coefficients (reference fill
+//                f90:1305-1334) fused with the first inverse axis pass
+//   col_body     inverse pass along a strided axis, pruned to the crop
+//   rows_body    C2R pass along x with the crop (f90:1335-1340)
+#pragma once
+#include "ss3d_engine.cuh"
+#include "ss3d_internal.h"
+
+namespace ss3d {
+
+template <typename R> __device__ __forceinline__ const cpx_t<R>* twtab(const Tw& tw);
+template <> __device__ __forceinline__ const float2* twtab<float>(const Tw& tw) { return tw.f; }
+template <> __device__ __forceinline__ const double2* twtab<double>(const Tw& tw) { return tw.d; }
+
+// ---------------------------------------------------------------- strided axis passes
+// A "line" is one column along the transformed axis.  Lines of one group are
+// contiguous in memory; groups are gstride apart; realizations rstride apart.
+struct AxisArgs {
+  long long S;         // element stride along the axis
+  int nout;            // positions stored (p < nout)
+  int lines;           // lines per group
+  int ngroups;
+  long long gstride;
+  int tpg;             // tiles per group
+  long long rstride;   // realization stride in the complex buffer
+  int nreal;
+  int axis;            // 1 = y, 2 = z (index decoding of the synthesis)
+};
+
+__device__ __forceinline__ bool line_valid(const Geo& g, int line, int lines) {
+  return line < lines && (line % g.HP) < g.H;
+}
+
+// ---------------------------------------------------------------- register-resident column passes
+// Tile configuration per transform length: TX columns, TPC threads per column,
+// ET = N / TPC elements per thread (16 in float, 8 in double).
+// Variant V (tuned at run time): bit 0 halves the elements per thread
+// (more threads, fewer registers), bit 1 halves the tile (fewer columns).
+template <typename R, int LOGN, int V = 0> struct ColCfg {
+  static constexpr int N = 1 << LOGN;
+  static constexpr int ETW0 = sizeof(R) == 4 ? 16 : 8;
+  static constexpr int ETW = (V & 1) ? (ETW0 / 2 < 8 ? 8 : ETW0 / 2) : ETW0;
+  static constexpr int ET = N < ETW ? N : ETW;
+  static constexpr int TPC = N / ET;
+  static constexpr int E = (sizeof(R) == 4 ? 8192 : 4096) >> ((V >> 1) & 1);
+  static constexpr int TX0 = E / N;
+  static constexpr int TX = TX0 > 64 ? 64 : (TX0 < 2 ? 2 : TX0);
+  static constexpr int NTH = TX * TPC;
+  static_assert(NTH <= 1024, "tile too large");
+};
+
+// c2c transform along a strided axis (in place allowed), unscaled, pruned store
+template <typename R, int LOGN, int TX, int TPC, int SIGN>
+__device__ __forceinline__ void col_body(const AxisArgs& a, const Geo& g, const cpx_t<R>* in, cpx_t<R>* out,
+                                         const Tw& tw, int item, unsigned char* smraw) {
+  using C = cpx_t<R>;
+  constexpr int N = 1 << LOGN;
+  constexpr int NTH = TX * TPC;
+  C* s = reinterpret_cast<C*>(smraw);
+  C* stw = s + N * TX;
+  const int r = item % a.nreal;
+  const int tile = item / a.nreal;
+  const int grp = tile / a.tpg;
+  const int line0 = (tile % a.tpg) * TX;
+  const int t = threadIdx.x % TX;
+  const bool valid = line_valid(g, line0 + t, a.lines);
+  const C* src = in + ((long long)grp * a.gstride + line0 + t + (long long)r * a.rstride);
+  C* dst = out + ((long long)grp * a.gstride + line0 + t + (long long)r * a.rstride);
+  const int S = (int)a.S;   // offsets inside one realization's grid fit in 32 bits
+  const int nout = a.nout;
+  for (int q = threadIdx.x; q < N; q += NTH) stw[q] = twtab<R>(tw)[N - 1 + q];
+  __syncthreads();
+  fft_tile<LOGN, TX, TPC, SIGN>(
+      s, stw, [&](int pos) { return valid ? src[pos * S] : cmk<C>(R(0), R(0)); },
+      [&](int pos, C v) {
+        if (valid && pos < nout) dst[pos * S] = v;
+      });
+}
+
+// First inverse pass with the coefficient synthesis fused into the loader.
+// axis 2: columns are (i, j) plane offsets, positions k;  axis 1 (npz = 1):
+// columns are i, positions j.
+template <typename R, int LOGN, int TX, int TPC>
+__device__ __forceinline__ void colgen_body(const AxisArgs& a, const Geo& g, const R* __restrict__ amp,
+                                            const uint32_t* __restrict__ rowstates,
+                                            const uint32_t* __restrict__ apow, cpx_t<R>* out, const Tw& tw,
+                                            int item, unsigned char* smraw) {
+  using C = cpx_t<R>;
+  constexpr int N = 1 << LOGN;
+  constexpr int NTH = TX * TPC;
+  C* s = reinterpret_cast<C*>(smraw);
+  C* stw = s + N * TX;
+  const int r = item % a.nreal;
+  const int tile = item / a.nreal;
+  const int grp = tile / a.tpg;
+  const int line0 = (tile % a.tpg) * TX;
+  const int t = threadIdx.x % TX;
+  const int line = line0 + t;
+  const bool valid = line_valid(g, line, a.lines);
+  int i, j0;
+  if (a.axis == 2) {
+    i = line % g.HP;
+    j0 = line / g.HP;
+  } else {
+    i = line;
+    j0 = 0;
+  }
+  if (!valid) i = 0;
+  const uint32_t ai = __ldg(apow + i), aip = __ldg(apow + ((g.npx - i) & (g.npx - 1)));
+  const bool iedge = (i == 0) || (2 * i == g.npx);
+  const uint32_t* rs = rowstates + (size_t)r * g.npy * g.npz;
+  const long long cbase = (long long)grp * a.gstride + line;
+  const R* ap = amp + cbase;
+  C* dst = out + cbase + (long long)r * a.rstride;
+  const int S = (int)a.S;   // offsets inside one realization's grid fit in 32 bits
+  const int nout = a.nout;
+  const bool zaxis = a.axis == 2;
+  for (int q = threadIdx.x; q < N; q += NTH) stw[q] = twtab<R>(tw)[N - 1 + q];
+  __syncthreads();
+  fft_tile<LOGN, TX, TPC, +1>(
+      s, stw,
+      [&](int pos) {
+        if (!valid) return cmk<C>(R(0), R(0));
+        const R am = __ldg(ap + pos * S);
+        return zaxis ? coef_col<R>(g, j0, pos, am, rs, ai, aip, iedge)
+                     : coef_col<R>(g, pos, grp, am, rs, ai, aip, iedge);
+      },
+      [&](int pos, C v) {
+        if (valid && pos < nout) dst[pos * S] = v;
+      });
+}
+
+// ---------------------------------------------------------------- block reduction helpers
+template <int NTH>
+__device__ __forceinline__ void block_sum2(double& a, double& b) {
+  __shared__ double red[2][NTH / 32];
+#pragma unroll
+  for (int off = 16; off > 0; off >>= 1) {
+    a += __shfl_down_sync(0xffffffffu, a, off);
+    b += __shfl_down_sync(0xffffffffu, b, off);
+  }
+  __syncthreads();
+  if ((threadIdx.x & 31) == 0) {
+    red[0][threadIdx.x >> 5] = a;
+    red[1][threadIdx.x >> 5] = b;
+  }
+  __syncthreads();
+  if (threadIdx.x == 0) {
+    double s1 = 0, s2 = 0;
+    for (int w = 0; w < NTH / 32; ++w) {
+      s1 += red[0][w];
+      s2 += red[1][w];
+    }
+    a = s1;
+    b = s2;
+  }
+}
+
+// ---------------------------------------------------------------- x pass: C2R + crop
+// Row (j,k) of the half spectrum (N+1 values) -> npx = 2N reals, of which the
+// first nx go to out[r][k][j][:].  Packing for a length-N inverse FFT:
+//   Z[q] = (X[q] + conj X[N-q]) + i w^q (X[q] - conj X[N-q]),  w = e^{+2 pi i/(2N)}
+// then x[2m] = Re z[m], x[2m+1] = Im z[m].  The imaginary parts of X[0] and
+// X[N] are dropped: the reference keeps the real part of the full complex
+// inverse (f90:1339), which does not see them.
+template <typename R, int LOGN, int V = 0> struct RowCfg {
+  using CF = ColCfg<R, LOGN, V>;
+  static constexpr int N = CF::N, TPC = CF::TPC, ET = CF::ET;
+  static constexpr int TX0 = CF::E / N;
+  static constexpr int TX = TX0 > 64 ? 64 : (TX0 < 1 ? 1 : TX0);
+  static constexpr int NTH0 = TX * TPC;
+  static constexpr int NTH = NTH0 < 32 ? 32 : NTH0;
+  static constexpr int PITCH = TX + 1;
+};
+
+// inverse length-N FFT of the TX rows staged in s (pitch TX+1), in place;
+// twN holds e^{-2 pi i m/N}, m < N
+template <typename R, int LOGN, int TX, int TPC>
+__device__ __forceinline__ void fft_rows_inv(cpx_t<R>* s, const cpx_t<R>* twN) {
+  using C = cpx_t<R>;
+  constexpr int PITCH = TX + 1;
+  static_assert(TX * TPC >= 32, "row tile needs at least one warp");
+  if constexpr (LOGN > 0) {
+    const int t = threadIdx.x % TX;
+    fft_tile<LOGN, TX, TPC, +1, PITCH, true, true>(
+        s, twN, [&](int pos) { return s[pos * PITCH + t]; }, [&](int pos, C v) { s[pos * PITCH + t] = v; });
+    __syncthreads();
+  }
+}
+
+// part (may be NULL): per-block sums of x and x^2 for the mean/variance line
+template <typename R, typename O, int LOGN, int TX, int TPC>
+__device__ __forceinline__ void rows_body(const Geo& g, const cpx_t<R>* __restrict__ in, long long rstride,
+                                          O* __restrict__ out, long long ostride, int nreal, int nblk_per_r,
+                                          double* __restrict__ part, const Tw& tw, int item, unsigned char* smraw) {
+  using C = cpx_t<R>;
+  constexpr int N = 1 << LOGN, PITCH = TX + 1, NTH = TX * TPC;
+  constexpr int NW = NTH / 32;
+  C* s = reinterpret_cast<C*>(smraw);   // [N+1][PITCH]
+  C* stw = s + (N + 1) * PITCH;         // 2N entries e^{-2 pi i m/(2N)}
+  C* stwN = stw + 2 * N;                // N entries e^{-2 pi i m/N}
+  const int r = item % nreal;
+  const int blk = item / nreal;
+  const int nrows = g.ny * g.nz;
+  const int row0 = blk * TX;
+  const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
+  for (int q = threadIdx.x; q < 2 * N; q += NTH) stw[q] = twtab<R>(tw)[2 * N - 1 + q];
+  for (int q = threadIdx.x; q < N; q += NTH) stwN[q] = twtab<R>(tw)[N - 1 + q];
+  const C* src = in + (long long)r * rstride;
+  // stage rows: one warp per row, lanes along the row (coalesced)
+  for (int t = warp; t < TX; t += NW) {
+    const int row = row0 + t;
+    const bool ok = row < nrows;
+    const int j = ok ? row % g.ny : 0, k = ok ? row / g.ny : 0;
+    const C* rp = src + ((long long)k * g.npy + j) * g.HP;
+    constexpr int NIT = (N + 1 + 31) / 32;
+    C tmp[NIT];
+#pragma unroll
+    for (int it = 0; it < NIT; ++it) {
+      const int p = lane + 32 * it;
+      tmp[it] = (ok && p <= N) ? rp[p] : cmk<C>(R(0), R(0));
+    }
+#pragma unroll
+    for (int it = 0; it < NIT; ++it) {
+      const int p = lane + 32 * it;
+      if (p <= N) s[p * PITCH + t] = tmp[it];
+    }
+  }
+  __syncthreads();
+  // packing Z[q] from X[q], X[N-q], in place over the pairs (q, N-q)
+  for (int q = threadIdx.x; q < (N / 2 + 1) * TX; q += NTH) {
+    const int t = q % TX, k = q / TX;
+    const int kc = N - k;
+    C a = s[k * PITCH + t], b = s[kc * PITCH + t];
+    if (k == 0) {
+      a.y = R(0);
+      b.y = R(0);
+    }
+    C w = stw[k];
+    w.y = -w.y;
+    const C bc = cmk<C>(b.x, -b.y);
+    const C zk = cadd(cadd(a, bc), cmul_si<+1>(cmul(w, csub(a, bc))));
+    if (k != 0 && kc != k) {
+      C w2 = stw[kc];
+      w2.y = -w2.y;
+      const C ac = cmk<C>(a.x, -a.y);
+      s[kc * PITCH + t] = cadd(cadd(b, ac), cmul_si<+1>(cmul(w2, csub(b, ac))));
+    }
+    s[k * PITCH + t] = zk;
+  }
+  __syncthreads();
+  fft_rows_inv<R, LOGN, TX, TPC>(s, stwN);
+  // write x[0..nx) of each row: one warp per row, lanes along m; sums for the stats
+  double s1 = 0.0, s2 = 0.0;
+  O* dst = out + (long long)r * ostride;
+  const int nxh = (g.nx + 1) / 2;
+  const bool even = (g.nx & 1) == 0;
+  for (int t = warp; t < TX; t += NW) {
+    const int row = row0 + t;
+    if (row >= nrows) break;
+    O* rp = dst + (long long)row * g.nx;
+    for (int m = lane; m < nxh; m += 32) {
+      const C z = s[m * PITCH + t];
+      const O a0 = (O)z.x, a1 = (O)z.y;
+      s1 += (double)z.x;
+      s2 += (double)z.x * (double)z.x;
+      if (even) {
+        if constexpr (sizeof(O) == 4) {
+          reinterpret_cast<float2*>(rp)[m] = make_float2((float)a0, (float)a1);
+        } else {
+          reinterpret_cast<double2*>(rp)[m] = make_double2((double)a0, (double)a1);
+        }
+        s1 += (double)z.y;
+        s2 += (double)z.y * (double)z.y;
+      } else {
+        rp[2 * m] = a0;
+        if (2 * m + 1 < g.nx) {
+          rp[2 * m + 1] = a1;
+          s1 += (double)z.y;
+          s2 += (double)z.y * (double)z.y;
+        }
+      }
+    }
+  }
+  if (part) {
+    block_sum2<NTH>(s1, s2);
+    if (threadIdx.x == 0) {
+      part[2 * ((long long)r * nblk_per_r + blk)] = s1;
+      part[2 * ((long long)r * nblk_per_r + blk) + 1] = s2;
+    }
+  }
+}
+
+}  // namespace ss3d
