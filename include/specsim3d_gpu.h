@@ -152,6 +152,49 @@ int ss3d_autotune(const ss3d_spectrum *sp, int igauss, int precision, int nreal,
  * computes the same values; they differ in tile shape only. */
 int ss3d_set_variant(int kind, int precision, int logn, int variant);
 
+/* ---------------------------------------------------------------- batched form */
+
+/* Many realizations of many grids in one CUDA-graph launch (FP32 synthesis and
+ * transforms, float output).  A job asks for realizations r_first ..
+ * r_first+nreal-1 of one spectrum into a DEVICE array out[nreal][nz][ny][nx];
+ * each result equals ss3d_realize(sp, iseed, r_first, nreal, igauss,
+ * SS3D_FP32, out, SS3D_OUT_F32, NULL) bit for bit.  The batch owns its work
+ * space (the complex grids of every job) and replays one graph on each run;
+ * the spectra and output arrays must outlive it.  The reference simulates one
+ * grid per process (its realization loop, f90:1300-1345); this form has no
+ * counterpart there. */
+typedef struct ss3d_batch ss3d_batch;
+typedef struct ss3d_batch_job {
+    const ss3d_spectrum *sp;
+    int iseed;
+    int igauss;
+    int64_t r_first;
+    int nreal;
+    float *out;
+} ss3d_batch_job;
+
+int ss3d_batch_create(const ss3d_batch_job *jobs, int njobs, ss3d_batch **out);
+/* One graph launch on the calling thread's stream; returns when done. */
+int ss3d_batch_run(ss3d_batch *b);
+/* Times the schedules and tile variants, keeps the fastest and re-captures the
+ * graph; results do not change. */
+int ss3d_batch_autotune(ss3d_batch *b);
+/* Output cells of one run, kernel launches of one run, and for the persistent
+ * schedule its CTAs and work items per pass (all outputs may be NULL). */
+int ss3d_batch_info(const ss3d_batch *b, int64_t *cells, int grid[3], int items[3], int *kernels);
+/* One run timed with CUDA events outside the graph: ms[0..2] the synthesis,
+ * middle and row passes (persistent schedule; -1 for chains), ms[3] the run. */
+int ss3d_batch_time(ss3d_batch *b, float ms[4]);
+/* Schedule: sched 0 chains (one chain of per-call kernels per job on parallel
+ * graph branches), 1 persistent (three kernels over one work list of every
+ * job's tiles; needs periodic axes of 16..1024 nodes and npx >= 16).  For the
+ * persistent schedule per pass: tile variant etv (0: 16, 1: 8 elements per
+ * thread), mode (0 strided items, 1 contiguous items, 2 one CTA per item) and
+ * CTAs per SM (0: occupancy limit). */
+int ss3d_batch_schedule(const ss3d_batch *b, int *sched, int etv[3], int mode[3], int cps[3]);
+int ss3d_batch_set_schedule(ss3d_batch *b, int sched, int pass, int etv, int mode, int cps);
+void ss3d_batch_free(ss3d_batch *b);
+
 /* ---------------------------------------------------------------- variogram */
 
 /* Experimental semivariograms of nreal fields res(nx,ny,nz,nreal) (FP64, host or

@@ -178,6 +178,81 @@ class Spectrum:
         return c[..., 0] + 1j * c[..., 1]
 
 
+class Batch:
+    """Many realizations of many grids in one CUDA-graph launch (FP32).
+
+    jobs: iterable of (spectrum, iseed, igauss, r_first, nreal, out), ``out`` a
+    contiguous float32 torch CUDA tensor of nreal * nz * ny * nx elements.
+    Each run writes every job's realizations; each equals
+    ``spectrum.realize(iseed, nreal, igauss, FP32, r_first, dtype=float32)``
+    bit for bit."""
+
+    CHAINS, PERSISTENT = 0, 1
+
+    def __init__(self, jobs, autotune=False):
+        jobs = list(jobs)
+        arr = (L.BatchJob * len(jobs))()
+        self._keep = []
+        for a, (sp, iseed, igauss, r_first, nreal, out) in zip(arr, jobs):
+            nx, ny, nz = sp.n
+            if out.numel() != int(nreal) * nx * ny * nz:
+                raise ValueError("output tensor has the wrong size")
+            ptr, code = _out_ptr(out)
+            if code != OUT_F32 or not out.is_cuda:
+                raise ValueError("batch outputs must be float32 CUDA tensors")
+            a.sp = sp.handle.value
+            a.iseed, a.igauss, a.r_first, a.nreal, a.out = int(iseed), int(igauss), int(r_first), int(nreal), ptr.value
+            self._keep.append((sp, out))
+        h = ctypes.c_void_p()
+        L.check(L.lib().ss3d_batch_create(arr, len(jobs), ctypes.byref(h)))
+        self._h = h
+        if autotune:
+            self.autotune()
+
+    def run(self):
+        L.check(L.lib().ss3d_batch_run(self._h))
+
+    def autotune(self):
+        L.check(L.lib().ss3d_batch_autotune(self._h))
+
+    def info(self):
+        cells = ctypes.c_int64()
+        grid = (ctypes.c_int * 3)()
+        items = (ctypes.c_int * 3)()
+        kern = ctypes.c_int()
+        L.check(L.lib().ss3d_batch_info(self._h, ctypes.byref(cells), grid, items, ctypes.byref(kern)))
+        return {"cells": int(cells.value), "grid": list(grid), "items": list(items), "kernels": int(kern.value)}
+
+    def time(self):
+        """One run timed outside the graph: [synthesis, middle, rows, whole] ms."""
+        ms = (ctypes.c_float * 4)()
+        L.check(L.lib().ss3d_batch_time(self._h, ms))
+        return [float(v) for v in ms]
+
+    def schedule(self):
+        sched = ctypes.c_int()
+        etv, mode, cps = ((ctypes.c_int * 3)() for _ in range(3))
+        L.check(L.lib().ss3d_batch_schedule(self._h, ctypes.byref(sched), etv, mode, cps))
+        return {"schedule": "persistent" if sched.value == 1 else "chains",
+                "elements_per_thread": [16 if v == 0 else 8 for v in etv], "mode": list(mode),
+                "ctas_per_sm": list(cps)}
+
+    def set_schedule(self, sched, pass_=0, elements_per_thread=8, mode=2, ctas_per_sm=0):
+        L.check(L.lib().ss3d_batch_set_schedule(self._h, int(sched), int(pass_),
+                                                0 if elements_per_thread == 16 else 1, int(mode), int(ctas_per_sm)))
+
+    def close(self):
+        if self._h:
+            L.lib().ss3d_batch_free(self._h)
+            self._h = None
+
+    def __del__(self):
+        try:
+            self.close()
+        except Exception:
+            pass
+
+
 def vario(res, dirs):
     """Experimental variograms (f90:394-480).
 

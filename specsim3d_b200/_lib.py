@@ -25,6 +25,8 @@ EXPORTS = (
     "ss3d_vario", "ss3d_condition",
     "ss3d_set_stream", "ss3d_last_error", "ss3d_version", "ss3d_profile", "ss3d_profile_read", "ss3d_autotune", "ss3d_set_variant",
     "ss3d_realize_workspace_bytes", "ss3d_release_workspace",
+    "ss3d_batch_create", "ss3d_batch_run", "ss3d_batch_autotune", "ss3d_batch_info", "ss3d_batch_time",
+    "ss3d_batch_schedule", "ss3d_batch_set_schedule", "ss3d_batch_free",
 )
 
 
@@ -44,6 +46,12 @@ class Struct(ctypes.Structure):
 class SpecStats(ctypes.Structure):
     _fields_ = [("np", ctypes.c_int * 3), ("c0", ctypes.c_double), ("maximag", ctypes.c_double),
                 ("maxreal", ctypes.c_double), ("spos", ctypes.c_double), ("sneg", ctypes.c_double)]
+
+
+class BatchJob(ctypes.Structure):
+    """ss3d_batch_job: realizations r_first.. of one spectrum into a device array."""
+    _fields_ = [("sp", ctypes.c_void_p), ("iseed", ctypes.c_int), ("igauss", ctypes.c_int),
+                ("r_first", ctypes.c_int64), ("nreal", ctypes.c_int), ("out", ctypes.c_void_p)]
 
 
 class CondParams(ctypes.Structure):
@@ -101,6 +109,14 @@ def lib():
         "ss3d_set_variant": (I, [I, I, I, I]),
         "ss3d_realize_workspace_bytes": (I64, [P, I, I, I]),
         "ss3d_release_workspace": (I, []),
+        "ss3d_batch_create": (I, [P, I, P]),
+        "ss3d_batch_run": (I, [P]),
+        "ss3d_batch_autotune": (I, [P]),
+        "ss3d_batch_info": (I, [P, P, P, P, P]),
+        "ss3d_batch_time": (I, [P, P]),
+        "ss3d_batch_schedule": (I, [P, P, P, P, P]),
+        "ss3d_batch_set_schedule": (I, [P, I, I, I, I, I]),
+        "ss3d_batch_free": (None, [P]),
     }
     for name, (res, args) in sig.items():
         f = getattr(L, name)

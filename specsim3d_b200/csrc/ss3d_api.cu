@@ -704,6 +704,23 @@ int ss3d::spectrum_view(const ss3d_spectrum* sp, NoallocView* v) {
   return 0;
 }
 
+// helpers of the batched form (ss3d_batch.cu)
+int ss3d::batch_ctx(int dev, Tw* tw, const uint32_t** ptab) {
+  (void)dev;
+  DevCtx* ctx;
+  if (int rc = get_ctx(&ctx)) return rc;
+  *tw = Tw{ctx->twf, ctx->twd};
+  *ptab = ctx->ptab;
+  return SS3D_OK;
+}
+int ss3d::batch_geo(const ss3d_spectrum* sp, int igauss, Geo* g, const float** amp32) {
+  int dev = -1;
+  if (!sp || !sp->amp32 || cudaGetDevice(&dev) != cudaSuccess || dev != sp->dev) return 1;
+  *g = geo_for(sp, igauss);
+  *amp32 = sp->amp32;
+  return 0;
+}
+
 // model helpers shared with the conditioning module
 void ss3d::setrot_public(const ss3d_struct& s, double rot[3][3], double axes[3][3]) { setrot_rc(s, rot, axes); }
 void ss3d::model_public(const ss3d_struct* st, int nst, double nugget, Model& m) { build_model(st, nst, nugget, m); }

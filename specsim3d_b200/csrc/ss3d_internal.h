@@ -104,4 +104,8 @@ cudaStream_t current_stream();                // stream selected with ss3d_set_s
 struct ss3d_spectrum;
 namespace ss3d {
 int spectrum_view(const ss3d_spectrum* sp, NoallocView* v);
+int batch_ctx(int dev, Tw* tw, const uint32_t** ptab);   // twiddle and jump tables of the current device
+// geometry of a spectrum for igauss and its FP32 amplitudes; 1 if the handle is
+// invalid or lives on another device than the current one
+int batch_geo(const ss3d_spectrum* sp, int igauss, Geo* g, const float** amp32);
 }  // namespace ss3d
