@@ -19,60 +19,58 @@ def _log_uniform_int(rng, lo, hi):
 
 
 def random_model(rng, n, itype):
-    """One structure with ranges uniform in [5, 0.4 x extent] per axis (the two
-    horizontal draws sorted into ahmax >= ahmin), azimuth uniform in [0, 180),
-    dip uniform in [-30, 30] (0 for 2D grids), nugget uniform in [0, 0.3] and
-    sill 1 - nugget, so that the total sill is 1."""
-    nx, ny, nz = n
-    a1 = rng.uniform(5.0, max(5.0, 0.4 * nx))
-    a2 = rng.uniform(5.0, max(5.0, 0.4 * ny))
-    ahmax, ahmin = max(a1, a2), min(a1, a2)
-    avert = rng.uniform(5.0, max(5.0, 0.4 * nz)) if nz > 1 else 5.0
+    """One structure: ranges U(5, 0.4 x extent) drawn per axis (x, y, z) and
+    sorted so that ahmax >= ahmin >= avert (an extent below 12.5 gives range
+    5), azimuth U(0, 180), dip U(-30, 30), plunge 0, sill 1, nugget U(0, 0.3)."""
+    ranges = sorted((rng.uniform(5.0, max(5.0, 0.4 * e)) for e in n), reverse=True)
     azimuth = rng.uniform(0.0, 180.0)
-    dip = rng.uniform(-30.0, 30.0) if nz > 1 else 0.0
+    dip = rng.uniform(-30.0, 30.0)
     nugget = rng.uniform(0.0, 0.3)
-    return [(itype, 1.0 - nugget, ahmax, ahmin, avert, azimuth, dip, 0.0)], nugget
+    return [(itype, 1.0, ranges[0], ranges[1], ranges[2], azimuth, dip, 0.0)], nugget
 
 
-def mixed_grids(seed=777, nshapes=16, total_real=1024, lo=32, hi=256, two_d_every=4):
+def mixed_grids(seed=777, nshapes=16, total_real=1024, lo=32, hi=256, two_d_mod=8):
     """Batched workload: total_real unconditional realizations over nshapes grid
-    shapes; nx, ny, nz log-uniform in [lo, hi], every two_d_every-th shape 2D
-    (nz = 1); model family cycling spherical / exponential / gaussian; ipad 1,
-    igauss 1; job s seeded seed + 1000 s.  Returns a list of dicts (n, structs,
-    nugget, d, ipad, igauss, iseed, nreal); realizations split evenly."""
+    shapes.  Shape s: nx, ny, nz = round(exp(U(ln lo, ln hi))) each, then
+    nz = 1 when s = two_d_mod - 1 (mod two_d_mod); model family s mod 3
+    (spherical, exponential, gaussian) drawn by random_model; ipad 1, igauss 1,
+    iseed = seed + s.  Realizations are split evenly over the shapes.  Returns
+    a list of dicts (n, structs, nugget, d, ipad, igauss, iseed, nreal)."""
     rng = np.random.default_rng(seed)
     per = total_real // nshapes
     jobs = []
     for s in range(nshapes):
-        nx = _log_uniform_int(rng, lo, hi)
-        ny = _log_uniform_int(rng, lo, hi)
-        nz = 1 if (two_d_every and s % two_d_every == two_d_every - 1) else _log_uniform_int(rng, lo, hi)
-        structs, nugget = random_model(rng, (nx, ny, nz), 1 + s % 3)
+        n = [_log_uniform_int(rng, lo, hi) for _ in range(3)]
+        if two_d_mod and s % two_d_mod == two_d_mod - 1:
+            n[2] = 1
+        structs, nugget = random_model(rng, n, 1 + s % 3)
         nreal = per + (1 if s < total_real - per * nshapes else 0)
-        jobs.append(dict(n=(nx, ny, nz), structs=structs, nugget=nugget, d=(1.0, 1.0, 1.0), ipad=1, igauss=1,
-                         iseed=seed + 1000 * s, nreal=nreal))
+        jobs.append(dict(n=tuple(n), structs=structs, nugget=nugget, d=(1.0, 1.0, 1.0), ipad=1, igauss=1,
+                         iseed=seed + s, nreal=nreal))
     return jobs
 
 
-def model_pool(seed=2024, size=64, lo=32, hi=256):
-    """Serving model pool: size (grid, model) entries, cubic grids with edge
-    log-uniform in [lo, hi], models drawn as in mixed_grids."""
+def model_pool(seed=2025, size=64, lo=32, hi=256):
+    """Serving model pool: size (grid, model) entries drawn like mixed_grids
+    (per-axis log-uniform grids, no 2D shapes)."""
     rng = np.random.default_rng(seed)
     pool = []
     for m in range(size):
-        n = _log_uniform_int(rng, lo, hi)
-        structs, nugget = random_model(rng, (n, n, n), 1 + m % 3)
-        pool.append(dict(n=(n, n, n), structs=structs, nugget=nugget, d=(1.0, 1.0, 1.0), ipad=1))
+        n = [_log_uniform_int(rng, lo, hi) for _ in range(3)]
+        structs, nugget = random_model(rng, n, 1 + m % 3)
+        pool.append(dict(n=tuple(n), structs=structs, nugget=nugget, d=(1.0, 1.0, 1.0), ipad=1))
     return pool
 
 
 def request_stream(rate, count=4000, seed=2024, pool_size=64, cond_frac=0.2, max_real=16):
-    """Serving request stream: Poisson arrivals at `rate` requests/s, a pool
-    model per request (uniform), nreal uniform in 1..max_real, conditional with
-    probability cond_frac and then carrying 200..2000 data points.  Returns a
+    """Serving request stream: Poisson arrivals at `rate` requests/s.  The draws
+    do not depend on the rate (inter-arrival times are unit exponentials divided
+    by the rate), so every rate replays the same requests: a pool model
+    (uniform), nreal uniform in 1..max_real, a seed, and with probability
+    cond_frac a conditional request carrying 200..2000 data points.  Returns a
     list of dicts (t_arrival, model, nreal, iseed, ndata)."""
-    rng = np.random.default_rng([seed, int(rate)])
-    t = np.cumsum(rng.exponential(1.0 / rate, size=count))
+    rng = np.random.default_rng(seed)
+    t = np.cumsum(rng.exponential(1.0, size=count)) / float(rate)
     reqs = []
     for q in range(count):
         cond = rng.uniform() < cond_frac
