@@ -48,6 +48,7 @@ def parse():
     ap.add_argument("--impl", default="ours", choices=["ours", "reference"])
     ap.add_argument("--no-cpu-baseline", action="store_true")
     ap.add_argument("--no-batch", action="store_true", help="skip the mixed-grid batched workload")
+    ap.add_argument("--no-serving", action="store_true", help="skip the serving workload")
     ap.add_argument("--profile-case", action="store_true",
                     help="profiling case: the same grid, 1 realization, three FP32 calls, no timing")
     return ap.parse_args()
@@ -241,6 +242,124 @@ def bench_mixed_grids(ss, stream, seed=777):
     }
 
 
+def _serving_cond(model, ndata, seed):
+    """Conditioning data of a serving request: ndata points at uniform-random
+    locations with skewed values exp(0.5 g), g standard normal (the conditional
+    recipe's value transform, without its truth field); normal-score transform,
+    linear tails, search ellipsoid = the model's ranges and angles, ndmax 24."""
+    rng = np.random.default_rng(seed)
+    n = model["n"]
+    xyz = np.stack([rng.uniform(0, n[a] - 1, ndata) for a in range(3)], axis=1)
+    val = np.exp(0.5 * rng.standard_normal(ndata))
+    st = model["structs"][0]
+    params = dict(ixc=1, iyc=2, izc=3, ivc=4, iwc=0, tmin=-1e21, tmax=1e21, itrans=1, skmean=0.0, zmin=0.0,
+                  zmax=2.0 * float(val.max()), ltail=1, ltpar=0.0, utail=1, utpar=0.0,
+                  radius=(st[2], st[3], st[4]), angles=(st[5], st[6], st[7]), ndmax=24)
+    return dict(params=params, rows=np.column_stack([xyz, val]), xmin=(0.0, 0.0, 0.0))
+
+
+def bench_serving(ss, rates=(200.0, 1000.0), count=300, slots=8, budget=64 << 30):
+    """Serving form on a Poisson request stream (seed 2024) over a pool of 64
+    models (seed 2025): grids log-uniform 32..256 per axis, nreal 1..16, 20 %
+    conditional with 200..2000 data, FP32 (FP64 for the conditional ones, whose
+    kriging runs on FP64 fields).  Open loop: a feeder submits each request at its
+    arrival time.  Latency = completion - arrival.  Beside it the plain path,
+    one request at a time with no spectra cache (spectrum, realizations and
+    conditioning per request): its service times are measured, and its latency
+    at each rate is the FIFO single-server recursion on those times."""
+    import threading
+    import torch
+    from specsim3d_b200 import workloads
+    pool = workloads.model_pool()
+    out = {"workload": f"{count} requests per rate, Poisson arrivals (seed 2024), pool of 64 models (seed 2025), "
+                       "grids log-uniform 32..256 per axis, nreal U{1..16}, 20 % conditional (200..2000 points)",
+           "slots": slots, "hbm_budget_gb": budget / 2 ** 30, "rates": {}}
+
+    def alloc(q):
+        m = pool[q["model"]]
+        nx, ny, nz = m["n"]
+        return torch.empty((q["nreal"], nz, ny, nx), dtype=torch.float64 if q["ndata"] else torch.float32,
+                           device="cuda")
+
+    def cond_of(q, k):
+        return _serving_cond(pool[q["model"]], q["ndata"], 5000 + k) if q["ndata"] else None
+
+    def prec_of(q):
+        return ss.FP64 if q["ndata"] else ss.FP32
+
+    base_reqs = workloads.request_stream(1.0, count=count)
+    conds = [cond_of(q, k) for k, q in enumerate(base_reqs)]
+    cells_of = [q["nreal"] * int(np.prod(pool[q["model"]]["n"])) for q in base_reqs]
+    for rate in rates:
+        reqs = workloads.request_stream(rate, count=count)
+        srv = ss.Server(slots=slots, hbm_budget=budget)
+        tickets = [None] * count
+        keep = [None] * count
+        t_start = srv.clock() + 0.05
+
+        def feeder():
+            for k, q in enumerate(reqs):
+                t_arr = t_start + q["t_arrival"]
+                dt = t_arr - srv.clock()
+                if dt > 0:
+                    time.sleep(dt)
+                o = alloc(q)
+                keep[k] = o
+                tickets[k] = srv.submit(pool[q["model"]], q["iseed"], q["nreal"], 1, prec_of(q), out=o,
+                                        t_arrival=t_arr, cond=conds[k])
+
+        th = threading.Thread(target=feeder)
+        th.start()
+        res = []
+        for k in range(count):
+            while tickets[k] is None:
+                time.sleep(0.0005)
+            res.append(srv.wait(tickets[k]))
+            keep[k] = None
+        th.join()
+        st = srv.stats()
+        srv.close()
+        ok = [r for r in res if r["status"] == 0]
+        lat = np.array([r["t_done"] - r["t_arrival"] for r in ok]) * 1e3
+        span = max(r["t_done"] for r in ok) - t_start
+        cells = sum(c for c, r in zip(cells_of, res) if r["status"] == 0)
+        out["rates"][str(int(rate))] = {
+            "p50_ms": round(float(np.percentile(lat, 50)), 3), "p99_ms": round(float(np.percentile(lat, 99)), 3),
+            "mcells_s": round(cells / span / 1e6, 1), "completed": len(ok), "failed": count - len(ok),
+            "cache_hits": st["cache_hits"], "cache_misses": st["cache_misses"], "peak_running": st["peak_running"],
+            "peak_gb": round(st["peak_bytes"] / 2 ** 30, 2)}
+    # plain path: one request at a time, no cache
+    svc = []
+    for k, q in enumerate(base_reqs):
+        m = pool[q["model"]]
+        torch.cuda.synchronize()
+        t0 = time.perf_counter()
+        o = alloc(q)
+        sp = ss.Spectrum(m["structs"], m["nugget"], m["d"], m["n"], m["ipad"])
+        sp.realize(q["iseed"], q["nreal"], 1, prec_of(q), out=o)
+        if conds[k] is not None:
+            c = conds[k]
+            ss.condition(o, c["xmin"], m["d"], m["structs"], m["nugget"], c["params"], c["rows"], prec_of(q))
+        sp.close()
+        torch.cuda.synchronize()
+        svc.append(time.perf_counter() - t0)
+        del o
+    tot_cells = sum(cells_of)
+    plain = {"mcells_s": round(tot_cells / sum(svc) / 1e6, 1), "mean_service_ms": round(1e3 * float(np.mean(svc)), 3),
+             "rates": {}}
+    for rate in rates:
+        reqs = workloads.request_stream(rate, count=count)
+        done, lat = 0.0, []
+        for q, sv in zip(reqs, svc):
+            done = max(done, q["t_arrival"]) + sv
+            lat.append(done - q["t_arrival"])
+        lat = np.array(lat) * 1e3
+        plain["rates"][str(int(rate))] = {"p50_ms": round(float(np.percentile(lat, 50)), 3),
+                                         "p99_ms": round(float(np.percentile(lat, 99)), 3)}
+    out["one_at_a_time"] = plain
+    return out
+
+
 def run_ours(args):
     import torch
     import torch.distributed as dist
@@ -413,6 +532,8 @@ def run_ours(args):
     }
     if world == 1 and not args.no_batch:
         line["mixed_grids"] = bench_mixed_grids(ss, stream)
+    if world == 1 and not args.no_serving:
+        line["serving"] = bench_serving(ss)
     if rank == 0 and world == 1 and not args.no_cpu_baseline:
         try:
             sec, t_spec, cores, _ = cpu_reference_sample(1, 0)

@@ -244,6 +244,80 @@ int ss3d_condition(double *res, const int n[3], int nreal, const double xmin[3],
                    int nrows, int nvar, int precision, ss3d_cond_stats *cs, double *vrt, double *gtt, double *dxs,
                    double *dys, double *dzs, double *dval, double *dg);
 
+/* ---------------------------------------------------------------- serving form */
+
+/* A request loop over the simulation path (no counterpart in the reference,
+ * which runs one parameter file per process).  ss3d_server_submit queues a
+ * request and returns at once; `slots` worker threads, each with its own CUDA
+ * stream and work space, admit queued requests in arrival order as soon as a
+ * slot is free and the request's device footprint (work space, conditioning
+ * temporaries, and the spectrum with its build temporaries when the model is
+ * not resident) fits the HBM budget; a request that does not fit waits, and
+ * later requests may pass it at most max_bypass times.  Spectra stay resident
+ * in an LRU cache keyed by model, grid and ipad.  Each request runs
+ * ss3d_spectrum_create (on a cache miss), ss3d_realize and, with data,
+ * ss3d_condition, so its result equals the same calls made alone.
+ * The caller keeps `out` and `rows` alive until ss3d_server_wait returns. */
+typedef struct ss3d_server ss3d_server;
+
+typedef struct ss3d_server_config {
+    int slots;                   /* requests on the GPU at once (1..64) */
+    int max_bypass;              /* passes of a waiting queue head (0: 16) */
+    int64_t hbm_budget;          /* device bytes for spectra and work (0: 80 % of free memory) */
+    int64_t cache_budget;        /* bytes of idle spectra kept (0: half the budget) */
+    int64_t retain_bytes;        /* work space a slot keeps between requests (0: 1 GiB);
+                                    slots * retain_bytes is reserved out of hbm_budget */
+    double dry_run_ns_per_cell;  /* > 0: no GPU work, sleeps of this many ns per cell
+                                    (scheduler tests); needs an explicit hbm_budget */
+} ss3d_server_config;
+
+typedef struct ss3d_request {
+    const ss3d_struct *st;       /* model: nst structures and the nugget */
+    int nst;
+    double nugget;
+    double d[3];                 /* cell size */
+    int n[3];                    /* grid */
+    int ipad;
+    int iseed, igauss;
+    int64_t r_first;
+    int nreal;
+    int precision;               /* SS3D_FP64 or SS3D_FP32 */
+    void *out;                   /* res(nx,ny,nz,nreal), host or device */
+    int out_dtype;               /* SS3D_OUT_F32 / SS3D_OUT_F64 (F64 with conditioning data) */
+    double t_arrival;            /* arrival on the server clock (< 0: the submit time) */
+    /* conditioning (nrows = 0: unconditional), as ss3d_condition */
+    const ss3d_cond_params *cp;
+    const double *rows;
+    int nrows, nvar;
+    double xmin[3];
+} ss3d_request;
+
+typedef struct ss3d_result {
+    int status;                  /* SS3D_OK or the failing stage's code */
+    int cache_hit;               /* the spectrum was resident or being built */
+    double t_arrival, t_submit, t_admit, t_done;   /* seconds on the server clock */
+    int64_t footprint;           /* device bytes the request was admitted with */
+} ss3d_result;
+
+typedef struct ss3d_serve_stats {
+    int64_t submitted, completed, failed;
+    int64_t cache_hits, cache_misses, evictions;
+    int64_t cells;               /* output cells of completed requests */
+    int64_t peak_bytes;          /* peak of charged + cached bytes */
+    int64_t peak_running, running, queued, cached_spectra;
+    int64_t cache_bytes, charged_bytes, budget_bytes;
+} ss3d_serve_stats;
+
+int ss3d_server_create(const ss3d_server_config *cfg, ss3d_server **out);
+int ss3d_server_submit(ss3d_server *s, const ss3d_request *req, int64_t *ticket);
+/* Blocks until the request is done; returns its status (message in
+ * ss3d_last_error on this thread).  Each ticket is waited for once. */
+int ss3d_server_wait(ss3d_server *s, int64_t ticket, ss3d_result *res);
+int ss3d_server_stats(ss3d_server *s, ss3d_serve_stats *stats);
+double ss3d_server_clock(ss3d_server *s);   /* seconds since creation */
+/* Stops the slots after the running requests; queued requests fail. */
+void ss3d_server_free(ss3d_server *s);
+
 /* ---------------------------------------------------------------- runtime */
 
 /* Stream (a cudaStream_t passed as void*) on which later calls from the

@@ -8,6 +8,8 @@ the reference program src/specsim3d.f90:
     Spectrum.realize       Hermitian synthesis + inverse FFT f90:1302-1345
     vario                  experimental variograms           f90:394-480
     condition              kriging of the residual           f90:700-1081
+    Batch                  many grids per CUDA-graph launch  (batched form)
+    Server                 request loop, spectra cache       (serving form)
 
 Arrays follow the Fortran layout res(nx,ny,nz,nreal), i.e. numpy shape
 (nreal, nz, ny, nx).  Outputs can be numpy arrays (host) or torch CUDA tensors
@@ -21,7 +23,7 @@ import numpy as np
 from . import _lib as L
 from ._lib import FP32, FP64, OUT_F32, OUT_F64, SpecsimError
 
-__all__ = ["Spectrum", "grid_size", "covariance", "setrot", "vario", "condition", "FP32", "FP64",
+__all__ = ["Spectrum", "Batch", "Server", "grid_size", "covariance", "setrot", "vario", "condition", "FP32", "FP64",
            "SpecsimError", "set_stream"]
 
 
@@ -305,3 +307,96 @@ def condition(res, xmin, d, structs, nugget, params, rows, precision=FP64):
                  nnone=cs.nnone, nexact=cs.nexact, data_mean=cs.data_mean, data_var=cs.data_var)
     nd = cs.nd
     return stats, {k: v[:nd] for k, v in outs.items()}
+
+
+def _cond_params(params):
+    cp = L.CondParams()
+    for k, v in params.items():
+        if k in ("radius", "angles"):
+            getattr(cp, k)[:] = [float(x) for x in v]
+        else:
+            setattr(cp, k, v)
+    return cp
+
+
+class Server:
+    """Serving form: a request loop over the simulation path (ss3d_server_*).
+
+    ``slots`` requests run on the GPU at once, each on its own stream; queued
+    requests are admitted in arrival order as slots and HBM free up (budget
+    ``hbm_budget`` bytes, 0 = 80 % of free memory); spectra of seen models stay
+    resident (LRU, ``cache_budget`` bytes of idle spectra).  ``dry_run_ns_per_cell``
+    > 0 replaces the GPU work by sleeps (scheduler tests without a GPU)."""
+
+    def __init__(self, slots=4, hbm_budget=0, cache_budget=0, retain_bytes=0, max_bypass=0, dry_run_ns_per_cell=0.0):
+        cfg = L.ServerConfig(int(slots), int(max_bypass), int(hbm_budget), int(cache_budget), int(retain_bytes),
+                             float(dry_run_ns_per_cell))
+        h = ctypes.c_void_p()
+        L.check(L.lib().ss3d_server_create(ctypes.byref(cfg), ctypes.byref(h)))
+        self._h = h
+        self._keep = {}
+
+    def submit(self, model, iseed, nreal, igauss=1, precision=FP32, r_first=0, out=None, t_arrival=-1.0, cond=None):
+        """Queue one request; returns its ticket.
+
+        model: dict(structs, nugget, d, n, ipad).  out: numpy array or torch
+        tensor of shape (nreal, nz, ny, nx), float32 or float64 (float64 with
+        cond); None only in a dry run.  cond: dict(params, rows, xmin) as for
+        condition().  t_arrival: arrival on the server clock (< 0: now)."""
+        arr = L.structs_array(model["structs"])
+        q = L.Request()
+        q.st = ctypes.cast(arr, ctypes.c_void_p)
+        q.nst = len(arr)
+        q.nugget = float(model["nugget"])
+        q.d[:] = [float(v) for v in model["d"]]
+        q.n[:] = [int(v) for v in model["n"]]
+        q.ipad = int(model["ipad"])
+        q.iseed, q.igauss, q.r_first, q.nreal, q.precision = int(iseed), int(igauss), int(r_first), int(nreal), int(precision)
+        q.t_arrival = float(t_arrival)
+        keep = [arr, out]
+        if out is not None:
+            ptr, code = _out_ptr(out)
+            q.out, q.out_dtype = ptr.value, code
+        else:
+            q.out, q.out_dtype = None, (OUT_F64 if cond is not None else OUT_F32)
+        if cond is not None:
+            cp = _cond_params(cond["params"])
+            rows = np.ascontiguousarray(np.asarray(cond["rows"], dtype=np.float64))
+            q.cp = ctypes.cast(ctypes.pointer(cp), ctypes.c_void_p)
+            q.rows = rows.ctypes.data
+            q.nrows, q.nvar = rows.shape
+            q.xmin[:] = [float(v) for v in cond["xmin"]]
+            keep += [cp, rows]
+        t = ctypes.c_int64()
+        L.check(L.lib().ss3d_server_submit(self._h, ctypes.byref(q), ctypes.byref(t)))
+        self._keep[t.value] = keep
+        return t.value
+
+    def wait(self, ticket):
+        """Block until the request is done: dict(status, message, cache_hit, t_arrival, t_submit, t_admit,
+        t_done, footprint)."""
+        r = L.Result()
+        rc = L.lib().ss3d_server_wait(self._h, int(ticket), ctypes.byref(r))
+        msg = L.lib().ss3d_last_error().decode() if rc else ""
+        self._keep.pop(int(ticket), None)
+        return dict(status=rc, message=msg, cache_hit=bool(r.cache_hit), t_arrival=r.t_arrival, t_submit=r.t_submit,
+                    t_admit=r.t_admit, t_done=r.t_done, footprint=int(r.footprint))
+
+    def stats(self):
+        st = L.ServeStats()
+        L.check(L.lib().ss3d_server_stats(self._h, ctypes.byref(st)))
+        return {k: int(getattr(st, k)) for k, _ in L.ServeStats._fields_}
+
+    def clock(self):
+        return float(L.lib().ss3d_server_clock(self._h))
+
+    def close(self):
+        if self._h:
+            L.lib().ss3d_server_free(self._h)
+            self._h = None
+
+    def __del__(self):
+        try:
+            self.close()
+        except Exception:
+            pass

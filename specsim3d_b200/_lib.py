@@ -27,6 +27,8 @@ EXPORTS = (
     "ss3d_realize_workspace_bytes", "ss3d_release_workspace",
     "ss3d_batch_create", "ss3d_batch_run", "ss3d_batch_autotune", "ss3d_batch_info", "ss3d_batch_time",
     "ss3d_batch_schedule", "ss3d_batch_set_schedule", "ss3d_batch_free",
+    "ss3d_server_create", "ss3d_server_submit", "ss3d_server_wait", "ss3d_server_stats", "ss3d_server_clock",
+    "ss3d_server_free",
 )
 
 
@@ -52,6 +54,35 @@ class BatchJob(ctypes.Structure):
     """ss3d_batch_job: realizations r_first.. of one spectrum into a device array."""
     _fields_ = [("sp", ctypes.c_void_p), ("iseed", ctypes.c_int), ("igauss", ctypes.c_int),
                 ("r_first", ctypes.c_int64), ("nreal", ctypes.c_int), ("out", ctypes.c_void_p)]
+
+
+class ServerConfig(ctypes.Structure):
+    _fields_ = [("slots", ctypes.c_int), ("max_bypass", ctypes.c_int), ("hbm_budget", ctypes.c_int64),
+                ("cache_budget", ctypes.c_int64), ("retain_bytes", ctypes.c_int64),
+                ("dry_run_ns_per_cell", ctypes.c_double)]
+
+
+class Request(ctypes.Structure):
+    """ss3d_request (serving form)."""
+    _fields_ = [("st", ctypes.c_void_p), ("nst", ctypes.c_int), ("nugget", ctypes.c_double),
+                ("d", ctypes.c_double * 3), ("n", ctypes.c_int * 3), ("ipad", ctypes.c_int),
+                ("iseed", ctypes.c_int), ("igauss", ctypes.c_int), ("r_first", ctypes.c_int64),
+                ("nreal", ctypes.c_int), ("precision", ctypes.c_int), ("out", ctypes.c_void_p),
+                ("out_dtype", ctypes.c_int), ("t_arrival", ctypes.c_double), ("cp", ctypes.c_void_p),
+                ("rows", ctypes.c_void_p), ("nrows", ctypes.c_int), ("nvar", ctypes.c_int),
+                ("xmin", ctypes.c_double * 3)]
+
+
+class Result(ctypes.Structure):
+    _fields_ = [("status", ctypes.c_int), ("cache_hit", ctypes.c_int), ("t_arrival", ctypes.c_double),
+                ("t_submit", ctypes.c_double), ("t_admit", ctypes.c_double), ("t_done", ctypes.c_double),
+                ("footprint", ctypes.c_int64)]
+
+
+class ServeStats(ctypes.Structure):
+    _fields_ = [(k, ctypes.c_int64) for k in (
+        "submitted", "completed", "failed", "cache_hits", "cache_misses", "evictions", "cells", "peak_bytes",
+        "peak_running", "running", "queued", "cached_spectra", "cache_bytes", "charged_bytes", "budget_bytes")]
 
 
 class CondParams(ctypes.Structure):
@@ -117,6 +148,12 @@ def lib():
         "ss3d_batch_schedule": (I, [P, P, P, P, P]),
         "ss3d_batch_set_schedule": (I, [P, I, I, I, I, I]),
         "ss3d_batch_free": (None, [P]),
+        "ss3d_server_create": (I, [P, P]),
+        "ss3d_server_submit": (I, [P, P, P]),
+        "ss3d_server_wait": (I, [P, I64, P]),
+        "ss3d_server_stats": (I, [P, P]),
+        "ss3d_server_clock": (D, [P]),
+        "ss3d_server_free": (None, [P]),
     }
     for name, (res, args) in sig.items():
         f = getattr(L, name)

@@ -57,7 +57,7 @@ void ss3d::mark(Marks* m, int stage, cudaStream_t st) {
   if (cudaEventCreate(&m->ev[m->n]) != cudaSuccess) return;
   cudaEventRecord(m->ev[m->n], st);
   m->stage[m->n] = stage;
-  g_mark_launch[m->n] = g_launch_count;
+  g_mark_launch[m->n] = g_launch_count.load();
   m->n++;
 }
 
@@ -88,7 +88,7 @@ extern "C" int ss3d_profile_read(double ms[SS3D_NSTAGE], int64_t launches[SS3D_N
     if (ms) ms[q] = g_prof_ms[q];
     if (launches) launches[q] = g_prof_launch[q];
   }
-  if (launches_total) *launches_total = (int64_t)g_launch_count;
+  if (launches_total) *launches_total = (int64_t)g_launch_count.load();
   return SS3D_OK;
 }
 extern "C" const char* ss3d_version(void) { return "specsim3d_b200 0.1 (sm_100a)"; }
@@ -316,18 +316,24 @@ struct Workspace {
   void* p = nullptr;
   size_t bytes = 0;
   int dev = 0;
-  void release() {
+  // stream-ordered release on the thread's stream: no device-wide synchronisation
+  void release(cudaStream_t st) {
     if (p) {
       int cur = 0;
       cudaGetDevice(&cur);
       cudaSetDevice(dev);
-      cudaFree(p);
+      cudaFreeAsync(p, st);
       cudaSetDevice(cur);
     }
     p = nullptr;
     bytes = 0;
   }
-  ~Workspace() { release(); }
+  ~Workspace() {
+    if (p) {
+      cudaSetDevice(dev);
+      cudaFree(p);
+    }
+  }
 };
 thread_local Workspace g_ws[64];
 
@@ -335,8 +341,8 @@ int ws_reserve(int dev, size_t bytes, void** ptr) {
   if (dev < 0 || dev >= 64) return fail(SS3D_EINVAL, "device ordinal %d out of range", dev);
   Workspace& w = g_ws[dev];
   if (w.bytes < bytes) {
-    w.release();
-    CK(cudaMalloc(&w.p, bytes));
+    w.release(g_stream);
+    CK(cudaMallocAsync(&w.p, bytes, g_stream));
     w.bytes = bytes;
     w.dev = dev;
   }
@@ -385,18 +391,20 @@ extern "C" int ss3d_spectrum_create(const ss3d_struct* st, int nst, double nugge
   double2* work = nullptr;
   SpecPartial* part = nullptr;
   const int npart = 148 * 8;
-  cudaError_t e = cudaMalloc(&work, sizeof(double2) * nh);
+  // temporaries come from the stream-ordered pool: no device-wide synchronisation
+  // when they are freed, so that other threads' streams keep running
+  cudaError_t e = cudaMallocAsync((void**)&work, sizeof(double2) * nh, s);
   if (e == cudaSuccess) e = cudaMalloc(&sp->amp64, sizeof(double) * nh);
   if (e == cudaSuccess) e = cudaMalloc(&sp->amp32, sizeof(float) * nh);
-  if (e == cudaSuccess) e = cudaMalloc(&part, sizeof(SpecPartial) * (npart + 1));
+  if (e == cudaSuccess) e = cudaMallocAsync((void**)&part, sizeof(SpecPartial) * (npart + 1), s);
   if (e == cudaSuccess)
     e = launch_spectrum(sp->model, d, g, work, sp->amp64, sp->amp32, part, npart, part + npart, Tw{ctx->twf, ctx->twd},
                         s);
   SpecPartial res{};
   if (e == cudaSuccess) e = cudaMemcpyAsync(&res, part + npart, sizeof res, cudaMemcpyDeviceToHost, s);
   if (e == cudaSuccess) e = cudaStreamSynchronize(s);
-  if (work) cudaFree(work);
-  if (part) cudaFree(part);
+  if (work) cudaFreeAsync(work, s);
+  if (part) cudaFreeAsync(part, s);
   if (e != cudaSuccess) {
     ss3d_spectrum_free(sp);
     return cuda_fail(e, "spectrum");
@@ -473,6 +481,10 @@ uint32_t seed0(int iseed) {
 }  // namespace
 
 namespace {
+// complex planes per realization in the work space: the first (z) inverse pass
+// stores only the planes k < nz that survive the crop
+int work_planes(const Geo& g) { return g.npz > 1 ? g.nz : 1; }
+
 // Work-space layout of one realize call: batches of at most 16 realizations
 // and about 8 GiB; host output goes through two staging buffers.
 struct RealizeLayout {
@@ -483,7 +495,7 @@ RealizeLayout realize_layout(const Geo& g, bool dbl, bool dev_out, int nreal, si
   RealizeLayout L{};
   const size_t M = (size_t)g.nx * g.ny * g.nz;
   const size_t cel = dbl ? sizeof(double2) : sizeof(float2);
-  L.per_work = (size_t)g.npz * g.npy * g.HP * cel;
+  L.per_work = (size_t)work_planes(g) * g.npy * g.HP * cel;
   const int nbx = realize_part_blocks(g, dbl);
   const size_t budget = (size_t)8 << 30;
   const size_t per_real = L.per_work + (dev_out ? 0 : 2 * M * oel) + (size_t)g.npy * g.npz * 4 + (size_t)nbx * 16;
@@ -501,14 +513,32 @@ RealizeLayout realize_layout(const Geo& g, bool dbl, bool dev_out, int nreal, si
 }
 }  // namespace
 
+// work-space bytes of a realize call on periodic grid np with output grid n,
+// before any spectrum exists (admission control of the serving form); an
+// upper bound: host output staged as double
+int64_t ss3d::realize_bytes_for(const int np[3], const int n[3], int nreal, int precision, int host_out) {
+  Geo g{};
+  g.npx = np[0];
+  g.npy = np[1];
+  g.npz = np[2];
+  g.nx = n[0];
+  g.ny = n[1];
+  g.nz = n[2];
+  g.H = np[0] >= 2 ? np[0] / 2 + 1 : 1;
+  g.HP = (g.H + 1) & ~1;
+  const bool dbl = precision == SS3D_FP64;
+  return (int64_t)realize_layout(g, dbl, host_out == 0, nreal, 8).total;
+}
+
 extern "C" int64_t ss3d_realize_workspace_bytes(const ss3d_spectrum* sp, int nreal, int precision, int host_out) {
   if (!sp || nreal < 0 || (precision != SS3D_FP64 && precision != SS3D_FP32)) return -1;
   const bool dbl = precision == SS3D_FP64;
-  return (int64_t)realize_layout(sp->geo, dbl, host_out == 0, nreal, dbl ? 8 : 4).total;
+  return (int64_t)realize_layout(sp->geo, dbl, host_out == 0, nreal, 8).total;
 }
 
 extern "C" int ss3d_release_workspace(void) {
-  for (Workspace& w : g_ws) w.release();
+  for (Workspace& w : g_ws) w.release(g_stream);
+  cudaStreamSynchronize(g_stream);
   return SS3D_OK;
 }
 
@@ -547,7 +577,7 @@ extern "C" int ss3d_realize(const ss3d_spectrum* csp, int iseed, int64_t r_first
   double* part = (double*)(base + lay.off_part);
   double* zs = (double*)(base + lay.off_zs);
   char* stage[2] = {base + lay.off_stage, base + lay.off_stage + lay.stage_bytes};
-  const long long wstride = (long long)g.npz * g.npy * g.HP;
+  const long long wstride = (long long)work_planes(g) * g.npy * g.HP;
   const uint32_t s0 = seed0(iseed);
   Tw tw{ctx->twf, ctx->twd};
   cudaEvent_t done[2] = {nullptr, nullptr};

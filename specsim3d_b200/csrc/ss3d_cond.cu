@@ -411,14 +411,19 @@ double gauinv(double p0) {
   return x - u / (1.0 + 0.5 * x * u);
 }
 
+// Temporaries of one call from the stream-ordered pool of the call's stream:
+// freeing them does not synchronise the device, so other threads' streams
+// keep running.
 struct DevBuf {
+  cudaStream_t st;
   std::vector<void*> ptrs;
+  explicit DevBuf(cudaStream_t s) : st(s) {}
   ~DevBuf() {
-    for (void* p : ptrs) cudaFree(p);
+    for (void* p : ptrs) cudaFreeAsync(p, st);
   }
   template <typename T>
   cudaError_t alloc(T** p, size_t n) {
-    cudaError_t e = cudaMalloc((void**)p, sizeof(T) * std::max<size_t>(n, 1));
+    cudaError_t e = cudaMallocAsync((void**)p, sizeof(T) * std::max<size_t>(n, 1), st);
     if (e == cudaSuccess) ptrs.push_back(*p);
     return e;
   }
@@ -596,7 +601,7 @@ extern "C" int ss3d_condition(double* res, const int n[3], int nreal, const doub
   const bool dev_res = cudaPointerGetAttributes(&pa, res) == cudaSuccess &&
                        (pa.type == cudaMemoryTypeDevice || pa.type == cudaMemoryTypeManaged);
   cudaGetLastError();
-  DevBuf bufs;
+  DevBuf bufs(stm);
   double* dres = res;
   cudaError_t e = cudaSuccess;
   if (!dev_res) {

@@ -29,7 +29,7 @@
 
 namespace ss3d {
 
-unsigned long long g_launch_count = 0;
+std::atomic<unsigned long long> g_launch_count{0};
 
 constexpr int NT = 256;  // threads per block of every FFT kernel
 

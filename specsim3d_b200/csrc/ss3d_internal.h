@@ -1,6 +1,7 @@
 // ss3d_internal.h -- host/device shared declarations of the CUDA library
 // (not part of the public C ABI in include/specsim3d_gpu.h).
 #pragma once
+#include <atomic>
 #include <cuda_runtime.h>
 
 #include <cmath>
@@ -68,7 +69,7 @@ struct Marks {
   cudaEvent_t ev[16];
 };
 void mark(Marks* m, int stage, cudaStream_t st);   // records an event opening `stage`
-extern unsigned long long g_launch_count;          // kernels launched by the library
+extern std::atomic<unsigned long long> g_launch_count;   // kernels launched by the library (all threads)
 
 // ---- launchers (ss3d_fft.cu); all return cudaError_t of the last launch
 cudaError_t launch_spectrum(const Model& m, const double d[3], const Geo& g, double2* work, double* amp64,
@@ -104,6 +105,7 @@ cudaStream_t current_stream();                // stream selected with ss3d_set_s
 struct ss3d_spectrum;
 namespace ss3d {
 int spectrum_view(const ss3d_spectrum* sp, NoallocView* v);
+int64_t realize_bytes_for(const int np[3], const int n[3], int nreal, int precision, int host_out);
 int batch_ctx(int dev, Tw* tw, const uint32_t** ptab);   // twiddle and jump tables of the current device
 // geometry of a spectrum for igauss and its FP32 amplitudes; 1 if the handle is
 // invalid or lives on another device than the current one

@@ -1,0 +1,92 @@
+"""Scheduler of the serving form, run without a GPU (dry-run mode: the GPU
+stages become sleeps proportional to the work; admission, the spectra cache and
+the memory accounting are the production code paths).
+
+Checks: the device bytes charged never exceed the budget; slots run requests
+at the same time; repeated models hit the cache; a request that can never fit
+fails with SS3D_ENOMEM instead of blocking the queue; a large request waiting
+at the head is passed at most max_bypass times.
+"""
+import numpy as np
+import pytest
+
+from specsim3d_b200 import _lib, workloads
+import specsim3d_b200 as ss
+
+GB = 1 << 30
+
+
+def _server(**kw):
+    kw.setdefault("slots", 4)
+    kw.setdefault("retain_bytes", 1 << 20)
+    kw.setdefault("dry_run_ns_per_cell", 0.02)
+    return ss.Server(**kw)
+
+
+def test_budget_cache_and_overlap():
+    pool = workloads.model_pool(size=12, lo=16, hi=96)
+    reqs = workloads.request_stream(rate=1000.0, count=120, pool_size=12, cond_frac=0.0, max_real=6)
+    srv = _server(hbm_budget=2 * GB, cache_budget=GB // 2)
+    tickets = [srv.submit(pool[q["model"]], q["iseed"], q["nreal"]) for q in reqs]
+    res = [srv.wait(t) for t in tickets]
+    st = srv.stats()
+    srv.close()
+    assert all(r["status"] == 0 for r in res)
+    assert st["completed"] == len(reqs) and st["failed"] == 0
+    assert st["peak_bytes"] <= st["budget_bytes"]
+    assert st["peak_running"] >= 2
+    assert st["cache_hits"] > 0 and st["cache_hits"] + st["cache_misses"] == len(reqs)
+    assert all(r["t_admit"] >= r["t_submit"] and r["t_done"] >= r["t_admit"] for r in res)
+
+
+def test_tight_budget_serialises_without_deadlock():
+    pool = workloads.model_pool(size=4, lo=48, hi=64)
+    srv = _server(hbm_budget=120 << 20, cache_budget=0)
+    tickets = [srv.submit(pool[k % 4], 11 + k, 2) for k in range(16)]
+    res = [srv.wait(t) for t in tickets]
+    st = srv.stats()
+    srv.close()
+    assert all(r["status"] == 0 for r in res), [r["message"] for r in res if r["status"]]
+    assert st["peak_bytes"] <= st["budget_bytes"]
+
+
+def test_request_above_budget_fails_alone():
+    big = dict(structs=[(1, 1.0, 50.0, 50.0, 50.0, 0.0, 0.0, 0.0)], nugget=0.0, d=(1, 1, 1), n=(256, 256, 256), ipad=1)
+    small = dict(structs=[(1, 1.0, 5.0, 5.0, 5.0, 0.0, 0.0, 0.0)], nugget=0.0, d=(1, 1, 1), n=(16, 16, 16), ipad=1)
+    srv = _server(hbm_budget=256 << 20)
+    t_big = srv.submit(big, 1, 4)
+    t_small = [srv.submit(small, 2 + k, 1) for k in range(3)]
+    r_big = srv.wait(t_big)
+    assert r_big["status"] == _lib.SS3D_ENOMEM and "budget" in r_big["message"]
+    assert all(srv.wait(t)["status"] == 0 for t in t_small)
+    srv.close()
+
+
+def test_head_of_queue_is_not_starved():
+    big = dict(structs=[(2, 1.0, 30.0, 30.0, 30.0, 0.0, 0.0, 0.0)], nugget=0.0, d=(1, 1, 1), n=(128, 128, 64), ipad=1)
+    small = dict(structs=[(1, 1.0, 5.0, 5.0, 5.0, 0.0, 0.0, 0.0)], nugget=0.0, d=(1, 1, 1), n=(24, 24, 24), ipad=1)
+    srv = _server(slots=2, hbm_budget=1 * GB, max_bypass=3, dry_run_ns_per_cell=1.0)
+    # fill the budget with a first big request, then queue a second big one and many small ones
+    t0 = srv.submit(big, 1, 16)
+    t1 = srv.submit(big, 2, 16)
+    ts = [srv.submit(small, 10 + k, 1) for k in range(20)]
+    r1 = srv.wait(t1)
+    rs = [srv.wait(t) for t in ts]
+    srv.wait(t0)
+    srv.close()
+    passed = sum(1 for r in rs if r["t_admit"] < r1["t_admit"])
+    assert r1["status"] == 0
+    assert passed <= 3 + 1, passed      # max_bypass, plus one admitted before the head was queued behind memory
+
+
+def test_invalid_requests_rejected_at_submit():
+    srv = _server(hbm_budget=GB)
+    good = dict(structs=[(1, 1.0, 5.0, 5.0, 5.0, 0.0, 0.0, 0.0)], nugget=0.0, d=(1, 1, 1), n=(16, 16, 16), ipad=1)
+    with pytest.raises(_lib.SpecsimError):
+        srv.submit(good, 1, 0)
+    with pytest.raises(_lib.SpecsimError):
+        srv.submit(good, 1, 1, igauss=3)
+    bad = dict(good, n=(16, 0, 16))
+    with pytest.raises(_lib.SpecsimError):
+        srv.submit(bad, 1, 1)
+    srv.close()
