@@ -261,8 +261,9 @@ def _serving_cond(model, ndata, seed):
 def bench_serving(ss, rates=(200.0, 1000.0), count=300, slots=8, budget=64 << 30):
     """Serving form on a Poisson request stream (seed 2024) over a pool of 64
     models (seed 2025): grids log-uniform 32..256 per axis, nreal 1..16, 20 %
-    conditional with 200..2000 data, FP32 (FP64 for the conditional ones, whose
-    kriging runs on FP64 fields).  Open loop: a feeder submits each request at its
+    conditional with 200..2000 data, precision form throughout (FP32 synthesis
+    and transforms; the conditional requests' fields are float64 and their
+    kriging solves are FP32 with one FP64 residual refinement).  Open loop: a feeder submits each request at its
     arrival time.  Latency = completion - arrival.  Beside it the plain path,
     one request at a time with no spectra cache (spectrum, realizations and
     conditioning per request): its service times are measured, and its latency
@@ -285,7 +286,7 @@ def bench_serving(ss, rates=(200.0, 1000.0), count=300, slots=8, budget=64 << 30
         return _serving_cond(pool[q["model"]], q["ndata"], 5000 + k) if q["ndata"] else None
 
     def prec_of(q):
-        return ss.FP64 if q["ndata"] else ss.FP32
+        return ss.FP32        # precision form; conditional fields are float64 arrays, kriging FP32 + FP64 refinement
 
     base_reqs = workloads.request_stream(1.0, count=count)
     conds = [cond_of(q, k) for k, q in enumerate(base_reqs)]

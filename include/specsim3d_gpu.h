@@ -252,7 +252,9 @@ int ss3d_condition(double *res, const int n[3], int nreal, const double xmin[3],
  * stream and work space, admit queued requests in arrival order as soon as a
  * slot is free and the request's device footprint (work space, conditioning
  * temporaries, and the spectrum with its build temporaries when the model is
- * not resident) fits the HBM budget; a request that does not fit waits, and
+ * not resident) fits the HBM budget (device memory of the library's own
+ * stream-ordered pool, which keeps up to 4 GiB of freed memory mapped, is not
+ * counted); a request that does not fit waits, and
  * later requests may pass it at most max_bypass times.  Spectra stay resident
  * in an LRU cache keyed by model, grid and ipad.  Each request runs
  * ss3d_spectrum_create (on a cache miss), ss3d_realize and, with data,
@@ -265,8 +267,10 @@ typedef struct ss3d_server_config {
     int max_bypass;              /* passes of a waiting queue head (0: 16) */
     int64_t hbm_budget;          /* device bytes for spectra and work (0: 80 % of free memory) */
     int64_t cache_budget;        /* bytes of idle spectra kept (0: half the budget) */
-    int64_t retain_bytes;        /* work space a slot keeps between requests (0: 1 GiB);
-                                    slots * retain_bytes is reserved out of hbm_budget */
+    int64_t retain_bytes;        /* largest work space a slot keeps between requests
+                                    (0: min(4 GiB, hbm_budget / (2 slots))); kept bytes
+                                    stay charged to the budget, and an idle slot gives
+                                    them back when the queue head does not fit */
     double dry_run_ns_per_cell;  /* > 0: no GPU work, sleeps of this many ns per cell
                                     (scheduler tests); needs an explicit hbm_budget */
 } ss3d_server_config;

@@ -144,6 +144,16 @@ int get_ctx(DevCtx** out) {
     CK(cudaMemcpy(c.twf, hf.data(), sizeof(float2) * ntw, cudaMemcpyHostToDevice));
     CK(cudaMemcpy(c.twd, hd.data(), sizeof(double2) * ntw, cudaMemcpyHostToDevice));
     CK(cudaMemcpy(c.ptab, ht.data(), sizeof(uint32_t) * 3 * 2048, cudaMemcpyHostToDevice));
+    // Work spaces and temporaries come from the device's stream-ordered pool.
+    // Keep up to 4 GiB of freed pool memory mapped between synchronisations,
+    // so that a work space released by one call and taken again by the next
+    // does not pay for unmapping and mapping its pages each time.
+    cudaMemPool_t pool;
+    if (cudaDeviceGetDefaultMemPool(&pool, dev) == cudaSuccess) {
+      uint64_t keep = (uint64_t)4 << 30;
+      cudaMemPoolSetAttribute(pool, cudaMemPoolAttrReleaseThreshold, &keep);
+    }
+    cudaGetLastError();
     c.ready = true;
   }
   *out = &c;
@@ -486,7 +496,7 @@ namespace {
 int work_planes(const Geo& g) { return g.npz > 1 ? g.nz : 1; }
 
 // Work-space layout of one realize call: batches of at most 16 realizations
-// and about 8 GiB; host output goes through two staging buffers.
+// and about 4 GiB; host output goes through two staging buffers.
 struct RealizeLayout {
   int bt;
   size_t per_work, off_work, off_rs, off_apow, off_part, off_zs, off_stage, stage_bytes, total;
@@ -497,7 +507,7 @@ RealizeLayout realize_layout(const Geo& g, bool dbl, bool dev_out, int nreal, si
   const size_t cel = dbl ? sizeof(double2) : sizeof(float2);
   L.per_work = (size_t)work_planes(g) * g.npy * g.HP * cel;
   const int nbx = realize_part_blocks(g, dbl);
-  const size_t budget = (size_t)8 << 30;
+  const size_t budget = (size_t)4 << 30;
   const size_t per_real = L.per_work + (dev_out ? 0 : 2 * M * oel) + (size_t)g.npy * g.npz * 4 + (size_t)nbx * 16;
   L.bt = (int)std::min<size_t>((size_t)std::max(nreal, 1), std::max<size_t>(1, budget / per_real));
   L.bt = std::min(L.bt, 16);

@@ -8,8 +8,13 @@
 // that arrive while others run are admitted as slots and memory free up, and
 // their kernels overlap on the device (continuous batching).
 //
-//   footprint = realization work space (+ conditioning temporaries)
+//   footprint = growth of the slot's realization work space
+//             + conditioning temporaries
 //             + spectrum and its build temporaries when the model is not resident
+//
+// A slot keeps its work space between requests (taking it again costs nothing)
+// up to retain_bytes; what it keeps stays charged to the budget.  When the head
+// of the queue does not fit, an idle slot gives its work space back first.
 //
 // Spectra of models seen before stay resident in an LRU cache keyed by the
 // model, grid and ipad; idle spectra are evicted when an admission needs the
@@ -57,8 +62,9 @@ struct Req {
   std::string key;            // spectrum cache key
   int64_t spec_bytes = 0;     // resident spectrum
   int64_t build_bytes = 0;    // temporaries of a spectrum build
-  int64_t work_bytes = 0;     // realization work space + conditioning temporaries
-  int64_t held = 0;           // bytes charged while the request runs
+  int64_t work_bytes = 0;     // realization work space (kept by the slot afterwards)
+  int64_t tmp_bytes = 0;      // conditioning temporaries
+  int64_t held = 0;           // transient bytes charged while the request runs
   int64_t cells = 0;
   int bypassed = 0;
   bool building = false;      // this request builds the spectrum
@@ -109,7 +115,8 @@ struct ss3d_server {
   std::map<int64_t, Req*> reqs;      // submitted and not yet waited for
   std::map<std::string, Entry> cache;
   int64_t next_ticket = 1;
-  int64_t charged = 0;               // bytes held by running requests
+  int64_t charged = 0;               // running requests' temporaries + slots' work spaces
+  std::vector<int64_t> retained;     // work space kept by each slot
   int64_t cache_bytes = 0;           // bytes of resident (or building) spectra
   uint64_t tick = 0;
   bool stop = false;
@@ -152,16 +159,21 @@ void evict_locked(ss3d_server* s, const std::string& keep, std::vector<ss3d_spec
   }
 }
 
-// First admissible request of the queue, or nullptr.  Called with the lock.
-Req* admit_locked(ss3d_server* s, std::vector<ss3d_spectrum*>& freed) {
+// First admissible request of the queue for slot w, or nullptr.  Called with
+// the lock.  *give_back is set when the head does not fit and slot w keeps a
+// work space that would help.
+Req* admit_locked(ss3d_server* s, int w, std::vector<ss3d_spectrum*>& freed, bool* give_back) {
+  *give_back = false;
   for (size_t i = 0; i < s->queue.size(); ++i) {
     Req* r = s->queue[i];
     auto it = s->cache.find(r->key);
     const bool have = it != s->cache.end();
-    const int64_t need = r->work_bytes + (have ? 0 : r->spec_bytes + r->build_bytes);
-    if (need > s->budget()) {
+    const int64_t grow = std::max<int64_t>(0, r->work_bytes - s->retained[w]);
+    const int64_t need = grow + r->tmp_bytes + (have ? 0 : r->spec_bytes + r->build_bytes);
+    const int64_t alone = r->work_bytes + r->tmp_bytes + (have ? 0 : r->spec_bytes + r->build_bytes);
+    if (alone > s->budget()) {
       s->queue.erase(s->queue.begin() + (long)i);
-      finish_locked(s, r, SS3D_ENOMEM, "request needs " + std::to_string(need) + " bytes of device memory, above "
+      finish_locked(s, r, SS3D_ENOMEM, "request needs " + std::to_string(alone) + " bytes of device memory, above "
                                            "the server's budget of " + std::to_string(s->budget()));
       s->cv.notify_all();
       --i;
@@ -171,8 +183,9 @@ Req* admit_locked(ss3d_server* s, std::vector<ss3d_spectrum*>& freed) {
     if (s->charged + s->cache_bytes + need <= s->budget()) {
       s->queue.erase(s->queue.begin() + (long)i);
       if (i > 0) s->queue.front()->bypassed++;
-      r->held = r->work_bytes + (have ? 0 : r->build_bytes);
-      s->charged += r->held;
+      s->retained[w] += grow;
+      r->held = r->tmp_bytes + (have ? 0 : r->build_bytes);
+      s->charged += grow + r->held;
       if (have) {
         it->second.refs++;
         it->second.last = ++s->tick;
@@ -194,6 +207,7 @@ Req* admit_locked(ss3d_server* s, std::vector<ss3d_spectrum*>& freed) {
       s->stats.running++;
       return r;
     }
+    if (i == 0 && s->retained[w] > 0) *give_back = true;
     // the head does not fit: later requests may pass it a bounded number of times
     if (i == 0 && r->bypassed >= s->cfg.max_bypass) return nullptr;
   }
@@ -254,7 +268,7 @@ int run_request(ss3d_server* s, Req* r, std::string& msg) {
   return rc;
 }
 
-void worker_main(ss3d_server* s) {
+void worker_main(ss3d_server* s, int w) {
   cudaStream_t st = nullptr;
   if (!s->dry) {
     cudaSetDevice(s->dev);
@@ -263,15 +277,31 @@ void worker_main(ss3d_server* s) {
   }
   std::vector<ss3d_spectrum*> freed;
   std::unique_lock<std::mutex> lk(s->mu);
-  for (;;) {
-    Req* r = nullptr;
-    s->cv.wait(lk, [&] { return s->stop || (r = admit_locked(s, freed)) != nullptr; });
-    if (!r) break;
+  auto give_back_workspace = [&] {   // with the lock held; drops and retakes it
+    const int64_t b = s->retained[w];
     lk.unlock();
-    release_spectra(freed);
+    if (!s->dry) ss3d_release_workspace();
+    lk.lock();
+    s->charged -= b;
+    s->retained[w] = 0;
+    s->cv.notify_all();
+  };
+  while (!s->stop) {
+    bool give_back = false;
+    Req* r = admit_locked(s, w, freed, &give_back);
+    if (!freed.empty()) {
+      lk.unlock();
+      release_spectra(freed);
+      lk.lock();
+    }
+    if (!r) {
+      if (give_back) give_back_workspace();
+      else s->cv.wait(lk);
+      continue;
+    }
+    lk.unlock();
     std::string msg;
     const int rc = run_request(s, r, msg);
-    if (!s->dry && r->work_bytes > s->cfg.retain_bytes) ss3d_release_workspace();
     lk.lock();
     s->charged -= r->held;
     r->held = 0;
@@ -288,12 +318,11 @@ void worker_main(ss3d_server* s) {
     evict_locked(s, std::string(), freed, [&] { return s->cache_bytes <= s->cfg.cache_budget; });
     finish_locked(s, r, rc, msg);
     s->cv.notify_all();
-    if (!freed.empty()) {
-      lk.unlock();
-      release_spectra(freed);
-      lk.lock();
-    }
+    if (s->retained[w] > s->cfg.retain_bytes) give_back_workspace();
   }
+  const int64_t b = s->retained[w];
+  s->charged -= b;
+  s->retained[w] = 0;
   lk.unlock();
   release_spectra(freed);
   if (!s->dry) {
@@ -323,16 +352,12 @@ extern "C" int ss3d_server_create(const ss3d_server_config* cfg, ss3d_server** o
     delete s;
     return set_error(SS3D_EINVAL, "dry run needs an explicit hbm_budget");
   }
-  if (s->cfg.retain_bytes <= 0) s->cfg.retain_bytes = (int64_t)1 << 30;
-  // work spaces kept by idle slots are reserved out of the budget
-  s->cfg.hbm_budget -= (int64_t)s->cfg.slots * s->cfg.retain_bytes;
-  if (s->cfg.hbm_budget <= 0) {
-    delete s;
-    return set_error(SS3D_EINVAL, "hbm_budget below the work spaces kept by the slots (slots * retain_bytes)");
-  }
+  if (s->cfg.retain_bytes <= 0)
+    s->cfg.retain_bytes = std::min<int64_t>((int64_t)4 << 30, s->cfg.hbm_budget / (2 * s->cfg.slots));
   if (s->cfg.cache_budget <= 0) s->cfg.cache_budget = s->cfg.hbm_budget / 2;
   if (s->cfg.max_bypass <= 0) s->cfg.max_bypass = 16;
-  for (int w = 0; w < s->cfg.slots; w++) s->workers.emplace_back(worker_main, s);
+  s->retained.assign(s->cfg.slots, 0);
+  for (int w = 0; w < s->cfg.slots; w++) s->workers.emplace_back(worker_main, s, w);
   *out = s;
   return SS3D_OK;
 }
@@ -376,8 +401,8 @@ extern "C" int ss3d_server_submit(ss3d_server* s, const ss3d_request* q, int64_t
   r->work_bytes = realize_bytes_for(np, q->n, q->nreal, q->precision, host_out ? 1 : 0);
   if (cond) {
     const int64_t per_node = 4LL * q->cp->ndmax + 4;
-    r->work_bytes += (host_out ? M * q->nreal * 8 : 0) + std::min<int64_t>(M, ((int64_t)1 << 30) / per_node) * per_node +
-                     (int64_t)q->nrows * (8LL * q->nreal + 96) + (1 << 20);
+    r->tmp_bytes = (host_out ? M * q->nreal * 8 : 0) + std::min<int64_t>(M, ((int64_t)1 << 30) / per_node) * per_node +
+                   (int64_t)q->nrows * (8LL * q->nreal + 96) + (1 << 20);
   }
   r->cells = M * q->nreal;
   std::lock_guard<std::mutex> lk(s->mu);
@@ -408,7 +433,7 @@ extern "C" int ss3d_server_wait(ss3d_server* s, int64_t ticket, ss3d_result* res
     res->t_submit = r->t_submit;
     res->t_admit = r->t_admit;
     res->t_done = r->t_done;
-    res->footprint = r->work_bytes + (r->building ? r->spec_bytes + r->build_bytes : 0);
+    res->footprint = r->work_bytes + r->tmp_bytes + (r->building ? r->spec_bytes + r->build_bytes : 0);
   }
   const int rc = r->status;
   const std::string msg = r->msg;

@@ -90,3 +90,23 @@ def test_invalid_requests_rejected_at_submit():
     with pytest.raises(_lib.SpecsimError):
         srv.submit(bad, 1, 1)
     srv.close()
+
+
+def test_idle_slots_give_back_work_space():
+    """Slots keep their work spaces between requests; a large request that only
+    fits once they give them back must still run."""
+    med = dict(structs=[(1, 1.0, 10.0, 10.0, 10.0, 0.0, 0.0, 0.0)], nugget=0.0, d=(1, 1, 1), n=(96, 96, 96), ipad=1)
+    big = dict(structs=[(1, 1.0, 20.0, 20.0, 20.0, 0.0, 0.0, 0.0)], nugget=0.0, d=(1, 1, 1), n=(200, 200, 200), ipad=1)
+    probe = _server(slots=1, hbm_budget=64 * GB)
+    fp_med = probe.wait(probe.submit(med, 1, 16))["footprint"]
+    fp_big = probe.wait(probe.submit(big, 1, 16))["footprint"]
+    probe.close()
+    budget = fp_big + fp_med // 2
+    srv = _server(slots=4, hbm_budget=budget, retain_bytes=budget, cache_budget=1)
+    ts = [srv.submit(med, 10 + k, 16) for k in range(8)]
+    tb = srv.submit(big, 3, 16)
+    res = [srv.wait(t) for t in ts] + [srv.wait(tb)]
+    st = srv.stats()
+    srv.close()
+    assert all(r["status"] == 0 for r in res), [r["message"] for r in res if r["status"]]
+    assert st["peak_bytes"] <= st["budget_bytes"]

@@ -111,10 +111,10 @@ def test_mix_equals_alone():
 
 def test_mix_equals_alone_under_tight_budget():
     """A budget that admits about one request at a time (the largest of these
-    needs 22 MB), and a cache smaller than one spectrum: admissions wait and
+    needs 27 MB with host output), and a cache smaller than one spectrum: admissions wait and
     spectra are rebuilt, results do not change."""
     reqs = _requests(10, seed=11)
-    got, res, st = _run_mix(reqs, slots=3, hbm_budget=3 * (1 << 20) + (24 << 20), cache_budget=1,
+    got, res, st = _run_mix(reqs, slots=3, hbm_budget=3 * (1 << 20) + (48 << 20), cache_budget=1,
                             retain_bytes=1 << 20)
     assert all(r["status"] == 0 for r in res), [r["message"] for r in res if r["status"]]
     assert st["peak_bytes"] <= st["budget_bytes"]
