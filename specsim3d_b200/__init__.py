@@ -328,9 +328,10 @@ class Server:
     resident (LRU, ``cache_budget`` bytes of idle spectra).  ``dry_run_ns_per_cell``
     > 0 replaces the GPU work by sleeps (scheduler tests without a GPU)."""
 
-    def __init__(self, slots=4, hbm_budget=0, cache_budget=0, retain_bytes=0, max_bypass=0, dry_run_ns_per_cell=0.0):
-        cfg = L.ServerConfig(int(slots), int(max_bypass), int(hbm_budget), int(cache_budget), int(retain_bytes),
-                             float(dry_run_ns_per_cell))
+    def __init__(self, slots=4, hbm_budget=0, cache_budget=0, retain_bytes=0, max_bypass=0, max_cond=0,
+                 dry_run_ns_per_cell=0.0):
+        cfg = L.ServerConfig(int(slots), int(max_bypass), int(max_cond), int(hbm_budget), int(cache_budget),
+                             int(retain_bytes), float(dry_run_ns_per_cell))
         h = ctypes.c_void_p()
         L.check(L.lib().ss3d_server_create(ctypes.byref(cfg), ctypes.byref(h)))
         self._h = h

@@ -21,7 +21,9 @@
 // memory or when the cache exceeds its own budget.  A request whose spectrum
 // is being built by another slot waits for that build instead of repeating it.
 // When the head of the queue does not fit, later requests that fit may pass it,
-// at most max_bypass times, so that a large request is never starved.
+// at most max_bypass times, so that a large request is never starved.  At most
+// max_cond conditional requests run at once: their search and kriging kernels
+// fill the GPU by themselves, and several of them only contend.
 //
 // The stages are the library's own entry points (ss3d_spectrum_create,
 // ss3d_realize, ss3d_condition), so a request's result does not depend on what
@@ -116,6 +118,7 @@ struct ss3d_server {
   std::map<std::string, Entry> cache;
   int64_t next_ticket = 1;
   int64_t charged = 0;               // running requests' temporaries + slots' work spaces
+  int cond_running = 0;              // conditional requests on the GPU
   std::vector<int64_t> retained;     // work space kept by each slot
   int64_t cache_bytes = 0;           // bytes of resident (or building) spectra
   uint64_t tick = 0;
@@ -179,6 +182,13 @@ Req* admit_locked(ss3d_server* s, int w, std::vector<ss3d_spectrum*>& freed, boo
       --i;
       continue;
     }
+    // conditional requests fill the GPU with their search and kriging
+    // kernels: at most max_cond of them run at once, the other slots keep
+    // serving unconditional requests beside them
+    if (r->cond && s->cond_running >= s->cfg.max_cond) {
+      if (i == 0 && r->bypassed >= s->cfg.max_bypass) return nullptr;
+      continue;
+    }
     evict_locked(s, r->key, freed, [&] { return s->charged + s->cache_bytes + need <= s->budget(); });
     if (s->charged + s->cache_bytes + need <= s->budget()) {
       s->queue.erase(s->queue.begin() + (long)i);
@@ -201,6 +211,7 @@ Req* admit_locked(ss3d_server* s, int w, std::vector<ss3d_spectrum*>& freed, boo
         r->building = true;
         s->stats.cache_misses++;
       }
+      if (r->cond) s->cond_running++;
       r->t_admit = s->now();
       s->stats.peak_bytes = std::max(s->stats.peak_bytes, s->charged + s->cache_bytes);
       s->stats.peak_running = std::max<int64_t>(s->stats.peak_running, s->stats.running + 1);
@@ -306,6 +317,7 @@ void worker_main(ss3d_server* s, int w) {
     s->charged -= r->held;
     r->held = 0;
     s->stats.running--;
+    if (r->cond) s->cond_running--;
     auto it = s->cache.find(r->key);
     if (it != s->cache.end()) {
       it->second.refs--;
@@ -356,6 +368,7 @@ extern "C" int ss3d_server_create(const ss3d_server_config* cfg, ss3d_server** o
     s->cfg.retain_bytes = std::min<int64_t>((int64_t)4 << 30, s->cfg.hbm_budget / (2 * s->cfg.slots));
   if (s->cfg.cache_budget <= 0) s->cfg.cache_budget = s->cfg.hbm_budget / 2;
   if (s->cfg.max_bypass <= 0) s->cfg.max_bypass = 16;
+  if (s->cfg.max_cond <= 0) s->cfg.max_cond = 1;
   s->retained.assign(s->cfg.slots, 0);
   for (int w = 0; w < s->cfg.slots; w++) s->workers.emplace_back(worker_main, s, w);
   *out = s;
