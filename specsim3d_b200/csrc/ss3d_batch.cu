@@ -79,10 +79,14 @@ __device__ __forceinline__ void run_item(const BJob& J, int local, const Tw& tw,
   if constexpr (PASS == 0) {
     const AxisArgs A = J.A;
     switch (J.LA) {
-#define SS3D_BA(L)                                                                                     \
-  case L:                                                                                              \
-    colgen_body<float, L, BCfg<L, ETV>::TX, BCfg<L, ETV>::TPC>(A, g, J.amp, J.rs, J.apow, J.work, tw, \
-                                                               local, sm);                            \
+#define SS3D_BA(L)                                                                                          \
+  case L:                                                                                                   \
+    if (g.d == 2)                                                                                           \
+      colgen_body<float, L, BCfg<L, ETV>::TX, BCfg<L, ETV>::TPC, 1>(A, g, J.amp, J.rs, J.apow, J.work, tw, \
+                                                                    local, sm);                            \
+    else                                                                                                    \
+      colgen_body<float, L, BCfg<L, ETV>::TX, BCfg<L, ETV>::TPC, 0>(A, g, J.amp, J.rs, J.apow, J.work, tw, \
+                                                                    local, sm);                            \
     break;
       SS3D_BA(4) SS3D_BA(5) SS3D_BA(6) SS3D_BA(7) SS3D_BA(8) SS3D_BA(9) SS3D_BA(10)
 #undef SS3D_BA

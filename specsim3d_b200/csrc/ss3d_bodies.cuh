@@ -73,19 +73,65 @@ __device__ __forceinline__ void col_body(const AxisArgs& a, const Geo& g, const 
   C* dst = out + ((long long)grp * a.gstride + line0 + t + (long long)r * a.rstride);
   const int S = (int)a.S;   // offsets inside one realization's grid fit in 32 bits
   const int nout = a.nout;
+  constexpr int NR0 = N / Sched<LOGN>::radix(0);
   for (int q = threadIdx.x; q < N; q += NTH) stw[q] = twtab<R>(tw)[N - 1 + q];
   __syncthreads();
   fft_tile<LOGN, TX, TPC, SIGN>(
-      s, stw, [&](int pos) { return valid ? src[pos * S] : cmk<C>(R(0), R(0)); },
+      s, stw, [&](int jb, int r) { return valid ? src[(jb + r * NR0) * S] : cmk<C>(R(0), R(0)); },
       [&](int pos, C v) {
         if (valid && pos < nout) dst[pos * S] = v;
       });
 }
 
+// Coefficient from the Park-Miller state s1 of its first draw (f90:1312-1331):
+// GAUSS 1: amp (g1 + i g2) sqrt(1/2) from the Box-Muller pair of draws s1, s1 a;
+// GAUSS 0: amp e^{i phi}, phi = 2 pi u(s1).  A self-conjugate index takes
+// amp g1 (Gaussian) or +/-amp (phases: + when u < 1/2); conj gives the
+// conjugate (index whose draw belongs to its partner).  Branch-free.
+template <typename R, int GAUSS>
+__device__ __forceinline__ cpx_t<R> coef_from_state(uint32_t s1, R am, bool self, bool conj) {
+  using C = cpx_t<R>;
+  if constexpr (GAUSS) {
+    const uint32_t s2 = pm_mulmod(s1, PM_A);
+    if constexpr (sizeof(R) == 4) {
+      const float L = m2log_f(s1);
+      const float rr = L * rsqrtf(L);
+      float cs, sn;
+      phasor_f(s2, cs, sn);
+      const float a = self ? am : am * 0.70710678118654752f;
+      const float re = a * (rr * cs);
+      const float im = (conj ? -a : a) * (rr * sn);
+      return cmk<C>(re, self ? 0.f : im);
+    } else {
+      const double rr = sqrt(m2log_d(s1));
+      double cs, sn;
+      phasor_d(s2, cs, sn);
+      const double g1 = rr * cs, g2 = rr * sn;
+      const double h = 0.70710678118654757;   // sqrt(0.5d0)
+      const double re = self ? am * g1 : am * g1 * h;
+      const double im = am * (conj ? -g2 : g2) * h;
+      return cmk<C>(re, self ? 0.0 : im);
+    }
+  } else {
+    R cs, sn;
+    if constexpr (sizeof(R) == 4) phasor_f(s1, cs, sn); else phasor_d(s1, cs, sn);
+    const R sgn = (2ull * s1) < (uint64_t)PM_M ? am : -am;   // urand() < 0.5
+    const R re = self ? sgn : am * cs;
+    const R im = conj ? -(am * sn) : am * sn;
+    return cmk<C>(re, self ? R(0) : im);
+  }
+}
+
 // First inverse pass with the coefficient synthesis fused into the loader.
 // axis 2: columns are (i, j) plane offsets, positions k;  axis 1 (npz = 1):
-// columns are i, positions j.
-template <typename R, int LOGN, int TX, int TPC>
+// columns are i, positions j.  Along the transformed axis (length N) the
+// position p and its conjugate partner pp = (N - p) mod N decide which draw a
+// coefficient takes: p < N/2 its own row's (less), p > N/2 the partner row's
+// (conjugated), and p in {0, N/2} (partner = itself) the other index decides,
+// as the reference's lin/linp comparison (f90:1315-1331) does.  The pass-0
+// loader sees p = jb + r N/R0 with r constant, so only the two slots r = 0 and
+// r = R0/2 of the butterflies with jb = 0 need a run-time decision.
+template <typename R, int LOGN, int TX, int TPC, int GAUSS>
 __device__ __forceinline__ void colgen_body(const AxisArgs& a, const Geo& g, const R* __restrict__ amp,
                                             const uint32_t* __restrict__ rowstates,
                                             const uint32_t* __restrict__ apow, cpx_t<R>* out, const Tw& tw,
@@ -93,6 +139,8 @@ __device__ __forceinline__ void colgen_body(const AxisArgs& a, const Geo& g, con
   using C = cpx_t<R>;
   constexpr int N = 1 << LOGN;
   constexpr int NTH = TX * TPC;
+  constexpr int R0 = Sched<LOGN>::radix(0);
+  constexpr int NR0 = N / R0;
   C* s = reinterpret_cast<C*>(smraw);
   C* stw = s + N * TX;
   const int r = item % a.nreal;
@@ -102,33 +150,48 @@ __device__ __forceinline__ void colgen_body(const AxisArgs& a, const Geo& g, con
   const int t = threadIdx.x % TX;
   const int line = line0 + t;
   const bool valid = line_valid(g, line, a.lines);
-  int i, j0;
-  if (a.axis == 2) {
-    i = line % g.HP;
-    j0 = line / g.HP;
-  } else {
-    i = line;
-    j0 = 0;
-  }
+  const bool zaxis = a.axis == 2;
+  int i = zaxis ? line % g.HP : line;
+  const int j0 = zaxis ? line / g.HP : 0;
   if (!valid) i = 0;
   const uint32_t ai = __ldg(apow + i), aip = __ldg(apow + ((g.npx - i) & (g.npx - 1)));
   const bool iedge = (i == 0) || (2 * i == g.npx);
+  // z pass: rows (j0, p) and (jp0, pp); y pass (2D): rows p and pp of plane 0
+  const int jp0 = (-j0) & (g.npy - 1);
+  const bool cgt = zaxis && j0 > jp0;                      // mid positions: partner's draw
+  const bool selfcol = (!zaxis || j0 == jp0) && iedge;     // mid positions: self-conjugate
+  const int rowstride = zaxis ? g.npy : 1;
   const uint32_t* rs = rowstates + (size_t)r * g.npy * g.npz;
+  const uint32_t* rs_own = rs + (zaxis ? j0 : 0);
+  const uint32_t* rs_par = rs + (zaxis ? jp0 : 0);
   const long long cbase = (long long)grp * a.gstride + line;
   const R* ap = amp + cbase;
   C* dst = out + cbase + (long long)r * a.rstride;
   const int S = (int)a.S;   // offsets inside one realization's grid fit in 32 bits
   const int nout = a.nout;
-  const bool zaxis = a.axis == 2;
   for (int q = threadIdx.x; q < N; q += NTH) stw[q] = twtab<R>(tw)[N - 1 + q];
   __syncthreads();
   fft_tile<LOGN, TX, TPC, +1>(
       s, stw,
-      [&](int pos) {
+      [&](int jb, int rr) {
         if (!valid) return cmk<C>(R(0), R(0));
-        const R am = __ldg(ap + pos * S);
-        return zaxis ? coef_col<R>(g, j0, pos, am, rs, ai, aip, iedge)
-                     : coef_col<R>(g, pos, grp, am, rs, ai, aip, iedge);
+        const int p = jb + rr * NR0;
+        const R am = __ldg(ap + p * S);
+        bool greater, mid;
+        if (rr == 0) {                 // p < N/R0 <= N/2; p = 0 when jb = 0
+          mid = jb == 0;
+          greater = mid && cgt;
+        } else if (2 * rr == R0) {     // p >= N/2; p = N/2 when jb = 0
+          mid = jb == 0;
+          greater = !mid || cgt;
+        } else {
+          mid = false;
+          greater = 2 * rr > R0;
+        }
+        const int pp = (N - p) & (N - 1);
+        const uint32_t st = __ldg(greater ? rs_par + pp * rowstride : rs_own + p * rowstride);
+        const uint32_t s1 = pm_mulmod(st, greater ? aip : ai);
+        return coef_from_state<R, GAUSS>(s1, am, mid && selfcol, greater);
       },
       [&](int pos, C v) {
         if (valid && pos < nout) dst[pos * S] = v;
@@ -187,8 +250,10 @@ __device__ __forceinline__ void fft_rows_inv(cpx_t<R>* s, const cpx_t<R>* twN) {
   static_assert(TX * TPC >= 32, "row tile needs at least one warp");
   if constexpr (LOGN > 0) {
     const int t = threadIdx.x % TX;
+    constexpr int NR0 = (1 << LOGN) / Sched<LOGN>::radix(0);
     fft_tile<LOGN, TX, TPC, +1, PITCH, true, true>(
-        s, twN, [&](int pos) { return s[pos * PITCH + t]; }, [&](int pos, C v) { s[pos * PITCH + t] = v; });
+        s, twN, [&](int jb, int r) { return s[(jb + r * NR0) * PITCH + t]; },
+        [&](int pos, C v) { s[pos * PITCH + t] = v; });
     __syncthreads();
   }
 }

@@ -114,17 +114,15 @@ __host__ __device__ __forceinline__ int row_class(const Geo& g, int j, int k) {
 
 // ---------------------------------------------------------------- coefficient synthesis
 // Unit phasor e^{2 pi i s/m} in float.  The nearest quarter turn n is taken
-// in integers (exact), the remainder |x| <= pi/4 goes through Taylor
-// polynomials of sin (to x^9) and cos (to x^8): truncation below 3e-8, argument
-// error below 5e-8 (one float rounding of the exact integer remainder).
+// in integers (exact); the remainder |x| <= pi/4 (argument error below 5e-8:
+// one float rounding of the exact integer remainder) goes through the hardware
+// sine and cosine (__sincosf, absolute error about 5e-7 on this range).
 __device__ __forceinline__ void phasor_f(uint32_t s, float& c, float& sn) {
   const int n = __float2int_rn((float)s * (4.0f / 2147483647.0f));   // nearest quarter (off by one at most)
   const int rem = (int)(4u * s - (uint32_t)n * PM_M);                // exact 4s - n m, |.| <= m/2 + 2^11
   const float x = (float)rem * 7.3145904e-10f;                         // (pi/2) / (2^31-1)
-  const float x2 = x * x;
-  const float sp = x * fmaf(x2, fmaf(x2, fmaf(x2, fmaf(x2, 2.7557319e-6f, -1.9841270e-4f), 8.3333333e-3f),
-                                     -1.6666667e-1f), 1.0f);
-  const float cp = fmaf(x2, fmaf(x2, fmaf(x2, fmaf(x2, 2.4801587e-5f, -1.3888889e-3f), 4.1666667e-2f), -0.5f), 1.0f);
+  float sp, cp;
+  __sincosf(x, &sp, &cp);
   // rotate by n quarter turns: (c, s) -> (cp, sp), (-sp, cp), (-cp, -sp), (sp, -cp)
   const bool odd = n & 1;
   const float c0 = odd ? sp : cp, s0 = odd ? cp : sp;

@@ -69,6 +69,10 @@ __device__ __forceinline__ void fft_tile_rest(C* __restrict__ s, const C* __rest
 }
 
 
+// load(jb, r) returns the input at position jb + r * N / R0 (R0 the radix of
+// pass 0); r is a constant after unrolling, so a loader can resolve anything
+// that depends on which part of the transform the position lies in at compile
+// time.  store(pos, v) receives the output at position pos.
 // PITCH: shared-memory row pitch (>= TX).  LOAD_SYNC: barrier between the
 // pass-0 loads and the pass-0 shared-memory writes (loader reads s).
 // STORE_SYNC: barrier before the final stores (storer writes s).
@@ -91,7 +95,7 @@ __device__ __forceinline__ void fft_tile(C* __restrict__ s, const C* __restrict_
     for (int m = 0; m < NBT; ++m) {
       const int jb = c + TPC * m;
 #pragma unroll
-      for (int r = 0; r < R; ++r) v[m * R + r] = load(jb + r * (N / R));
+      for (int r = 0; r < R; ++r) v[m * R + r] = load(jb, r);   // position jb + r * N / R
     }
 #pragma unroll
     for (int m = 0; m < NBT; ++m) dftR<R, SIGN>(&v[m * R]);

@@ -67,14 +67,15 @@ __global__ void __launch_bounds__(ColCfg<R, LOGN, V>::NTH) k_col(AxisArgs a, Geo
 }
 
 // first inverse pass with the coefficient synthesis fused into the loader
-template <typename R, int LOGN, int V>
+// (GAUSS: igauss of the realizations, 0 phases, 1 Gaussian coefficients)
+template <typename R, int LOGN, int V, int GAUSS>
 __global__ void __launch_bounds__(ColCfg<R, LOGN, V>::NTH) k_colgen(AxisArgs a, Geo g, const R* __restrict__ amp,
                                                                    const uint32_t* __restrict__ rowstates,
                                                                    const uint32_t* __restrict__ apow, cpx_t<R>* out,
                                                                    Tw tw) {
   extern __shared__ __align__(16) unsigned char smraw[];
   using CF = ColCfg<R, LOGN, V>;
-  colgen_body<R, LOGN, CF::TX, CF::TPC>(a, g, amp, rowstates, apow, out, tw, blockIdx.x, smraw);
+  colgen_body<R, LOGN, CF::TX, CF::TPC, GAUSS>(a, g, amp, rowstates, apow, out, tw, blockIdx.x, smraw);
 }
 
 // Standalone synthesis of the full half spectrum of nreal realizations.
@@ -396,12 +397,13 @@ static cudaError_t run_axis_gen_v(const AxisArgs& a, const Geo& g, const R* amp,
     return cudaErrorInvalidValue;
   } else {
     size_t smem = (size_t)(CF::N * CF::TX + CF::N) * sizeof(cpx_t<R>);
-    cudaError_t e = set_smem(k_colgen<R, L, V>, smem);
+    auto kern = g.d == 2 ? k_colgen<R, L, V, 1> : k_colgen<R, L, V, 0>;
+    cudaError_t e = set_smem(kern, smem);
     if (e != cudaSuccess) return e;
     AxisArgs b = a;
     b.tpg = (a.lines + CF::TX - 1) / CF::TX;
     unsigned blocks = (unsigned)((long long)b.tpg * a.ngroups * a.nreal);
-    k_colgen<R, L, V><<<blocks, CF::NTH, smem, st>>>(b, g, amp, rs, apow, out, tw);
+    kern<<<blocks, CF::NTH, smem, st>>>(b, g, amp, rs, apow, out, tw);
     ++g_launch_count;
     return cudaGetLastError();
   }

@@ -163,3 +163,17 @@ def test_tile_variants_give_identical_results(gpu):
     chosen = gpu.autotune(sp, 1, gpu.FP32, 2)
     assert set(chosen.values()) <= {0, 1, 2, 3}
     assert np.array_equal(sp.realize(77, 2, 1, gpu.FP32), sp.realize(77, 2, 1, gpu.FP32))
+
+
+@pytest.mark.parametrize("case", [0, 1, 2])
+@pytest.mark.parametrize("igauss", [0, 1])
+def test_coefficients_fp32(gpu, case, igauss):
+    """FP32 synthesis: hardware sine/cosine after an exact integer quarter-turn
+    reduction, series logarithm near u = 1; every coefficient within 2e-6 of
+    the largest against the oracle's FP64 values."""
+    n, sts, nug, d, ipad = CASES[case]
+    sp = gpu.Spectrum(sts, nug, d, n, ipad)
+    amp_o, _ = ora.spectrum(sts, nug, d, sp.np)
+    co = recipes.half_of_full(ora.coefficients(amp_o, sp.np, 8080 + case, 1, igauss), sp.np[0])
+    cg = sp.debug_coefficients(8080 + case, 1, igauss, gpu.FP32)
+    assert np.max(np.abs(cg - co)) <= 2e-6 * np.max(np.abs(co))
