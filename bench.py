@@ -361,6 +361,78 @@ def bench_serving(ss, rates=(200.0, 1000.0), count=300, slots=8, budget=64 << 30
     return out
 
 
+def bench_conditional(ss, stream):
+    """Conditional configuration: 128x128x64, exponential sill 1 nugget 0.05
+    ranges 40/20/8 azimuth 60; truth = realization of seed 4242 (igauss 0); 2,000
+    data at uniform-random locations (seed 99) with values exp(0.5 z) of the
+    truth, normal-score transform and back transform (zmax = 2 max, linear
+    tails); search = the ranges, ndmax 24; 16 realizations of seed 4243.  FP64
+    kriging against FP32 solves with one FP64-residual refinement: time per call
+    (realizations excluded) and the difference of the conditioned fields
+    relative to their standard deviation."""
+    import torch
+    n = (128, 128, 64)
+    structs = [(2, 1.0, 40.0, 20.0, 8.0, 60.0, 0.0, 0.0)]
+    sp = ss.Spectrum(structs, 0.05, (1.0, 1.0, 1.0), n, 1)
+    truth = sp.realize(4242, 1, 0, ss.FP64)[0]
+    rng = np.random.default_rng(99)
+    xyz = np.stack([rng.uniform(0, n[a] - 1, 2000) for a in range(3)], axis=1)
+    ix = np.rint(xyz).astype(int)
+    val = np.exp(0.5 * truth[ix[:, 2], ix[:, 1], ix[:, 0]])
+    rows = np.column_stack([xyz, val])
+    params = dict(ixc=1, iyc=2, izc=3, ivc=4, iwc=0, tmin=-1e21, tmax=1e21, itrans=1, skmean=0.0, zmin=0.0,
+                  zmax=2.0 * float(val.max()), ltail=1, ltpar=0.0, utail=1, utpar=0.0, radius=(40.0, 20.0, 8.0),
+                  angles=(60.0, 0.0, 0.0), ndmax=24)
+    fields = {}
+    times = {}
+    for name, prec in (("fp64", ss.FP64), ("fp32", ss.FP32)):
+        f = torch.empty((16, n[2], n[1], n[0]), dtype=torch.float64, device="cuda")
+        ts = []
+        for rep in range(3):
+            sp.realize(4243, 16, 0, ss.FP64, out=f)
+            torch.cuda.synchronize()
+            t0 = time.perf_counter()
+            st, _ = ss.condition(f, (0.0, 0.0, 0.0), (1.0, 1.0, 1.0), structs, 0.05, params, rows, prec)
+            torch.cuda.synchronize()
+            ts.append(time.perf_counter() - t0)
+        times[name] = min(ts)
+        fields[name] = f
+    d = (fields["fp32"] - fields["fp64"]).abs_()
+    sd = float(fields["fp64"].std().item())
+    M = n[0] * n[1] * n[2]
+    out = {"workload": "128x128x64, exponential 40/20/8 az 60, nugget 0.05, 2,000 data (seed 99) from the seed-4242 "
+                       "truth through exp(0.5 z), nscore + backtr, ndmax 24, 16 realizations (seed 4243)",
+           "fp64_ms": round(times["fp64"] * 1e3, 3), "fp32_ms": round(times["fp32"] * 1e3, 3),
+           "mcells_s_fp32": round(M * 16 / times["fp32"] / 1e6, 1),
+           "neighbours_total": st["nsum"], "regularised_systems": st["nfail"],
+           "fp32_vs_fp64": {"max_abs_over_sd": float(d.amax().item()) / sd,
+                            "rms_over_sd": float(d.pow_(2).mean().sqrt().item()) / sd, "target": 1e-5}}
+    sp.close()
+    return out
+
+
+def bench_vario(ss, sp, nreal, seed, igauss):
+    """--vario on the precision configuration: directions (1,0,0), (0,1,0),
+    (0,0,1), lags 1..100, FP64 sums over all node pairs of the FP64
+    realizations; exact pair counts."""
+    import torch
+    n = sp.n
+    f = torch.empty((nreal, n[2], n[1], n[0]), dtype=torch.float64, device="cuda")
+    sp.realize(seed, nreal, igauss, ss.FP64, out=f)
+    dirs = [(1, 0, 0, 100), (0, 1, 0, 100), (0, 0, 1, 100)]
+    ts = []
+    for rep in range(3):
+        torch.cuda.synchronize()
+        t0 = time.perf_counter()
+        gam, npairs = ss.vario(f, dirs)
+        ts.append(time.perf_counter() - t0)
+    pairs = int(npairs.sum()) * nreal
+    t = min(ts)
+    return {"workload": "256^3, 8 FP64 realizations, directions x, y, z, lags 1..100", "ms": round(t * 1e3, 3),
+            "pairs": pairs, "gpairs_s": round(pairs / t / 1e9, 2), "fp64_gflop_s": round(3 * pairs / t / 1e9, 1),
+            "pair_count_check": int(npairs[0, 0]) == (n[0] - 1) * n[1] * n[2]}
+
+
 def run_ours(args):
     import torch
     import torch.distributed as dist
@@ -380,7 +452,7 @@ def run_ours(args):
     n = WL["n"]
     nreal = WL["nreal"]
     M = cells_per_real()
-    r_first = rank * nreal
+    r_first, _ = ss.shard(rank, world, nreal)
     sp = ss.Spectrum(WL["structs"], WL["nugget"], WL["d"], n, WL["ipad"])
     c0 = sp.stats["c0"]
     out32 = torch.empty((nreal, n[2], n[1], n[0]), dtype=torch.float32, device=dev)
@@ -456,18 +528,22 @@ def run_ours(args):
     host = torch.empty((nreal, n[2], n[1], n[0]), dtype=torch.float32).pin_memory()
     hn = host.numpy()
     ke = max(1, min(k, 5))
-    ts = []
+    ts, parts = [], []
     for s in range(ke + 1):
         torch.cuda.synchronize()
         barrier()
         t0 = time.perf_counter()
         spe = ss.Spectrum(WL["structs"], WL["nugget"], WL["d"], n, WL["ipad"])
-        spe.realize(WL["seed"], nreal, WL["igauss"], ss.FP32, r_first=r_first, out=hn)
-        spe.close()
         t1 = time.perf_counter()
+        spe.realize(WL["seed"], nreal, WL["igauss"], ss.FP32, r_first=r_first, out=hn)
+        t2 = time.perf_counter()
+        spe.close()
+        t3 = time.perf_counter()
         if s > 0:
-            ts.append(t1 - t0)
+            ts.append(t3 - t0)
+            parts.append((t1 - t0, t2 - t1, t3 - t2))
     e2e_s = float(np.mean(ts))
+    e2e_parts = np.mean(np.array(parts), axis=0) * 1e3
     if world > 1:
         t = torch.tensor([e2e_s], device=dev, dtype=torch.float64)
         dist.all_reduce(t, op=dist.ReduceOp.MAX)
@@ -518,7 +594,8 @@ def run_ours(args):
         "clocks": clocks,
         "e2e": {"value": round(M * nreal * world / e2e_s / 1e6, 1), "unit": "Mcells/s",
                 "h2d_bytes_per_step": 0, "d2h_bytes_per_step": int(M * nreal * 4),
-                "includes": "spectrum build + realizations + D2H into pinned host memory (ss3d_realize)"},
+                "includes": "spectrum build + realizations + D2H into pinned host memory (ss3d_realize)",
+                "ms_spectrum_realize_free": [round(float(x), 3) for x in e2e_parts]},
         "gpu_launches": int(launches),
         "stages_ms_per_step_serialized": {kk: round(v[0] / kprof, 4) for kk, v in stages.items()},
         "roofline": {"bound": "hbm", "achieved": round(achieved, 1), "peak": peak, "unit": "GB/s",
@@ -535,6 +612,9 @@ def run_ours(args):
         line["mixed_grids"] = bench_mixed_grids(ss, stream)
     if world == 1 and not args.no_serving:
         line["serving"] = bench_serving(ss)
+    if world == 1 and not args.no_batch:
+        line["conditional"] = bench_conditional(ss, stream)
+        line["vario"] = bench_vario(ss, sp, nreal, WL["seed"], WL["igauss"])
     if rank == 0 and world == 1 and not args.no_cpu_baseline:
         try:
             sec, t_spec, cores, _ = cpu_reference_sample(1, 0)

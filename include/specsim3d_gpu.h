@@ -113,6 +113,13 @@ int ss3d_spectrum_amp(const ss3d_spectrum *sp, double *amp);
 int ss3d_realize(const ss3d_spectrum *sp, int iseed, int64_t r_first, int nreal, int igauss, int precision,
                  void *out, int out_dtype, double *zstats);
 
+/* State of the reference's Park-Miller stream right after the first draw of
+ * row (j, k) (0-based) of realization r (0-based) on the periodic grid np, as
+ * the realization kernels compute it by jump-ahead (host only, no GPU).  The
+ * reference draws this stream serially (f90:1302-1334); the function lets a
+ * host plan and check a split of realizations over processes or GPUs. */
+int ss3d_row_state(const int np[3], int igauss, int iseed, int64_t r, int j, int k, uint32_t *state);
+
 /* Test hooks for the synthesis (host output arrays, half spectrum [k][j][i],
  * i < npx/2+1):
  *   ss3d_debug_states: Park-Miller state after the first draw that produced

@@ -23,7 +23,7 @@ import numpy as np
 from . import _lib as L
 from ._lib import FP32, FP64, OUT_F32, OUT_F64, SpecsimError
 
-__all__ = ["Spectrum", "Batch", "Server", "grid_size", "covariance", "setrot", "vario", "condition", "FP32", "FP64",
+__all__ = ["Spectrum", "Batch", "Server", "row_state", "shard", "grid_size", "covariance", "setrot", "vario", "condition", "FP32", "FP64",
            "SpecsimError", "set_stream"]
 
 
@@ -86,6 +86,25 @@ def autotune(spectrum, igauss=1, precision=FP32, nreal=2):
     L.check(L.lib().ss3d_autotune(spectrum.handle, int(igauss), int(precision), int(nreal),
                                   ctypes.c_void_p(ch.ctypes.data)))
     return {"middle_pass": int(ch[0]), "synthesis_pass": int(ch[1]), "row_pass": int(ch[2])}
+
+
+def row_state(np3, igauss, iseed, r, j, k):
+    """Park-Miller state right after the first draw of row (j, k) of realization r
+    (0-based) on periodic grid np3, by host jump-ahead (no GPU)."""
+    st = ctypes.c_uint32()
+    L.check(L.lib().ss3d_row_state(L.iptr(_np3(np3, np.int32)), int(igauss), int(iseed), int(r), int(j), int(k),
+                                   ctypes.byref(st)))
+    return int(st.value)
+
+
+def shard(rank, world, nreal_per_rank):
+    """Realizations of one rank when realizations are split over processes or
+    GPUs: (r_first, nreal) = (rank * nreal_per_rank, nreal_per_rank).  Every
+    rank draws from the same seed's stream by jump-ahead, so the union of the
+    shards equals one run of world * nreal_per_rank realizations."""
+    if not 0 <= rank < world:
+        raise ValueError("rank out of range")
+    return rank * int(nreal_per_rank), int(nreal_per_rank)
 
 
 def _out_ptr(out):

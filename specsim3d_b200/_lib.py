@@ -21,7 +21,7 @@ OUT_F32, OUT_F64 = 0, 1
 EXPORTS = (
     "ss3d_setrot", "ss3d_covariance", "ss3d_grid_size",
     "ss3d_spectrum_create", "ss3d_spectrum_free", "ss3d_spectrum_info", "ss3d_spectrum_bytes", "ss3d_spectrum_amp",
-    "ss3d_realize", "ss3d_debug_states", "ss3d_debug_coefficients",
+    "ss3d_realize", "ss3d_debug_states", "ss3d_debug_coefficients", "ss3d_row_state",
     "ss3d_vario", "ss3d_condition",
     "ss3d_set_stream", "ss3d_last_error", "ss3d_version", "ss3d_profile", "ss3d_profile_read", "ss3d_autotune", "ss3d_set_variant",
     "ss3d_realize_workspace_bytes", "ss3d_release_workspace",
@@ -141,6 +141,7 @@ def lib():
         "ss3d_set_variant": (I, [I, I, I, I]),
         "ss3d_realize_workspace_bytes": (I64, [P, I, I, I]),
         "ss3d_release_workspace": (I, []),
+        "ss3d_row_state": (I, [P, I, I, I64, I, I, P]),
         "ss3d_batch_create": (I, [P, I, P]),
         "ss3d_batch_run": (I, [P]),
         "ss3d_batch_autotune": (I, [P]),

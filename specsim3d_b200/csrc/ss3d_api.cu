@@ -476,6 +476,13 @@ extern "C" int ss3d_spectrum_amp(const ss3d_spectrum* sp, double* amp) {
 
 // ---------------------------------------------------------------- realizations
 namespace {
+Geo geo_for_np(Geo g, int igauss) {
+  g.d = igauss ? 2 : 1;
+  uint64_t N = (uint64_t)g.npx * g.npy * g.npz;
+  uint64_t nself = (uint64_t)(g.npx >= 2 ? 2 : 1) * (g.npy >= 2 ? 2 : 1) * (g.npz >= 2 ? 2 : 1);
+  g.D = (uint64_t)g.d * ((N + nself) / 2);
+  return g;
+}
 Geo geo_for(const ss3d_spectrum* sp, int igauss) {
   Geo g = sp->geo;
   g.d = igauss ? 2 : 1;
@@ -654,6 +661,39 @@ extern "C" int ss3d_realize(const ss3d_spectrum* csp, int iseed, int64_t r_first
       zstats[3 * r + 2] = 0.0;
     }
   }
+  return SS3D_OK;
+}
+
+// ---------------------------------------------------------------- host jump-ahead
+// State of the Park-Miller stream right after the first draw of row (j, k) of
+// realization r: 16807^(11 + r D + d prefix(j, k)) s0 mod (2^31 - 1), the value
+// the realization kernels start that row from.  Host arithmetic only, so that
+// a host can plan and check a split of realizations over processes or GPUs.
+extern "C" int ss3d_row_state(const int np[3], int igauss, int iseed, int64_t r, int j, int k, uint32_t* state) {
+  if (!np || !state) return fail(SS3D_EINVAL, "NULL argument");
+  if (np[0] < 1 || np[1] < 1 || np[2] < 1) return fail(SS3D_EINVAL, "grid sizes must be positive");
+  if (j < 0 || j >= np[1] || k < 0 || k >= np[2] || r < 0) return fail(SS3D_EINVAL, "row or realization out of range");
+  Geo g{};
+  g.npx = np[0];
+  g.npy = np[1];
+  g.npz = np[2];
+  g.nx = g.npx;
+  g.ny = g.npy;
+  g.nz = g.npz;
+  g.H = g.npx >= 2 ? g.npx / 2 + 1 : 1;
+  g.HP = (g.H + 1) & ~1;
+  g = geo_for_np(g, igauss);
+  const uint64_t M1 = (uint64_t)(PM_M - 1);
+  uint64_t t = ((uint64_t)r % M1) * (g.D % M1) % M1;
+  t = (t + (uint64_t)g.d * row_prefix(g, j, k)) % M1;
+  uint64_t e = (11ull + t) % M1;
+  uint32_t base = PM_A, acc = 1;
+  while (e) {
+    if (e & 1) acc = pm_mulmod(acc, base);
+    base = pm_mulmod(base, base);
+    e >>= 1;
+  }
+  *state = pm_mulmod(acc, seed0(iseed));
   return SS3D_OK;
 }
 
