@@ -150,10 +150,12 @@ __device__ __forceinline__ void colgen_body(const AxisArgs& a, const Geo& g, con
   const int t = threadIdx.x % TX;
   const int line = line0 + t;
   const bool valid = line_valid(g, line, a.lines);
+  // lines past the grid or in the row padding compute with line 0's indices
+  // (in range) and contribute zeros: no branch in the loader
+  const int lsafe = valid ? line : 0;
   const bool zaxis = a.axis == 2;
-  int i = zaxis ? line % g.HP : line;
-  const int j0 = zaxis ? line / g.HP : 0;
-  if (!valid) i = 0;
+  const int i = zaxis ? lsafe % g.HP : lsafe;
+  const int j0 = zaxis ? lsafe / g.HP : 0;
   const uint32_t ai = __ldg(apow + i), aip = __ldg(apow + ((g.npx - i) & (g.npx - 1)));
   const bool iedge = (i == 0) || (2 * i == g.npx);
   // z pass: rows (j0, p) and (jp0, pp); y pass (2D): rows p and pp of plane 0
@@ -164,7 +166,7 @@ __device__ __forceinline__ void colgen_body(const AxisArgs& a, const Geo& g, con
   const uint32_t* rs = rowstates + (size_t)r * g.npy * g.npz;
   const uint32_t* rs_own = rs + (zaxis ? j0 : 0);
   const uint32_t* rs_par = rs + (zaxis ? jp0 : 0);
-  const long long cbase = (long long)grp * a.gstride + line;
+  const long long cbase = (long long)grp * a.gstride + lsafe;
   const R* ap = amp + cbase;
   C* dst = out + cbase + (long long)r * a.rstride;
   const int S = (int)a.S;   // offsets inside one realization's grid fit in 32 bits
@@ -174,7 +176,6 @@ __device__ __forceinline__ void colgen_body(const AxisArgs& a, const Geo& g, con
   fft_tile<LOGN, TX, TPC, +1>(
       s, stw,
       [&](int jb, int rr) {
-        if (!valid) return cmk<C>(R(0), R(0));
         const int p = jb + rr * NR0;
         const R am = __ldg(ap + p * S);
         bool greater, mid;
@@ -191,7 +192,8 @@ __device__ __forceinline__ void colgen_body(const AxisArgs& a, const Geo& g, con
         const int pp = (N - p) & (N - 1);
         const uint32_t st = __ldg(greater ? rs_par + pp * rowstride : rs_own + p * rowstride);
         const uint32_t s1 = pm_mulmod(st, greater ? aip : ai);
-        return coef_from_state<R, GAUSS>(s1, am, mid && selfcol, greater);
+        const C v = coef_from_state<R, GAUSS>(s1, am, mid && selfcol, greater);
+        return valid ? v : cmk<C>(R(0), R(0));
       },
       [&](int pos, C v) {
         if (valid && pos < nout) dst[pos * S] = v;
@@ -320,8 +322,10 @@ __device__ __forceinline__ void rows_body(const Geo& g, const cpx_t<R>* __restri
   }
   __syncthreads();
   fft_rows_inv<R, LOGN, TX, TPC>(s, stwN);
-  // write x[0..nx) of each row: one warp per row, lanes along m; sums for the stats
+  // write x[0..nx) of each row: one warp per row, lanes along m; FP64 sums for
+  // the stats only when they are asked for (part != NULL, a uniform branch)
   double s1 = 0.0, s2 = 0.0;
+  const bool stats = part != nullptr;
   O* dst = out + (long long)r * ostride;
   const int nxh = (g.nx + 1) / 2;
   const bool even = (g.nx & 1) == 0;
@@ -332,20 +336,21 @@ __device__ __forceinline__ void rows_body(const Geo& g, const cpx_t<R>* __restri
     for (int m = lane; m < nxh; m += 32) {
       const C z = s[m * PITCH + t];
       const O a0 = (O)z.x, a1 = (O)z.y;
-      s1 += (double)z.x;
-      s2 += (double)z.x * (double)z.x;
+      const bool second = even || 2 * m + 1 < g.nx;
       if (even) {
         if constexpr (sizeof(O) == 4) {
           reinterpret_cast<float2*>(rp)[m] = make_float2((float)a0, (float)a1);
         } else {
           reinterpret_cast<double2*>(rp)[m] = make_double2((double)a0, (double)a1);
         }
-        s1 += (double)z.y;
-        s2 += (double)z.y * (double)z.y;
       } else {
         rp[2 * m] = a0;
-        if (2 * m + 1 < g.nx) {
-          rp[2 * m + 1] = a1;
+        if (second) rp[2 * m + 1] = a1;
+      }
+      if (stats) {
+        s1 += (double)z.x;
+        s2 += (double)z.x * (double)z.x;
+        if (second) {
           s1 += (double)z.y;
           s2 += (double)z.y * (double)z.y;
         }

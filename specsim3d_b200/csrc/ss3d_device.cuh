@@ -133,24 +133,21 @@ __device__ __forceinline__ void phasor_d(uint32_t s, double& c, double& sn) {
   double u = (double)s / 2147483647.0;
   sincospi(2.0 * u, &sn, &c);
 }
-// -2 ln(s/m) in float for s in [1, m-1].  For u = s/m >= 1/2 the logarithm is
-// 2 atanh(z), z = (u-1)/(u+1) = -(m-s)/(m+s) with |z| <= 1/3, from the exact
-// integer difference m-s (odd series to z^13, truncation below 2e-8 relative);
-// below 1/2 |ln u| >= ln 2 and the hardware log2 (relative error ~2^-22) is
-// accurate enough.
+// -2 ln(s/m) in float for s in [1, m-1].  For u = s/m >= 3/4 the logarithm is
+// 2 atanh(z), z = (u-1)/(u+1) = -(m-s)/(m+s) with |z| <= 1/7, from the exact
+// integer difference m-s (odd series to z^7, truncation below 2e-8 relative);
+// below 3/4 |ln u| >= 0.28 and the hardware log2 (absolute error ~2^-22) is
+// accurate to a few 1e-7 relative.
 __device__ __forceinline__ float m2log_f(uint32_t s) {
   const float a = (float)(PM_M - s);
   const float z = -__fdividef(a, 4294967294.0f - a);        // (u-1)/(u+1), m + s = 2m - (m - s)
   const float z2 = z * z;
-  float p = fmaf(z2, 1.0f / 13.0f, 1.0f / 11.0f);
-  p = fmaf(z2, p, 1.0f / 9.0f);
-  p = fmaf(z2, p, 1.0f / 7.0f);
-  p = fmaf(z2, p, 1.0f / 5.0f);
+  float p = fmaf(z2, 1.0f / 7.0f, 1.0f / 5.0f);
   p = fmaf(z2, p, 1.0f / 3.0f);
   p = fmaf(z2, p, 1.0f);
   const float near1 = -4.0f * (p * z);
   const float far = -1.3862944f * __log2f((float)s * (1.0f / 2147483647.0f));   // -2 ln 2 * log2(u)
-  return s >= (1u << 30) ? near1 : far;
+  return s >= 1610612736u ? near1 : far;                    // u >= 3/4
 }
 __device__ __forceinline__ double m2log_d(uint32_t s) {
   double u = (double)s / 2147483647.0;
