@@ -272,7 +272,8 @@ typedef struct ss3d_server ss3d_server;
 typedef struct ss3d_server_config {
     int slots;                   /* requests on the GPU at once (1..64) */
     int max_bypass;              /* passes of a waiting queue head (0: 16) */
-    int max_cond;                /* conditional requests on the GPU at once (0: 1) */
+    int max_cond;                /* conditional requests on the GPU at once (0: 2); they run
+                                    on low-priority streams, the others on high-priority ones */
     int64_t hbm_budget;          /* device bytes for spectra and work (0: 80 % of free memory) */
     int64_t cache_budget;        /* bytes of idle spectra kept (0: half the budget) */
     int64_t retain_bytes;        /* largest work space a slot keeps between requests

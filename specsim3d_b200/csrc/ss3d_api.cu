@@ -9,6 +9,7 @@
 #include <cstdio>
 #include <cstdlib>
 #include <cstring>
+#include <map>
 #include <mutex>
 #include <string>
 #include <vector>
@@ -95,6 +96,21 @@ extern "C" const char* ss3d_version(void) { return "specsim3d_b200 0.1 (sm_100a)
 extern "C" int ss3d_set_stream(void* stream) {
   g_stream = (cudaStream_t)stream;
   return SS3D_OK;
+}
+
+// ---------------------------------------------------------------- kernel attributes
+cudaError_t ss3d::func_smem(const void* kernel, size_t bytes) {
+  static std::mutex mu;
+  static std::map<std::pair<int, const void*>, size_t> done;
+  int dev = 0;
+  cudaError_t e = cudaGetDevice(&dev);
+  if (e != cudaSuccess) return e;
+  std::lock_guard<std::mutex> lk(mu);
+  size_t& have = done[{dev, kernel}];
+  if (bytes <= have) return cudaSuccess;
+  e = cudaFuncSetAttribute(kernel, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)bytes);
+  if (e == cudaSuccess) have = bytes;
+  return e;
 }
 
 // ---------------------------------------------------------------- device context
@@ -404,8 +420,8 @@ extern "C" int ss3d_spectrum_create(const ss3d_struct* st, int nst, double nugge
   // temporaries come from the stream-ordered pool: no device-wide synchronisation
   // when they are freed, so that other threads' streams keep running
   cudaError_t e = cudaMallocAsync((void**)&work, sizeof(double2) * nh, s);
-  if (e == cudaSuccess) e = cudaMalloc(&sp->amp64, sizeof(double) * nh);
-  if (e == cudaSuccess) e = cudaMalloc(&sp->amp32, sizeof(float) * nh);
+  if (e == cudaSuccess) e = cudaMallocAsync((void**)&sp->amp64, sizeof(double) * nh, s);
+  if (e == cudaSuccess) e = cudaMallocAsync((void**)&sp->amp32, sizeof(float) * nh, s);
   if (e == cudaSuccess) e = cudaMallocAsync((void**)&part, sizeof(SpecPartial) * (npart + 1), s);
   if (e == cudaSuccess)
     e = launch_spectrum(sp->model, d, g, work, sp->amp64, sp->amp32, part, npart, part + npart, Tw{ctx->twf, ctx->twd},
@@ -432,13 +448,16 @@ extern "C" int ss3d_spectrum_create(const ss3d_struct* st, int nst, double nugge
   return SS3D_OK;
 }
 
+// The amplitudes come from the device's stream-ordered pool and go back to it
+// on the calling thread's stream (no device-wide synchronisation); the caller
+// has finished every use of the spectrum on other streams.
 extern "C" void ss3d_spectrum_free(ss3d_spectrum* sp) {
   if (!sp) return;
   int cur = 0;
   cudaGetDevice(&cur);
   cudaSetDevice(sp->dev);
-  if (sp->amp64) cudaFree(sp->amp64);
-  if (sp->amp32) cudaFree(sp->amp32);
+  if (sp->amp64) cudaFreeAsync(sp->amp64, g_stream);
+  if (sp->amp32) cudaFreeAsync(sp->amp32, g_stream);
   cudaSetDevice(cur);
   delete sp;
 }

@@ -253,7 +253,7 @@ cudaError_t plan(ss3d_batch* b) {
     b->grid[p] = 0;
     if (!start[p]) continue;
     BatchKernel k = kBatchKernels[p][b->etv[p]];
-    e = cudaFuncSetAttribute(k, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)sm[p]);
+    e = func_smem(reinterpret_cast<const void*>(k), sm[p]);
     int occ = 0;
     if (e == cudaSuccess) e = cudaOccupancyMaxActiveBlocksPerMultiprocessor(&occ, k, BNT, sm[p]);
     if (e == cudaSuccess && occ < 1) e = cudaErrorInvalidConfiguration;

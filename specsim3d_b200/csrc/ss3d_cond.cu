@@ -116,19 +116,63 @@ __global__ void k_cond_search(CondGeo G, long long node0, int count, const doubl
   nnb[q] = nn | (flag << 16);
 }
 
-// Cholesky factor of A + ridge I (lower, in place in L = A copy), solve L L^T w = b.
-// Warp-cooperative, right-looking.  Returns false on a non-positive pivot.
+// Lower-triangle pair table shared by a block: entry e (row-major over the
+// lower triangle with the diagonal) holds (r, c), c <= r, in two bytes, so that
+// the lanes of a warp can take the elements of a triangle in turn without a
+// division.  Entries of a triangle of side m are the first m (m + 1) / 2.
+__host__ __device__ inline size_t cond_tri_bytes(int ndmax) {
+  return ((size_t)ndmax * (ndmax + 1) / 2 * 2 + 15) & ~(size_t)15;
+}
+
+__device__ inline void fill_tri(uint8_t* tri, int ndmax) {
+  const int T = ndmax * (ndmax + 1) / 2;
+  for (int e = threadIdx.x; e < T; e += blockDim.x) {
+    int r = (int)((sqrtf(8.0f * (float)e + 1.0f) - 1.0f) * 0.5f);
+    while (r * (r + 1) / 2 > e) --r;
+    while ((r + 1) * (r + 2) / 2 <= e) ++r;
+    tri[2 * e] = (uint8_t)r;
+    tri[2 * e + 1] = (uint8_t)(e - r * (r + 1) / 2);
+  }
+}
+
+// Forward and back substitution with the factor L (lower, leading dimension
+// ld): L L^T w = b, warp-parallel by columns; tmp is n scratch values.
 template <typename T>
-__device__ bool warp_chol_solve(T* L, const T* A, int ld, int n, T ridge, T* w, const T* b, int lane) {
+__device__ void warp_tri_solve(const T* L, int ld, int n, T* w, const T* b, T* tmp, int lane) {
+  for (int p = lane; p < n; p += 32) tmp[p] = b[p];
+  __syncwarp();
+  for (int p = 0; p < n; ++p) {
+    const T wp = tmp[p] / L[p * ld + p];
+    for (int r = p + 1 + lane; r < n; r += 32) tmp[r] -= L[r * ld + p] * wp;
+    if (lane == 0) w[p] = wp;
+    __syncwarp();
+  }
+  for (int p = lane; p < n; p += 32) tmp[p] = w[p];
+  __syncwarp();
+  for (int p = n - 1; p >= 0; --p) {
+    const T wp = tmp[p] / L[p * ld + p];
+    for (int r = lane; r < p; r += 32) tmp[r] -= L[p * ld + r] * wp;
+    if (lane == 0) w[p] = wp;
+    __syncwarp();
+  }
+}
+
+// Cholesky factor of A + ridge I (lower, in place in L = A copy) and the solve
+// of L L^T w = b, warp-cooperative and right-looking: the trailing update of
+// each column goes over the lanes by the pair table (each element receives its
+// updates in column order, as in the serial algorithm).  Returns false on a
+// non-positive pivot (the reference's chol_solve failure, f90:1040-1079).
+template <typename T>
+__device__ bool warp_chol_solve(T* L, const T* A, int ld, int n, T ridge, T* w, const T* b, T* tmp,
+                                const uint8_t* __restrict__ tri, int lane) {
   for (int q = lane; q < n * ld; q += 32) L[q] = A[q];
   __syncwarp();
-  if (lane == 0)
-    for (int p = 0; p < n; ++p) L[p * ld + p] += ridge;
+  for (int p = lane; p < n; p += 32) L[p * ld + p] += ridge;
   __syncwarp();
   bool ok = true;
   for (int c = 0; c < n; ++c) {
     const T piv = L[c * ld + c];
-    if (!(piv > T(0))) {
+    if (!(piv > T(0))) {   // uniform: every lane reads the same value
       ok = false;
       break;
     }
@@ -137,48 +181,22 @@ __device__ bool warp_chol_solve(T* L, const T* A, int ld, int n, T ridge, T* w, 
     for (int r = c + 1 + lane; r < n; r += 32) L[r * ld + c] = L[r * ld + c] / dgl;
     if (lane == 0) L[c * ld + c] = dgl;
     __syncwarp();
-    for (int r = c + 1 + lane; r < n; r += 32) {
-      const T lrc = L[r * ld + c];
-      for (int cc = c + 1; cc <= r; ++cc) L[r * ld + cc] -= lrc * L[cc * ld + c];
+    const int m = n - c - 1, nt = m * (m + 1) / 2;
+    for (int e = lane; e < nt; e += 32) {
+      const int r = c + 1 + tri[2 * e], cc = c + 1 + tri[2 * e + 1];
+      L[r * ld + cc] -= L[r * ld + c] * L[cc * ld + c];
     }
     __syncwarp();
   }
-  ok = __shfl_sync(0xffffffffu, ok ? 1 : 0, 0) != 0;
   if (!ok) return false;
-  if (lane == 0) {
-    for (int p = 0; p < n; ++p) {
-      T s = b[p];
-      for (int m = 0; m < p; ++m) s -= L[p * ld + m] * w[m];
-      w[p] = s / L[p * ld + p];
-    }
-    for (int p = n - 1; p >= 0; --p) {
-      T s = w[p];
-      for (int m = p + 1; m < n; ++m) s -= L[m * ld + p] * w[m];
-      w[p] = s / L[p * ld + p];
-    }
-  }
-  __syncwarp();
+  warp_tri_solve<T>(L, ld, n, w, b, tmp, lane);
   return true;
-}
-
-// triangular solves with an existing factor (lane 0)
-template <typename T>
-__device__ void chol_resolve(const T* L, int ld, int n, T* w, const T* b) {
-  for (int p = 0; p < n; ++p) {
-    T s = b[p];
-    for (int m = 0; m < p; ++m) s -= L[p * ld + m] * w[m];
-    w[p] = s / L[p * ld + p];
-  }
-  for (int p = n - 1; p >= 0; --p) {
-    T s = w[p];
-    for (int m = p + 1; m < n; ++m) s -= L[m * ld + p] * w[m];
-    w[p] = s / L[p * ld + p];
-  }
 }
 
 // kriging of the residual at nodes [node0, node0+count): warp per node.
 // precision 0: FP64 factor and solve; 1: FP32 factor and solve plus one
 // refinement step with the residual b - A w formed in FP64.
+// Dynamic shared memory: the pair table, then one region per warp.
 template <int PREC>
 __global__ void k_cond_krige(CondGeo G, Model mdl, long long node0, int count, const int* __restrict__ nbr,
                              const int* __restrict__ nnb, const double* __restrict__ dxs,
@@ -186,13 +204,18 @@ __global__ void k_cond_krige(CondGeo G, Model mdl, long long node0, int count, c
                              const double* __restrict__ dg, const double* __restrict__ simd, double* __restrict__ res,
                              unsigned long long* __restrict__ counters) {
   extern __shared__ __align__(16) unsigned char smc[];
+  __shared__ unsigned long long bcount[4];
   const int lane = threadIdx.x & 31, wib = threadIdx.x >> 5;
   const int nwb = blockDim.x >> 5;
   const int ndmax = G.ndmax;
   const int ld = ndmax;
-  // per warp: A (double), L (double or float), b, w (double), bf, wf (float), id (int)
+  uint8_t* tri = smc;
+  fill_tri(tri, ndmax);
+  if (threadIdx.x < 4) bcount[threadIdx.x] = 0;
+  __syncthreads();
+  // per warp: A (double), L (double or float), b, w, r, tmp (double), id (int)
   const size_t per = cond_warp_bytes(ndmax);
-  unsigned char* mine = smc + per * wib;
+  unsigned char* mine = smc + cond_tri_bytes(ndmax) + per * wib;
   double* A = (double*)mine;
   double* Ld = A + ndmax * ndmax;
   double* b = Ld + ndmax * ndmax;
@@ -203,35 +226,35 @@ __global__ void k_cond_krige(CondGeo G, Model mdl, long long node0, int count, c
   float* Lf = (float*)Ld;
   float* bf = (float*)r;
   float* wf = (float*)tmp;
+  float* tf = Lf + ndmax * ndmax;   // FP32 scratch of the solves: the second half of Ld's region
   const long long M = (long long)G.nx * G.ny * G.nz;
   for (int q = blockIdx.x * nwb + wib; q < count; q += gridDim.x * nwb) {
     const long long node = node0 + q;
     const int code = nnb[q];
     const int nn = code & 0xffff, exact = code >> 16;
-    if (lane == 0) atomicAdd(&counters[0], (unsigned long long)nn);
+    if (lane == 0) atomicAdd_block(&bcount[0], (unsigned long long)nn);
     if (nn == 0) {
-      if (lane == 0) atomicAdd(&counters[2], 1ull);
+      if (lane == 0) atomicAdd_block(&bcount[2], 1ull);
       continue;
     }
     const int* nl = nbr + (long long)q * ndmax;
     if (exact) {
       const double v = dg[nl[0]];
       for (int l = lane; l < G.nreal; l += 32) res[node + M * l] = v;
-      if (lane == 0) atomicAdd(&counters[3], 1ull);
+      if (lane == 0) atomicAdd_block(&bcount[3], 1ull);
       continue;
     }
     const int i = (int)(node % G.nx), j = (int)((node / G.nx) % G.ny), k = (int)(node / ((long long)G.nx * G.ny));
     const double x = G.xmin + (double)i * G.dx, y = G.ymin + (double)j * G.dy, z = G.zmin + (double)k * G.dz;
     for (int p = lane; p < nn; p += 32) id[p] = nl[p];
     __syncwarp();
-    for (int e = lane; e < nn * nn; e += 32) {
-      const int p = e / nn, qq = e % nn;
-      if (qq <= p) {
-        const int cp = id[p], cq = id[qq];
-        const double v = covariance(mdl, dxs[cp] - dxs[cq], dys[cp] - dys[cq], dzs[cp] - dzs[cq]);
-        A[p * ld + qq] = v;
-        A[qq * ld + p] = v;
-      }
+    const int ntri = nn * (nn + 1) / 2;
+    for (int e = lane; e < ntri; e += 32) {
+      const int p = tri[2 * e], qq = tri[2 * e + 1];
+      const int cp = id[p], cq = id[qq];
+      const double v = covariance(mdl, dxs[cp] - dxs[cq], dys[cp] - dys[cq], dzs[cp] - dzs[cq]);
+      A[p * ld + qq] = v;
+      A[qq * ld + p] = v;
     }
     for (int p = lane; p < nn; p += 32) {
       const int cp = id[p];
@@ -243,31 +266,29 @@ __global__ void k_cond_krige(CondGeo G, Model mdl, long long node0, int count, c
     int tries = 0;
     for (tries = 1; tries <= 3; ++tries) {
       if (PREC == 0) {
-        ok = warp_chol_solve<double>(Ld, A, ld, nn, ridge, w, b, lane);
+        ok = warp_chol_solve<double>(Ld, A, ld, nn, ridge, w, b, tmp, tri, lane);
       } else {
         // FP32 copies of A and b; the factor is built in place in Lf
         for (int p = lane; p < nn; p += 32) bf[p] = (float)b[p];
         for (int e = lane; e < nn * ld; e += 32) Lf[e] = (float)A[e];
         __syncwarp();
-        ok = warp_chol_solve<float>(Lf, Lf, ld, nn, (float)ridge, wf, bf, lane);
+        ok = warp_chol_solve<float>(Lf, Lf, ld, nn, (float)ridge, wf, bf, tf, tri, lane);
         if (ok) {
-          // one refinement: r = b - (A + ridge I) w in FP64, solve L L^T d = r in FP32, w += d
-          if (lane == 0) {
-            for (int p = 0; p < nn; ++p) w[p] = (double)wf[p];
-          }
+          // one refinement: res = b - (A + ridge I) w in FP64, solve L L^T d = res in FP32, w += d.
+          // The FP64 residual goes to tmp (wf's region, free once w holds the
+          // solution), its FP32 copy to bf (r's region); the correction to wf.
+          for (int p = lane; p < nn; p += 32) w[p] = (double)wf[p];
           __syncwarp();
           for (int p = lane; p < nn; p += 32) {
-            double s = b[p] - ridge * w[p];
-            for (int m = 0; m < nn; ++m) s -= A[p * ld + m] * w[m];
-            r[p] = s;
+            double sres = b[p] - ridge * w[p];
+            for (int m = 0; m < nn; ++m) sres -= A[p * ld + m] * w[m];
+            tmp[p] = sres;
           }
           __syncwarp();
-          if (lane == 0) {
-            float dtmp[100], rtmp[100];
-            for (int p = 0; p < nn; ++p) rtmp[p] = (float)r[p];
-            chol_resolve<float>(Lf, ld, nn, dtmp, rtmp);
-            for (int p = 0; p < nn; ++p) w[p] += (double)dtmp[p];
-          }
+          for (int p = lane; p < nn; p += 32) bf[p] = (float)tmp[p];
+          __syncwarp();
+          warp_tri_solve<float>(Lf, ld, nn, wf, bf, tf, lane);
+          for (int p = lane; p < nn; p += 32) w[p] += (double)wf[p];
           __syncwarp();
         }
       }
@@ -275,10 +296,10 @@ __global__ void k_cond_krige(CondGeo G, Model mdl, long long node0, int count, c
       ridge = ridge * 1.0e3;
     }
     if (!ok) {
-      if (lane == 0) atomicAdd(&counters[1], 1ull);
+      if (lane == 0) atomicAdd_block(&bcount[1], 1ull);
       continue;
     }
-    if (tries > 1 && lane == 0) atomicAdd(&counters[1], 1ull);
+    if (tries > 1 && lane == 0) atomicAdd_block(&bcount[1], 1ull);
     double zk = 0.0;
     for (int p = 0; p < nn; ++p) zk += w[p] * dg[id[p]];
     for (int l = lane; l < G.nreal; l += 32) {
@@ -288,6 +309,8 @@ __global__ void k_cond_krige(CondGeo G, Model mdl, long long node0, int count, c
     }
     __syncwarp();
   }
+  __syncthreads();
+  if (threadIdx.x < 4 && bcount[threadIdx.x]) atomicAdd(&counters[threadIdx.x], bcount[threadIdx.x]);
 }
 
 __global__ void k_gather_simd(const double* __restrict__ res, long long M, const int* __restrict__ ix,
@@ -655,9 +678,9 @@ extern "C" int ss3d_condition(double* res, const int n[3], int nreal, const doub
   const int wpb = (int)std::max<size_t>(1, std::min<size_t>(8, (size_t)(96 * 1024) / per));
   if (e == cudaSuccess) {
     if (precision == SS3D_FP64)
-      e = cudaFuncSetAttribute(k_cond_krige<0>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)(per * wpb));
+      e = func_smem(reinterpret_cast<const void*>(k_cond_krige<0>), cond_tri_bytes(cp->ndmax) + per * wpb);
     else
-      e = cudaFuncSetAttribute(k_cond_krige<1>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)(per * wpb));
+      e = func_smem(reinterpret_cast<const void*>(k_cond_krige<1>), cond_tri_bytes(cp->ndmax) + per * wpb);
   }
   for (long long node0 = 0; node0 < M && e == cudaSuccess; node0 += chunk) {
     const int count = (int)std::min<long long>(chunk, M - node0);
@@ -666,12 +689,14 @@ extern "C" int ss3d_condition(double* res, const int n[3], int nreal, const doub
     ++g_launch_count;
     e = cudaGetLastError();
     if (e != cudaSuccess) break;
-    const int nblk = (int)std::min<long long>(148 * 16, ((long long)count + wpb - 1) / wpb);
+    // one block per wpb nodes (short blocks): work of other streams, e.g. of a
+    // serving loop's higher-priority requests, gets SMs as blocks finish
+    const int nblk = (int)(((long long)count + wpb - 1) / wpb);
     if (precision == SS3D_FP64)
-      k_cond_krige<0><<<nblk, 32 * wpb, per * wpb, stm>>>(G, mdl, node0, count, dnbr, dnnb, ddx, ddy, ddz, ddg,
+      k_cond_krige<0><<<nblk, 32 * wpb, cond_tri_bytes(cp->ndmax) + per * wpb, stm>>>(G, mdl, node0, count, dnbr, dnnb, ddx, ddy, ddz, ddg,
                                                           dsimd, dres, dcnt);
     else
-      k_cond_krige<1><<<nblk, 32 * wpb, per * wpb, stm>>>(G, mdl, node0, count, dnbr, dnnb, ddx, ddy, ddz, ddg,
+      k_cond_krige<1><<<nblk, 32 * wpb, cond_tri_bytes(cp->ndmax) + per * wpb, stm>>>(G, mdl, node0, count, dnbr, dnnb, ddx, ddy, ddz, ddg,
                                                           dsimd, dres, dcnt);
     ++g_launch_count;
     e = cudaGetLastError();

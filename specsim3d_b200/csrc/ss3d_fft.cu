@@ -344,7 +344,7 @@ static int ilog2(int n) {
 template <typename K>
 static cudaError_t set_smem(K kernel, size_t bytes) {
   if (bytes <= 48 * 1024) return cudaSuccess;
-  return cudaFuncSetAttribute(kernel, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)bytes);
+  return func_smem(reinterpret_cast<const void*>(kernel), bytes);
 }
 
 #define SS3D_LOGN_SWITCH(LOGN_VAR, MAXL, CALL)                  \

@@ -69,6 +69,10 @@ struct Marks {
   cudaEvent_t ev[16];
 };
 void mark(Marks* m, int stage, cudaStream_t st);   // records an event opening `stage`
+// Raises a kernel's dynamic shared memory limit on the current device once per
+// size: changing a function attribute while instances of it run on other
+// streams can make the call wait for them, so repeated calls return at once.
+cudaError_t func_smem(const void* kernel, size_t bytes);
 extern std::atomic<unsigned long long> g_launch_count;   // kernels launched by the library (all threads)
 
 // ---- launchers (ss3d_fft.cu); all return cudaError_t of the last launch

@@ -280,18 +280,24 @@ int run_request(ss3d_server* s, Req* r, std::string& msg) {
 }
 
 void worker_main(ss3d_server* s, int w) {
-  cudaStream_t st = nullptr;
+  // two streams per slot: unconditional requests at the highest priority,
+  // conditional ones (long search and kriging kernels) at the lowest, so that
+  // the block scheduler serves short requests between their blocks
+  cudaStream_t st_hi = nullptr, st_lo = nullptr;
   if (!s->dry) {
     cudaSetDevice(s->dev);
-    cudaStreamCreateWithFlags(&st, cudaStreamNonBlocking);
-    ss3d_set_stream(st);
+    int lo = 0, hi = 0;
+    cudaDeviceGetStreamPriorityRange(&lo, &hi);
+    cudaStreamCreateWithPriority(&st_hi, cudaStreamNonBlocking, hi);
+    cudaStreamCreateWithPriority(&st_lo, cudaStreamNonBlocking, lo);
+    ss3d_set_stream(st_hi);
   }
   std::vector<ss3d_spectrum*> freed;
   std::unique_lock<std::mutex> lk(s->mu);
   auto give_back_workspace = [&] {   // with the lock held; drops and retakes it
     const int64_t b = s->retained[w];
     lk.unlock();
-    if (!s->dry) ss3d_release_workspace();
+    if (!s->dry) ss3d_release_workspace();   // on the slot's last stream, synchronised
     lk.lock();
     s->charged -= b;
     s->retained[w] = 0;
@@ -312,6 +318,7 @@ void worker_main(ss3d_server* s, int w) {
     }
     lk.unlock();
     std::string msg;
+    if (!s->dry) ss3d_set_stream(r->cond ? st_lo : st_hi);
     const int rc = run_request(s, r, msg);
     lk.lock();
     s->charged -= r->held;
@@ -338,8 +345,11 @@ void worker_main(ss3d_server* s, int w) {
   lk.unlock();
   release_spectra(freed);
   if (!s->dry) {
+    ss3d_set_stream(st_hi);
     ss3d_release_workspace();
-    cudaStreamDestroy(st);
+    ss3d_set_stream(nullptr);
+    cudaStreamDestroy(st_hi);
+    cudaStreamDestroy(st_lo);
   }
 }
 
@@ -368,7 +378,7 @@ extern "C" int ss3d_server_create(const ss3d_server_config* cfg, ss3d_server** o
     s->cfg.retain_bytes = std::min<int64_t>((int64_t)4 << 30, s->cfg.hbm_budget / (2 * s->cfg.slots));
   if (s->cfg.cache_budget <= 0) s->cfg.cache_budget = s->cfg.hbm_budget / 2;
   if (s->cfg.max_bypass <= 0) s->cfg.max_bypass = 16;
-  if (s->cfg.max_cond <= 0) s->cfg.max_cond = 1;
+  if (s->cfg.max_cond <= 0) s->cfg.max_cond = 2;
   s->retained.assign(s->cfg.slots, 0);
   for (int w = 0; w < s->cfg.slots; w++) s->workers.emplace_back(worker_main, s, w);
   *out = s;

@@ -338,7 +338,7 @@ extern "C" int ss3d_vario(const double* res, const int n[3], int nreal, int ndir
     for (int l0 = 1; l0 <= nlag[d] && e == cudaSuccess; l0 += chunk) {
       const int nl = std::min(chunk, nlag[d] - l0 + 1);
       const size_t smem = sizeof(double) * VP * (size_t)(VT + VT + (nl - 1) * G.mu);
-      e = cudaFuncSetAttribute(k_vario, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
+      e = func_smem(reinterpret_cast<const void*>(k_vario), smem);
       if (e != cudaSuccess) break;
       std::vector<long long> npc(VLCH, 0);
       for (int li = 0; li < nl; li++) npc[li] = np_all[(l0 + li - 1) + (size_t)nlagmax * d];
