@@ -30,10 +30,14 @@
 
 namespace ss3d {
 
-// shared memory of one kriging warp: A and L (ndmax^2 doubles each), four
-// ndmax vectors of doubles and the neighbour ids, rounded up to 16 bytes
-__host__ __device__ inline size_t cond_warp_bytes(int ndmax) {
-  const size_t b = (size_t)ndmax * ndmax * 16 + (size_t)ndmax * 32 + (size_t)ndmax * 4;
+// shared memory of one kriging warp.  FP64 solves (prec 0): the covariance
+// matrix, factored in place (ndmax^2 doubles), four ndmax vectors of doubles
+// and the neighbour ids.  FP32 solves (prec 1): the FP64 matrix (kept for the
+// refinement residual), its FP32 factor (ndmax^2 floats), three ndmax vectors
+// of doubles, four of floats and the ids.  Rounded up to 16 bytes.
+__host__ __device__ inline size_t cond_warp_bytes(int ndmax, int prec) {
+  const size_t n = (size_t)ndmax;
+  const size_t b = prec == 0 ? n * n * 8 + n * 32 + n * 4 : n * n * 12 + n * 24 + n * 16 + n * 4;
   return (b + 15) & ~(size_t)15;
 }
 
@@ -136,13 +140,14 @@ __device__ inline void fill_tri(uint8_t* tri, int ndmax) {
 }
 
 // Forward and back substitution with the factor L (lower, leading dimension
-// ld): L L^T w = b, warp-parallel by columns; tmp is n scratch values.
+// ld) whose diagonal reciprocals are rinv: L L^T w = b, warp-parallel by
+// columns; tmp is n scratch values.
 template <typename T>
-__device__ void warp_tri_solve(const T* L, int ld, int n, T* w, const T* b, T* tmp, int lane) {
+__device__ void warp_tri_solve(const T* L, const T* rinv, int ld, int n, T* w, const T* b, T* tmp, int lane) {
   for (int p = lane; p < n; p += 32) tmp[p] = b[p];
   __syncwarp();
   for (int p = 0; p < n; ++p) {
-    const T wp = tmp[p] / L[p * ld + p];
+    const T wp = tmp[p] * rinv[p];
     for (int r = p + 1 + lane; r < n; r += 32) tmp[r] -= L[r * ld + p] * wp;
     if (lane == 0) w[p] = wp;
     __syncwarp();
@@ -150,36 +155,34 @@ __device__ void warp_tri_solve(const T* L, int ld, int n, T* w, const T* b, T* t
   for (int p = lane; p < n; p += 32) tmp[p] = w[p];
   __syncwarp();
   for (int p = n - 1; p >= 0; --p) {
-    const T wp = tmp[p] / L[p * ld + p];
+    const T wp = tmp[p] * rinv[p];
     for (int r = lane; r < p; r += 32) tmp[r] -= L[p * ld + r] * wp;
     if (lane == 0) w[p] = wp;
     __syncwarp();
   }
 }
 
-// Cholesky factor of A + ridge I (lower, in place in L = A copy) and the solve
-// of L L^T w = b, warp-cooperative and right-looking: the trailing update of
-// each column goes over the lanes by the pair table (each element receives its
-// updates in column order, as in the serial algorithm).  Returns false on a
-// non-positive pivot (the reference's chol_solve failure, f90:1040-1079).
+// Cholesky factor of L + ridge I in place (lower triangle; L holds the matrix
+// on entry), warp-cooperative and right-looking: the trailing update of each
+// column goes over the lanes by the pair table (each element receives its
+// updates in column order, as in the serial algorithm); the column is scaled
+// by the reciprocal of its pivot, kept in rinv for the solves.  Returns false
+// on a non-positive pivot (the reference's chol_solve failure, f90:1040-1079).
 template <typename T>
-__device__ bool warp_chol_solve(T* L, const T* A, int ld, int n, T ridge, T* w, const T* b, T* tmp,
-                                const uint8_t* __restrict__ tri, int lane) {
-  for (int q = lane; q < n * ld; q += 32) L[q] = A[q];
-  __syncwarp();
+__device__ bool warp_cholesky(T* L, T* rinv, int ld, int n, T ridge, const uint8_t* __restrict__ tri, int lane) {
   for (int p = lane; p < n; p += 32) L[p * ld + p] += ridge;
   __syncwarp();
-  bool ok = true;
   for (int c = 0; c < n; ++c) {
     const T piv = L[c * ld + c];
-    if (!(piv > T(0))) {   // uniform: every lane reads the same value
-      ok = false;
-      break;
-    }
+    if (!(piv > T(0))) return false;   // uniform: every lane reads the same value
     const T dgl = sqrt(piv);
+    const T inv = T(1) / dgl;
     __syncwarp();
-    for (int r = c + 1 + lane; r < n; r += 32) L[r * ld + c] = L[r * ld + c] / dgl;
-    if (lane == 0) L[c * ld + c] = dgl;
+    for (int r = c + 1 + lane; r < n; r += 32) L[r * ld + c] *= inv;
+    if (lane == 0) {
+      L[c * ld + c] = dgl;
+      rinv[c] = inv;
+    }
     __syncwarp();
     const int m = n - c - 1, nt = m * (m + 1) / 2;
     for (int e = lane; e < nt; e += 32) {
@@ -188,8 +191,6 @@ __device__ bool warp_chol_solve(T* L, const T* A, int ld, int n, T ridge, T* w, 
     }
     __syncwarp();
   }
-  if (!ok) return false;
-  warp_tri_solve<T>(L, ld, n, w, b, tmp, lane);
   return true;
 }
 
@@ -213,20 +214,20 @@ __global__ void k_cond_krige(CondGeo G, Model mdl, long long node0, int count, c
   fill_tri(tri, ndmax);
   if (threadIdx.x < 4) bcount[threadIdx.x] = 0;
   __syncthreads();
-  // per warp: A (double), L (double or float), b, w, r, tmp (double), id (int)
-  const size_t per = cond_warp_bytes(ndmax);
+  const size_t per = cond_warp_bytes(ndmax, PREC);
   unsigned char* mine = smc + cond_tri_bytes(ndmax) + per * wib;
-  double* A = (double*)mine;
-  double* Ld = A + ndmax * ndmax;
-  double* b = Ld + ndmax * ndmax;
+  const int n2 = ndmax * ndmax;
+  double* A = (double*)mine;     // covariance matrix (PREC 0: factored in place)
+  double* b = A + n2;
   double* w = b + ndmax;
-  double* r = w + ndmax;
-  double* tmp = r + ndmax;
-  int* id = (int*)(tmp + ndmax);
-  float* Lf = (float*)Ld;
-  float* bf = (float*)r;
-  float* wf = (float*)tmp;
-  float* tf = Lf + ndmax * ndmax;   // FP32 scratch of the solves: the second half of Ld's region
+  double* tmp = w + ndmax;
+  double* rinv = tmp + ndmax;    // PREC 0 only
+  float* Lf = (float*)(tmp + ndmax);   // PREC 1: FP32 factor, then bf, wf, tf, rinvf
+  float* bf = Lf + n2;
+  float* wf = bf + ndmax;
+  float* tf = wf + ndmax;
+  float* rinvf = tf + ndmax;
+  int* id = PREC == 0 ? (int*)(rinv + ndmax) : (int*)(rinvf + ndmax);
   const long long M = (long long)G.nx * G.ny * G.nz;
   for (int q = blockIdx.x * nwb + wib; q < count; q += gridDim.x * nwb) {
     const long long node = node0 + q;
@@ -249,13 +250,16 @@ __global__ void k_cond_krige(CondGeo G, Model mdl, long long node0, int count, c
     for (int p = lane; p < nn; p += 32) id[p] = nl[p];
     __syncwarp();
     const int ntri = nn * (nn + 1) / 2;
-    for (int e = lane; e < ntri; e += 32) {
-      const int p = tri[2 * e], qq = tri[2 * e + 1];
-      const int cp = id[p], cq = id[qq];
-      const double v = covariance(mdl, dxs[cp] - dxs[cq], dys[cp] - dys[cq], dzs[cp] - dzs[cq]);
-      A[p * ld + qq] = v;
-      A[qq * ld + p] = v;
-    }
+    auto fill_matrix = [&]() {
+      for (int e = lane; e < ntri; e += 32) {
+        const int p = tri[2 * e], qq = tri[2 * e + 1];
+        const int cp = id[p], cq = id[qq];
+        const double v = covariance(mdl, dxs[cp] - dxs[cq], dys[cp] - dys[cq], dzs[cp] - dzs[cq]);
+        A[p * ld + qq] = v;
+        A[qq * ld + p] = v;
+      }
+    };
+    fill_matrix();
     for (int p = lane; p < nn; p += 32) {
       const int cp = id[p];
       b[p] = covariance(mdl, dxs[cp] - x, dys[cp] - y, dzs[cp] - z);
@@ -266,17 +270,22 @@ __global__ void k_cond_krige(CondGeo G, Model mdl, long long node0, int count, c
     int tries = 0;
     for (tries = 1; tries <= 3; ++tries) {
       if (PREC == 0) {
-        ok = warp_chol_solve<double>(Ld, A, ld, nn, ridge, w, b, tmp, tri, lane);
+        if (tries > 1) {   // the failed factorization overwrote the matrix
+          fill_matrix();
+          __syncwarp();
+        }
+        ok = warp_cholesky<double>(A, rinv, ld, nn, ridge, tri, lane);
+        if (ok) warp_tri_solve<double>(A, rinv, ld, nn, w, b, tmp, lane);
       } else {
         // FP32 copies of A and b; the factor is built in place in Lf
         for (int p = lane; p < nn; p += 32) bf[p] = (float)b[p];
         for (int e = lane; e < nn * ld; e += 32) Lf[e] = (float)A[e];
         __syncwarp();
-        ok = warp_chol_solve<float>(Lf, Lf, ld, nn, (float)ridge, wf, bf, tf, tri, lane);
+        ok = warp_cholesky<float>(Lf, rinvf, ld, nn, (float)ridge, tri, lane);
         if (ok) {
-          // one refinement: res = b - (A + ridge I) w in FP64, solve L L^T d = res in FP32, w += d.
-          // The FP64 residual goes to tmp (wf's region, free once w holds the
-          // solution), its FP32 copy to bf (r's region); the correction to wf.
+          warp_tri_solve<float>(Lf, rinvf, ld, nn, wf, bf, tf, lane);
+          // one refinement: res = b - (A + ridge I) w in FP64 (to tmp), solve
+          // L L^T d = res in FP32, w += d
           for (int p = lane; p < nn; p += 32) w[p] = (double)wf[p];
           __syncwarp();
           for (int p = lane; p < nn; p += 32) {
@@ -287,7 +296,7 @@ __global__ void k_cond_krige(CondGeo G, Model mdl, long long node0, int count, c
           __syncwarp();
           for (int p = lane; p < nn; p += 32) bf[p] = (float)tmp[p];
           __syncwarp();
-          warp_tri_solve<float>(Lf, ld, nn, wf, bf, tf, lane);
+          warp_tri_solve<float>(Lf, rinvf, ld, nn, wf, bf, tf, lane);
           for (int p = lane; p < nn; p += 32) w[p] += (double)wf[p];
           __syncwarp();
         }
@@ -674,7 +683,7 @@ extern "C" int ss3d_condition(double* res, const int n[3], int nreal, const doub
     e = cudaGetLastError();
   }
   // kriging CTAs: warps per block limited by the shared memory of one warp
-  const size_t per = cond_warp_bytes(cp->ndmax);
+  const size_t per = cond_warp_bytes(cp->ndmax, precision == SS3D_FP64 ? 0 : 1);
   const int wpb = (int)std::max<size_t>(1, std::min<size_t>(8, (size_t)(96 * 1024) / per));
   if (e == cudaSuccess) {
     if (precision == SS3D_FP64)
