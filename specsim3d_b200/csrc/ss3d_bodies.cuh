@@ -162,10 +162,10 @@ __device__ __forceinline__ void colgen_body(const AxisArgs& a, const Geo& g, con
   const int jp0 = (-j0) & (g.npy - 1);
   const bool cgt = zaxis && j0 > jp0;                      // mid positions: partner's draw
   const bool selfcol = (!zaxis || j0 == jp0) && iedge;     // mid positions: self-conjugate
-  const int rowstride = zaxis ? g.npy : 1;
+  const int rowstride = zaxis ? 1 : g.npz;   // row states [j][k]: k runs fastest
   const uint32_t* rs = rowstates + (size_t)r * g.npy * g.npz;
-  const uint32_t* rs_own = rs + (zaxis ? j0 : 0);
-  const uint32_t* rs_par = rs + (zaxis ? jp0 : 0);
+  const uint32_t* rs_own = rs + (zaxis ? (size_t)j0 * g.npz : 0);
+  const uint32_t* rs_par = rs + (zaxis ? (size_t)jp0 * g.npz : 0);
   const long long cbase = (long long)grp * a.gstride + lsafe;
   const R* ap = amp + cbase;
   C* dst = out + cbase + (long long)r * a.rstride;

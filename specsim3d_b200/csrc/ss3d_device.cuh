@@ -116,7 +116,12 @@ __host__ __device__ __forceinline__ int row_class(const Geo& g, int j, int k) {
 // Unit phasor e^{2 pi i s/m} in float.  The nearest quarter turn n is taken
 // in integers (exact); the remainder |x| <= pi/4 (argument error below 5e-8:
 // one float rounding of the exact integer remainder) goes through the hardware
-// sine and cosine (__sincosf, absolute error about 5e-7 on this range).
+// sine and cosine (__sincosf, absolute error about 4e-7), and the quarter turns
+// are applied by exchanging and negating the two.  Reducing to the quarter
+// also keeps the small systematic error of the hardware functions from adding
+// up coherently: the four quadrants use it with opposite signs, whereas a
+// reduction to [-pi, pi] alone left a bias that summed to 4e-5 sqrt(C0) at the
+// cell where every phase is 1 (the origin) on a 512^3 spectrum.
 __device__ __forceinline__ void phasor_f(uint32_t s, float& c, float& sn) {
   const int n = __float2int_rn((float)s * (4.0f / 2147483647.0f));   // nearest quarter (off by one at most)
   const int rem = (int)(4u * s - (uint32_t)n * PM_M);                // exact 4s - n m, |.| <= m/2 + 2^11
@@ -170,7 +175,7 @@ __device__ __forceinline__ uint32_t first_state(const Geo& g, int i, int j, int 
     conj = true;
   }
   self = (cls == 1) && (i == 0 || 2 * i == g.npx);
-  return pm_mulmod(rs[sj + (size_t)g.npy * sk], apow[si]);
+  return pm_mulmod(rs[(size_t)sj * g.npz + sk], apow[si]);   // row states [j][k]
 }
 
 // Coefficient of half-spectrum index (i, j, k) for the realization whose row
@@ -229,7 +234,7 @@ __device__ __forceinline__ cpx_t<R> coef_col(const Geo& g, int j, int k, R amp, 
   const int jp = (-j) & (g.npy - 1), kp = (-k) & (g.npz - 1);
   const bool less = k < kp || (k == kp && j < jp);
   const bool greater = k > kp || (k == kp && j > jp);
-  const int row = greater ? jp + g.npy * kp : j + g.npy * k;
+  const int row = greater ? jp * g.npz + kp : j * g.npz + k;   // row states [j][k]
   const uint32_t s1 = pm_mulmod(__ldg(rs + row), greater ? aip : ai);
   const bool self = !less && !greater && iedge;
   if (g.d == 2) {

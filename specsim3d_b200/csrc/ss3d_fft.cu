@@ -99,7 +99,9 @@ __global__ void k_gen(Geo g, const R* __restrict__ amp, const uint32_t* __restri
 }
 
 // State of the first draw of every row of every realization of the batch:
-// s = 16807^(11 + (r_first + r) * D + d * prefix(row)) * s0  (mod 2^31-1)
+// s = 16807^(11 + (r_first + r) * D + d * prefix(row)) * s0  (mod 2^31-1).
+// Layout [r][j][k] (k fastest): the first inverse pass runs along k, so the
+// rows a warp needs are contiguous.
 __global__ void k_rowstates(Geo g, uint32_t s0, long long r_first, int nreal, const uint32_t* __restrict__ ptab,
                             uint32_t* rowstates) {
   const int rows = g.npy * g.npz;
@@ -108,7 +110,7 @@ __global__ void k_rowstates(Geo g, uint32_t s0, long long r_first, int nreal, co
        q += (long long)gridDim.x * blockDim.x) {
     int r = (int)(q / rows);
     int row = (int)(q - (long long)r * rows);
-    int j = row % g.npy, k = row / g.npy;
+    int j = row / g.npz, k = row % g.npz;
     const uint64_t M1 = (uint64_t)(PM_M - 1);
     uint64_t t = ((uint64_t)(r_first + r) % M1) * (g.D % M1) % M1;
     t = (t + (uint64_t)g.d * row_prefix(g, j, k)) % M1;

@@ -177,3 +177,21 @@ def test_coefficients_fp32(gpu, case, igauss):
     co = recipes.half_of_full(ora.coefficients(amp_o, sp.np, 8080 + case, 1, igauss), sp.np[0])
     cg = sp.debug_coefficients(8080 + case, 1, igauss, gpu.FP32)
     assert np.max(np.abs(cg - co)) <= 2e-6 * np.max(np.abs(co))
+
+
+def test_fp32_error_at_full_size(gpu):
+    """Precision form at the bench's full size (256^3 on 512^3, gaussian model):
+    every cell within 1e-5 sqrt(C0) of the FP64 path.  The origin cell sums every
+    coefficient with phase 1, so a systematic bias of the FP32 phasor shows up
+    there even when it is invisible on small grids."""
+    import torch
+    n = (256, 256, 256)
+    sp = gpu.Spectrum([(3, 1.0, 60.0, 30.0, 15.0, 30.0, 20.0, 10.0)], 0.1, (1.0, 1.0, 1.0), n, 1)
+    o32 = torch.empty((2, 256, 256, 256), dtype=torch.float32, device="cuda")
+    o64 = torch.empty((2, 256, 256, 256), dtype=torch.float64, device="cuda")
+    for igauss in (1, 0):
+        sp.realize(12345, 2, igauss, gpu.FP32, out=o32)
+        sp.realize(12345, 2, igauss, gpu.FP64, out=o64)
+        torch.cuda.synchronize()
+        err = float((o32.double() - o64).abs().amax().item()) / np.sqrt(sp.stats["c0"])
+        assert err <= 1e-5, (igauss, err)
