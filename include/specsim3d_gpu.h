@@ -259,9 +259,9 @@ int ss3d_condition(double *res, const int n[3], int nreal, const double xmin[3],
  * stream and work space, admit queued requests in arrival order as soon as a
  * slot is free and the request's device footprint (work space, conditioning
  * temporaries, and the spectrum with its build temporaries when the model is
- * not resident) fits the HBM budget (device memory of the library's own
- * stream-ordered pool, which keeps up to 4 GiB of freed memory mapped, is not
- * counted); a request that does not fit waits, and
+ * not resident) fits the HBM budget (freed memory that the library's
+ * stream-ordered pool keeps mapped is not counted); a request that does not
+ * fit waits, and
  * later requests may pass it at most max_bypass times.  Spectra stay resident
  * in an LRU cache keyed by model, grid and ipad.  Each request runs
  * ss3d_spectrum_create (on a cache miss), ss3d_realize and, with data,
@@ -344,6 +344,11 @@ int ss3d_set_stream(void *stream);
  * thread's work space. */
 int64_t ss3d_realize_workspace_bytes(const ss3d_spectrum *sp, int nreal, int precision, int host_out);
 int ss3d_release_workspace(void);
+
+/* The library takes its device memory from the device's stream-ordered pool
+ * and keeps freed memory mapped for its next calls; ss3d_trim_pool synchronises
+ * the device and returns the pool's unused memory to it. */
+int ss3d_trim_pool(void);
 
 /* Message of the last failing call on this thread ("" if none). */
 const char *ss3d_last_error(void);

@@ -24,7 +24,7 @@ EXPORTS = (
     "ss3d_realize", "ss3d_debug_states", "ss3d_debug_coefficients", "ss3d_row_state",
     "ss3d_vario", "ss3d_condition",
     "ss3d_set_stream", "ss3d_last_error", "ss3d_version", "ss3d_profile", "ss3d_profile_read", "ss3d_autotune", "ss3d_set_variant",
-    "ss3d_realize_workspace_bytes", "ss3d_release_workspace",
+    "ss3d_realize_workspace_bytes", "ss3d_release_workspace", "ss3d_trim_pool",
     "ss3d_batch_create", "ss3d_batch_run", "ss3d_batch_autotune", "ss3d_batch_info", "ss3d_batch_time",
     "ss3d_batch_schedule", "ss3d_batch_set_schedule", "ss3d_batch_free",
     "ss3d_server_create", "ss3d_server_submit", "ss3d_server_wait", "ss3d_server_stats", "ss3d_server_clock",
@@ -141,6 +141,7 @@ def lib():
         "ss3d_set_variant": (I, [I, I, I, I]),
         "ss3d_realize_workspace_bytes": (I64, [P, I, I, I]),
         "ss3d_release_workspace": (I, []),
+        "ss3d_trim_pool": (I, []),
         "ss3d_row_state": (I, [P, I, I, I64, I, I, P]),
         "ss3d_batch_create": (I, [P, I, P]),
         "ss3d_batch_run": (I, [P]),

@@ -160,13 +160,15 @@ int get_ctx(DevCtx** out) {
     CK(cudaMemcpy(c.twf, hf.data(), sizeof(float2) * ntw, cudaMemcpyHostToDevice));
     CK(cudaMemcpy(c.twd, hd.data(), sizeof(double2) * ntw, cudaMemcpyHostToDevice));
     CK(cudaMemcpy(c.ptab, ht.data(), sizeof(uint32_t) * 3 * 2048, cudaMemcpyHostToDevice));
-    // Work spaces and temporaries come from the device's stream-ordered pool.
-    // Keep up to 4 GiB of freed pool memory mapped between synchronisations,
-    // so that a work space released by one call and taken again by the next
-    // does not pay for unmapping and mapping its pages each time.
+    // Spectra, work spaces and temporaries come from the device's
+    // stream-ordered pool.  Freed pool memory stays mapped (release threshold
+    // unlimited): mapping device pages costs about a millisecond per few MB
+    // here, so a spectrum or work space freed by one call and taken again by
+    // the next must not be unmapped in between.  ss3d_release_workspace gives
+    // the pool's free memory back to the device.
     cudaMemPool_t pool;
     if (cudaDeviceGetDefaultMemPool(&pool, dev) == cudaSuccess) {
-      uint64_t keep = (uint64_t)4 << 30;
+      uint64_t keep = ~(uint64_t)0;
       cudaMemPoolSetAttribute(pool, cudaMemPoolAttrReleaseThreshold, &keep);
     }
     cudaGetLastError();
@@ -575,6 +577,16 @@ extern "C" int64_t ss3d_realize_workspace_bytes(const ss3d_spectrum* sp, int nre
 extern "C" int ss3d_release_workspace(void) {
   for (Workspace& w : g_ws) w.release(g_stream);
   cudaStreamSynchronize(g_stream);
+  return SS3D_OK;
+}
+
+extern "C" int ss3d_trim_pool(void) {
+  int dev = 0;
+  CK(cudaGetDevice(&dev));
+  cudaMemPool_t pool;
+  CK(cudaDeviceGetDefaultMemPool(&pool, dev));
+  CK(cudaDeviceSynchronize());
+  CK(cudaMemPoolTrimTo(pool, 0));
   return SS3D_OK;
 }
 
