@@ -154,9 +154,11 @@ int ss3d_realize_noalloc(const ss3d_spectrum *sp, int iseed, int64_t r_first, in
  * variants picked for {middle pass, synthesis pass, row pass}. */
 int ss3d_autotune(const ss3d_spectrum *sp, int igauss, int precision, int nreal, int chosen[3]);
 
-/* Explicit variant (0..3) of kernel kind 0 middle pass, 1 synthesis pass,
- * 2 row pass, for one precision and transform length 2^logn.  Every variant
- * computes the same values; they differ in tile shape only. */
+/* Explicit variant of kernel kind 0 middle pass, 1 synthesis pass, 2 row
+ * pass, for one precision and transform length 2^logn: 0..3 one line per
+ * thread; for the FP32 column passes (kinds 0, 1) also 4..7, two adjacent
+ * lines per thread on the packed FP32 instructions.  Every variant computes
+ * the same values; they differ in tile shape and instruction form only. */
 int ss3d_set_variant(int kind, int precision, int logn, int variant);
 
 /* ---------------------------------------------------------------- batched form */

@@ -200,6 +200,141 @@ __device__ __forceinline__ void colgen_body(const AxisArgs& a, const Geo& g, con
       });
 }
 
+// ---------------------------------------------------------------- column-pair passes (FP32)
+// The same two passes with two adjacent lines per thread held as a cpair (real
+// parts of both in x, imaginary parts in y): every butterfly operation is one
+// packed sm_100 instruction for two elements, and the two complex values are
+// one 16-byte access.  Lines 2u and 2u+1 lie in the same row (the row pitch HP
+// is even).  The operations per lane are those of the one-line bodies, so the
+// results are the same bits.  Variant bit 1 halves the tile, bit 0 doubles
+// the pairs per thread.
+template <int LOGN, int V = 0> struct PairCfg {
+  static constexpr int N = 1 << LOGN;
+  static constexpr int ETW = (V & 1) ? 16 : 8;
+  static constexpr int ET = N < ETW ? N : ETW;    // pairs per thread
+  static constexpr int TPC = N / ET;
+  static constexpr int E = 4096 >> ((V >> 1) & 1);
+  static constexpr int TX0 = E / N;
+  static constexpr int TX = TX0 > 64 ? 64 : (TX0 < 2 ? 2 : TX0);   // pairs of lines per tile
+  static constexpr int NTH = TX * TPC;
+  static_assert(NTH <= 1024, "tile too large");
+};
+
+// twiddles e^{-2 pi i m/N}, m < N, each component broadcast to both lanes
+template <int N, int NTH>
+__device__ __forceinline__ void load_tw_pair(cpair* stw, const Tw& tw) {
+  for (int q = threadIdx.x; q < N; q += NTH) {
+    const float2 w = tw.f[N - 1 + q];
+    stw[q] = cpair{make_float2(w.x, w.x), make_float2(w.y, w.y)};
+  }
+}
+
+__device__ __forceinline__ cpair pair_of(float4 v) { return cpair{make_float2(v.x, v.z), make_float2(v.y, v.w)}; }
+__device__ __forceinline__ float4 quad_of(cpair v) { return make_float4(v.x.x, v.y.x, v.x.y, v.y.y); }
+
+template <int LOGN, int TX, int TPC, int SIGN>
+__device__ __forceinline__ void col_body_pair(const AxisArgs& a, const Geo& g, const float2* in, float2* out,
+                                              const Tw& tw, int item, unsigned char* smraw) {
+  constexpr int N = 1 << LOGN;
+  constexpr int NTH = TX * TPC;
+  cpair* s = reinterpret_cast<cpair*>(smraw);
+  cpair* stw = s + N * TX;
+  const int r = item % a.nreal;
+  const int tile = item / a.nreal;
+  const int grp = tile / a.tpg;
+  const int line = ((tile % a.tpg) * TX + (int)threadIdx.x % TX) * 2;
+  const bool valid = line_valid(g, line, a.lines);
+  const long long off = (long long)grp * a.gstride + line + (long long)r * a.rstride;
+  const float4* src = reinterpret_cast<const float4*>(in + off);
+  float4* dst = reinterpret_cast<float4*>(out + off);
+  const int S2 = (int)(a.S / 2);   // stride in pairs: S is a multiple of the even row pitch
+  const int nout = a.nout;
+  constexpr int NR0 = N / Sched<LOGN>::radix(0);
+  load_tw_pair<N, NTH>(stw, tw);
+  __syncthreads();
+  fft_tile<LOGN, TX, TPC, SIGN>(
+      s, stw,
+      [&](int jb, int rr) {
+        return valid ? pair_of(src[(jb + rr * NR0) * S2]) : cpair{make_float2(0.f, 0.f), make_float2(0.f, 0.f)};
+      },
+      [&](int pos, cpair v) {
+        if (valid && pos < nout) dst[pos * S2] = quad_of(v);
+      });
+}
+
+// synthesis + first inverse pass for two lines (indices i0 = even, i1 = i0 + 1
+// of one row); the row state of a position serves both, the two amplitudes
+// are one 8-byte load.  Decisions as in colgen_body.
+template <int LOGN, int TX, int TPC, int GAUSS>
+__device__ __forceinline__ void colgen_body_pair(const AxisArgs& a, const Geo& g, const float* __restrict__ amp,
+                                                 const uint32_t* __restrict__ rowstates,
+                                                 const uint32_t* __restrict__ apow, float2* out, const Tw& tw,
+                                                 int item, unsigned char* smraw) {
+  constexpr int N = 1 << LOGN;
+  constexpr int NTH = TX * TPC;
+  constexpr int R0 = Sched<LOGN>::radix(0);
+  constexpr int NR0 = N / R0;
+  cpair* s = reinterpret_cast<cpair*>(smraw);
+  cpair* stw = s + N * TX;
+  const int r = item % a.nreal;
+  const int tile = item / a.nreal;
+  const int grp = tile / a.tpg;
+  const int line = ((tile % a.tpg) * TX + (int)threadIdx.x % TX) * 2;
+  const bool valid = line_valid(g, line, a.lines);
+  const int lsafe = valid ? line : 0;
+  const bool zaxis = a.axis == 2;
+  const int i0 = zaxis ? lsafe % g.HP : lsafe;
+  const int i1 = i0 + 1;                     // may be the row padding (amplitude 0)
+  const int j0 = zaxis ? lsafe / g.HP : 0;
+  const int m = g.npx - 1;                   // npx is a power of two: indices wrap inside the table
+  const uint32_t ai0 = __ldg(apow + (i0 & m)), aip0 = __ldg(apow + ((g.npx - i0) & m));
+  const uint32_t ai1 = __ldg(apow + (i1 & m)), aip1 = __ldg(apow + ((g.npx - i1) & m));
+  const bool iedge0 = (i0 == 0) || (2 * i0 == g.npx), iedge1 = 2 * i1 == g.npx;
+  const int jp0 = (-j0) & (g.npy - 1);
+  const bool cgt = zaxis && j0 > jp0;
+  const bool selfrow = !zaxis || j0 == jp0;
+  const bool self0 = selfrow && iedge0, self1 = selfrow && iedge1;
+  const int rowstride = zaxis ? 1 : g.npz;
+  const uint32_t* rs = rowstates + (size_t)r * g.npy * g.npz;
+  const uint32_t* rs_own = rs + (zaxis ? (size_t)j0 * g.npz : 0);
+  const uint32_t* rs_par = rs + (zaxis ? (size_t)jp0 * g.npz : 0);
+  const long long cbase = (long long)grp * a.gstride + lsafe;
+  const float2* ap = reinterpret_cast<const float2*>(amp + cbase);
+  float4* dst = reinterpret_cast<float4*>(out + cbase + (long long)r * a.rstride);
+  const int S2 = (int)(a.S / 2);
+  const int nout = a.nout;
+  load_tw_pair<N, NTH>(stw, tw);
+  __syncthreads();
+  fft_tile<LOGN, TX, TPC, +1>(
+      s, stw,
+      [&](int jb, int rr) {
+        const int p = jb + rr * NR0;
+        const float2 am = __ldg(ap + p * S2);
+        bool greater, mid;
+        if (rr == 0) {
+          mid = jb == 0;
+          greater = mid && cgt;
+        } else if (2 * rr == R0) {
+          mid = jb == 0;
+          greater = !mid || cgt;
+        } else {
+          mid = false;
+          greater = 2 * rr > R0;
+        }
+        const int pp = (N - p) & (N - 1);
+        const uint32_t st = __ldg(greater ? rs_par + pp * rowstride : rs_own + p * rowstride);
+        const float2 c0 = coef_from_state<float, GAUSS>(pm_mulmod(st, greater ? aip0 : ai0), am.x, mid && self0,
+                                                        greater);
+        const float2 c1 = coef_from_state<float, GAUSS>(pm_mulmod(st, greater ? aip1 : ai1), am.y, mid && self1,
+                                                        greater);
+        return valid ? cpair{make_float2(c0.x, c1.x), make_float2(c0.y, c1.y)}
+                     : cpair{make_float2(0.f, 0.f), make_float2(0.f, 0.f)};
+      },
+      [&](int pos, cpair v) {
+        if (valid && pos < nout) dst[pos * S2] = quad_of(v);
+      });
+}
+
 // ---------------------------------------------------------------- block reduction helpers
 template <int NTH>
 __device__ __forceinline__ void block_sum2(double& a, double& b) {

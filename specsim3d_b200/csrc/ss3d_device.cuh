@@ -17,25 +17,77 @@ constexpr uint32_t PM_M = 2147483647u;  // 2^31 - 1
 constexpr uint32_t PM_A = 16807u;
 
 // ---------------------------------------------------------------- complex
+// Three complex types share one set of operations, written once over the
+// component type K of C::x and C::y:
+//   double2  K = double  (FP64 path)
+//   float2   K = float   (FP32, one column per thread)
+//   cpair    K = float2  (FP32, two adjacent columns per thread: x holds the
+//                          real parts of both, y the imaginary parts)
+// For float and float2 every component operation is one explicitly rounded
+// IEEE operation (no contraction left to the compiler), and cpair runs the
+// packed sm_100 forms of the same operations lane by lane, so a transform
+// gives the same bits in either FP32 layout.
+struct __align__(16) cpair {
+  float2 x, y;
+};
+
 template <typename R> struct cpx;
 template <> struct cpx<float> { using T = float2; };
 template <> struct cpx<double> { using T = double2; };
 template <typename R> using cpx_t = typename cpx<R>::T;
 
-template <typename C> __device__ __forceinline__ C cmk(decltype(C::x) a, decltype(C::x) b) { C c; c.x = a; c.y = b; return c; }
-template <typename C> __device__ __forceinline__ C cadd(C a, C b) { return cmk<C>(a.x + b.x, a.y + b.y); }
-template <typename C> __device__ __forceinline__ C csub(C a, C b) { return cmk<C>(a.x - b.x, a.y - b.y); }
-template <typename C> __device__ __forceinline__ C cmul(C a, C b) {
-  return cmk<C>(a.x * b.x - a.y * b.y, a.x * b.y + a.y * b.x);
+__device__ __forceinline__ double kadd(double a, double b) { return a + b; }
+__device__ __forceinline__ double ksub(double a, double b) { return a - b; }
+__device__ __forceinline__ double kmul(double a, double b) { return a * b; }
+__device__ __forceinline__ double kfma(double a, double b, double c) { return fma(a, b, c); }
+__device__ __forceinline__ double kneg(double a) { return -a; }
+__device__ __forceinline__ float kadd(float a, float b) { return __fadd_rn(a, b); }
+__device__ __forceinline__ float ksub(float a, float b) { return __fsub_rn(a, b); }
+__device__ __forceinline__ float kmul(float a, float b) { return __fmul_rn(a, b); }
+__device__ __forceinline__ float kfma(float a, float b, float c) { return __fmaf_rn(a, b, c); }
+__device__ __forceinline__ float kneg(float a) { return -a; }
+#if defined(__CUDA_ARCH__) && __CUDA_ARCH__ >= 1000
+__device__ __forceinline__ float2 kadd(float2 a, float2 b) { return __fadd2_rn(a, b); }
+__device__ __forceinline__ float2 kmul(float2 a, float2 b) { return __fmul2_rn(a, b); }
+__device__ __forceinline__ float2 kfma(float2 a, float2 b, float2 c) { return __ffma2_rn(a, b, c); }
+#else
+__device__ __forceinline__ float2 kadd(float2 a, float2 b) { return make_float2(__fadd_rn(a.x, b.x), __fadd_rn(a.y, b.y)); }
+__device__ __forceinline__ float2 kmul(float2 a, float2 b) { return make_float2(__fmul_rn(a.x, b.x), __fmul_rn(a.y, b.y)); }
+__device__ __forceinline__ float2 kfma(float2 a, float2 b, float2 c) {
+  return make_float2(__fmaf_rn(a.x, b.x, c.x), __fmaf_rn(a.y, b.y, c.y));
 }
-// a * conj(b) when conjugate is true
+#endif
+__device__ __forceinline__ float2 kneg(float2 a) { return make_float2(-a.x, -a.y); }
+// a - b = fma(b, -1, a): the product is exact, so this is the IEEE difference
+__device__ __forceinline__ float2 ksub(float2 a, float2 b) { return kfma(b, make_float2(-1.f, -1.f), a); }
+
+template <typename K> __device__ __forceinline__ K kconst(double v);
+template <> __device__ __forceinline__ double kconst<double>(double v) { return v; }
+template <> __device__ __forceinline__ float kconst<float>(double v) { return (float)v; }
+template <> __device__ __forceinline__ float2 kconst<float2>(double v) { return make_float2((float)v, (float)v); }
+
+template <typename C> using comp_t = decltype(C::x);
+template <typename C> __device__ __forceinline__ C cmk(comp_t<C> a, comp_t<C> b) { C c; c.x = a; c.y = b; return c; }
+template <typename C> __device__ __forceinline__ C cadd(C a, C b) { return cmk<C>(kadd(a.x, b.x), kadd(a.y, b.y)); }
+template <typename C> __device__ __forceinline__ C csub(C a, C b) { return cmk<C>(ksub(a.x, b.x), ksub(a.y, b.y)); }
+template <typename C> __device__ __forceinline__ C cmul(C a, C b) {
+  return cmk<C>(kfma(kneg(a.y), b.y, kmul(a.x, b.x)), kfma(a.y, b.x, kmul(a.x, b.y)));
+}
+// a * b, or a * conj(b) when conjb is true
 template <typename C> __device__ __forceinline__ C cmul_sgn(C a, C b, bool conjb) {
-  decltype(C::x) by = conjb ? -b.y : b.y;
-  return cmk<C>(a.x * b.x - a.y * by, a.x * by + a.y * b.x);
+  if (conjb) return cmk<C>(kfma(a.y, b.y, kmul(a.x, b.x)), kfma(kneg(a.x), b.y, kmul(a.y, b.x)));
+  return cmul(a, b);
+}
+// a + s i b and a - s i b, s = SIGN (multiplication by +-i is exact)
+template <int SIGN, typename C> __device__ __forceinline__ C caddi(C a, C b) {
+  return SIGN > 0 ? cmk<C>(ksub(a.x, b.y), kadd(a.y, b.x)) : cmk<C>(kadd(a.x, b.y), ksub(a.y, b.x));
+}
+template <int SIGN, typename C> __device__ __forceinline__ C csubi(C a, C b) {
+  return SIGN > 0 ? cmk<C>(kadd(a.x, b.y), ksub(a.y, b.x)) : cmk<C>(ksub(a.x, b.y), kadd(a.y, b.x));
 }
 // multiply by (sign * i): forward (sign -1) gives -i, inverse gives +i
 template <int SIGN, typename C> __device__ __forceinline__ C cmul_si(C a) {
-  return SIGN > 0 ? cmk<C>(-a.y, a.x) : cmk<C>(a.y, -a.x);
+  return SIGN > 0 ? cmk<C>(kneg(a.y), a.x) : cmk<C>(a.y, kneg(a.x));
 }
 
 // ---------------------------------------------------------------- Park-Miller
@@ -269,25 +321,31 @@ template <int SIGN, typename C> __device__ __forceinline__ void dft2(C& a, C& b)
   C t = a; a = cadd(t, b); b = csub(t, b);
 }
 template <int SIGN, typename C> __device__ __forceinline__ void dft4(C& v0, C& v1, C& v2, C& v3) {
-  C t0 = cadd(v0, v2), t1 = csub(v0, v2), t2 = cadd(v1, v3), t3 = cmul_si<SIGN>(csub(v1, v3));
-  v0 = cadd(t0, t2); v2 = csub(t0, t2); v1 = cadd(t1, t3); v3 = csub(t1, t3);
+  C t0 = cadd(v0, v2), t1 = csub(v0, v2), t2 = cadd(v1, v3), d = csub(v1, v3);
+  v0 = cadd(t0, t2); v2 = csub(t0, t2); v1 = caddi<SIGN>(t1, d); v3 = csubi<SIGN>(t1, d);
 }
+// radix 8 as two radix 4 and the w8 combination.  With w8 = (1 + s i)/sqrt(2),
+// q = (x + y)/sqrt(2) and u = (x - y)/sqrt(2) of o = (x, y):
+//   s = +1:  o w8 = (u, q),   o w8^3 = (-q, u)
+//   s = -1:  o w8 = (q, -u),  o w8^3 = (-u, -q)
 template <int SIGN, typename C> __device__ __forceinline__ void dft8(C* v) {
-  using R = decltype(C::x);
+  using K = comp_t<C>;
   C e0 = v[0], e1 = v[2], e2 = v[4], e3 = v[6];
   C o0 = v[1], o1 = v[3], o2 = v[5], o3 = v[7];
   dft4<SIGN>(e0, e1, e2, e3);
   dft4<SIGN>(o0, o1, o2, o3);
-  const R r2 = (R)0.70710678118654752440;
-  // o1 *= w8, o2 *= w8^2 = sign*i, o3 *= w8^3
-  C w1 = cmk<C>(r2, SIGN * r2), w3 = cmk<C>(-r2, SIGN * r2);
-  o1 = cmul(o1, w1);
-  o2 = cmul_si<SIGN>(o2);
-  o3 = cmul(o3, w3);
+  const K r2 = kconst<K>(0.70710678118654752440);
+  const K q1 = kmul(kadd(o1.x, o1.y), r2), u1 = kmul(ksub(o1.x, o1.y), r2);
+  const K q3 = kmul(kadd(o3.x, o3.y), r2), u3 = kmul(ksub(o3.x, o3.y), r2);
   v[0] = cadd(e0, o0); v[4] = csub(e0, o0);
-  v[1] = cadd(e1, o1); v[5] = csub(e1, o1);
-  v[2] = cadd(e2, o2); v[6] = csub(e2, o2);
-  v[3] = cadd(e3, o3); v[7] = csub(e3, o3);
+  v[2] = caddi<SIGN>(e2, o2); v[6] = csubi<SIGN>(e2, o2);
+  if constexpr (SIGN > 0) {
+    v[1] = cmk<C>(kadd(e1.x, u1), kadd(e1.y, q1)); v[5] = cmk<C>(ksub(e1.x, u1), ksub(e1.y, q1));
+    v[3] = cmk<C>(ksub(e3.x, q3), kadd(e3.y, u3)); v[7] = cmk<C>(kadd(e3.x, q3), ksub(e3.y, u3));
+  } else {
+    v[1] = cmk<C>(kadd(e1.x, q1), ksub(e1.y, u1)); v[5] = cmk<C>(ksub(e1.x, q1), kadd(e1.y, u1));
+    v[3] = cmk<C>(ksub(e3.x, u3), ksub(e3.y, q3)); v[7] = cmk<C>(kadd(e3.x, u3), kadd(e3.y, q3));
+  }
 }
 template <int R, int SIGN, typename C> __device__ __forceinline__ void dftR(C* v) {
   if constexpr (R == 8) dft8<SIGN>(v);

@@ -57,25 +57,44 @@ __device__ __forceinline__ void load_tw(C* s, const C* g, int n, int cnt) {
 // (kind 0: column pass, 1: column pass with synthesis, 2: C2R rows)
 int g_variant[3][2][16] = {};
 
+// Tile configuration of a column pass: variants 0-3 one line per thread
+// (ColCfg), 4-7 two lines per thread (PairCfg, FP32 only).
+// LPT lines per tile, EB bytes per shared-memory entry.
+template <typename R, int LOGN, int V, bool PAIR = (V >= 4)> struct AxisCfg : ColCfg<R, LOGN, V> {
+  static constexpr int LPT = ColCfg<R, LOGN, V>::TX;
+  static constexpr int EB = sizeof(cpx_t<R>);
+};
+template <typename R, int LOGN, int V> struct AxisCfg<R, LOGN, V, true> : PairCfg<LOGN, V & 3> {
+  static_assert(sizeof(R) == 4, "two-line tiles are FP32 only");
+  static constexpr int LPT = 2 * PairCfg<LOGN, V & 3>::TX;
+  static constexpr int EB = sizeof(cpair);
+};
+
 // c2c transform along a strided axis (in place allowed), unscaled, pruned store
 template <typename R, int LOGN, int SIGN, int V>
-__global__ void __launch_bounds__(ColCfg<R, LOGN, V>::NTH) k_col(AxisArgs a, Geo g, const cpx_t<R>* in,
-                                                                cpx_t<R>* out, Tw tw) {
+__global__ void __launch_bounds__(AxisCfg<R, LOGN, V>::NTH) k_col(AxisArgs a, Geo g, const cpx_t<R>* in,
+                                                                 cpx_t<R>* out, Tw tw) {
   extern __shared__ __align__(16) unsigned char smraw[];
-  using CF = ColCfg<R, LOGN, V>;
-  col_body<R, LOGN, CF::TX, CF::TPC, SIGN>(a, g, in, out, tw, blockIdx.x, smraw);
+  using CF = AxisCfg<R, LOGN, V>;
+  if constexpr (V >= 4)
+    col_body_pair<LOGN, CF::TX, CF::TPC, SIGN>(a, g, in, out, tw, blockIdx.x, smraw);
+  else
+    col_body<R, LOGN, CF::TX, CF::TPC, SIGN>(a, g, in, out, tw, blockIdx.x, smraw);
 }
 
 // first inverse pass with the coefficient synthesis fused into the loader
 // (GAUSS: igauss of the realizations, 0 phases, 1 Gaussian coefficients)
 template <typename R, int LOGN, int V, int GAUSS>
-__global__ void __launch_bounds__(ColCfg<R, LOGN, V>::NTH) k_colgen(AxisArgs a, Geo g, const R* __restrict__ amp,
-                                                                   const uint32_t* __restrict__ rowstates,
-                                                                   const uint32_t* __restrict__ apow, cpx_t<R>* out,
-                                                                   Tw tw) {
+__global__ void __launch_bounds__(AxisCfg<R, LOGN, V>::NTH) k_colgen(AxisArgs a, Geo g, const R* __restrict__ amp,
+                                                                    const uint32_t* __restrict__ rowstates,
+                                                                    const uint32_t* __restrict__ apow,
+                                                                    cpx_t<R>* out, Tw tw) {
   extern __shared__ __align__(16) unsigned char smraw[];
-  using CF = ColCfg<R, LOGN, V>;
-  colgen_body<R, LOGN, CF::TX, CF::TPC, GAUSS>(a, g, amp, rowstates, apow, out, tw, blockIdx.x, smraw);
+  using CF = AxisCfg<R, LOGN, V>;
+  if constexpr (V >= 4)
+    colgen_body_pair<LOGN, CF::TX, CF::TPC, GAUSS>(a, g, amp, rowstates, apow, out, tw, blockIdx.x, smraw);
+  else
+    colgen_body<R, LOGN, CF::TX, CF::TPC, GAUSS>(a, g, amp, rowstates, apow, out, tw, blockIdx.x, smraw);
 }
 
 // Standalone synthesis of the full half spectrum of nreal realizations.
@@ -373,17 +392,17 @@ template <> struct MaxL<double> { static constexpr int v = MAX_LOGN_D; };
 template <typename R, int L, int SIGN, int V>
 static cudaError_t run_axis_c2c_v(const AxisArgs& a, const Geo& g, const cpx_t<R>* in, cpx_t<R>* out, Tw tw,
                                   cudaStream_t st) {
-  using CF = ColCfg<R, L, V>;
+  using CF = AxisCfg<R, L, V>;
   if constexpr (L == 0) {
     // length-1 transform: identity; copy when out-of-place
     if (in != out) return cudaErrorInvalidValue;
     return cudaSuccess;
   } else {
-    size_t smem = (size_t)(CF::N * CF::TX + CF::N) * sizeof(cpx_t<R>);
+    size_t smem = (size_t)(CF::N * CF::TX + CF::N) * CF::EB;
     cudaError_t e = set_smem(k_col<R, L, SIGN, V>, smem);
     if (e != cudaSuccess) return e;
     AxisArgs b = a;
-    b.tpg = (a.lines + CF::TX - 1) / CF::TX;
+    b.tpg = (a.lines + CF::LPT - 1) / CF::LPT;
     unsigned blocks = (unsigned)((long long)b.tpg * a.ngroups * a.nreal);
     k_col<R, L, SIGN, V><<<blocks, CF::NTH, smem, st>>>(b, g, in, out, tw);
     ++g_launch_count;
@@ -394,16 +413,16 @@ static cudaError_t run_axis_c2c_v(const AxisArgs& a, const Geo& g, const cpx_t<R
 template <typename R, int L, int V>
 static cudaError_t run_axis_gen_v(const AxisArgs& a, const Geo& g, const R* amp, const uint32_t* rs,
                                   const uint32_t* apow, cpx_t<R>* out, Tw tw, cudaStream_t st) {
-  using CF = ColCfg<R, L, V>;
+  using CF = AxisCfg<R, L, V>;
   if constexpr (L == 0) {
     return cudaErrorInvalidValue;
   } else {
-    size_t smem = (size_t)(CF::N * CF::TX + CF::N) * sizeof(cpx_t<R>);
+    size_t smem = (size_t)(CF::N * CF::TX + CF::N) * CF::EB;
     auto kern = g.d == 2 ? k_colgen<R, L, V, 1> : k_colgen<R, L, V, 0>;
     cudaError_t e = set_smem(kern, smem);
     if (e != cudaSuccess) return e;
     AxisArgs b = a;
-    b.tpg = (a.lines + CF::TX - 1) / CF::TX;
+    b.tpg = (a.lines + CF::LPT - 1) / CF::LPT;
     unsigned blocks = (unsigned)((long long)b.tpg * a.ngroups * a.nreal);
     kern<<<blocks, CF::NTH, smem, st>>>(b, g, amp, rs, apow, out, tw);
     ++g_launch_count;
@@ -441,6 +460,15 @@ static cudaError_t run_axis_c2c(const AxisArgs& a, const Geo& g, const cpx_t<R>*
       case 3: return run_axis_c2c_v<R, L, SIGN, 3>(a, g, in, out, tw, st);
       default: break;
     }
+    if constexpr (sizeof(R) == 4) {
+      switch (g_variant[0][1][L]) {
+        case 4: return run_axis_c2c_v<R, L, SIGN, 4>(a, g, in, out, tw, st);
+        case 5: return run_axis_c2c_v<R, L, SIGN, 5>(a, g, in, out, tw, st);
+        case 6: return run_axis_c2c_v<R, L, SIGN, 6>(a, g, in, out, tw, st);
+        case 7: return run_axis_c2c_v<R, L, SIGN, 7>(a, g, in, out, tw, st);
+        default: break;
+      }
+    }
   }
   return run_axis_c2c_v<R, L, SIGN, 0>(a, g, in, out, tw, st);
 }
@@ -454,6 +482,15 @@ static cudaError_t run_axis_gen(const AxisArgs& a, const Geo& g, const R* amp, c
       case 2: return run_axis_gen_v<R, L, 2>(a, g, amp, rs, apow, out, tw, st);
       case 3: return run_axis_gen_v<R, L, 3>(a, g, amp, rs, apow, out, tw, st);
       default: break;
+    }
+    if constexpr (sizeof(R) == 4) {
+      switch (g_variant[1][1][L]) {
+        case 4: return run_axis_gen_v<R, L, 4>(a, g, amp, rs, apow, out, tw, st);
+        case 5: return run_axis_gen_v<R, L, 5>(a, g, amp, rs, apow, out, tw, st);
+        case 6: return run_axis_gen_v<R, L, 6>(a, g, amp, rs, apow, out, tw, st);
+        case 7: return run_axis_gen_v<R, L, 7>(a, g, amp, rs, apow, out, tw, st);
+        default: break;
+      }
     }
   }
   return run_axis_gen_v<R, L, 0>(a, g, amp, rs, apow, out, tw, st);

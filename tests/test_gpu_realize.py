@@ -161,8 +161,49 @@ def test_tile_variants_give_identical_results(gpu):
         for kind, logn in ((0, 7), (1, 5), (2, 6)):
             L.ss3d_set_variant(kind, prec, logn, 0)
     chosen = gpu.autotune(sp, 1, gpu.FP32, 2)
-    assert set(chosen.values()) <= {0, 1, 2, 3}
+    assert chosen["row_pass"] in {0, 1, 2, 3} and set(chosen.values()) <= set(range(8))
     assert np.array_equal(sp.realize(77, 2, 1, gpu.FP32), sp.realize(77, 2, 1, gpu.FP32))
+
+
+def _kinds_of(np3):
+    """(kind, log2 length) of the column passes of a periodic grid."""
+    lg = [int(v).bit_length() - 1 for v in np3]
+    if np3[2] > 1:
+        return [(1, lg[2])] + ([(0, lg[1])] if np3[1] > 1 else [])
+    return [(1, lg[1])] if np3[1] > 1 else []
+
+
+@pytest.mark.parametrize("igauss", [0, 1])
+@pytest.mark.parametrize("n,ipad", [((40, 36, 20), 1), ((64, 64, 16), 1), ((33, 17, 1), 1), ((1, 24, 12), 1),
+                                     ((100, 1, 30), 1)])
+def test_two_line_variants_identical(gpu, n, ipad, igauss):
+    """FP32 column passes with two adjacent lines per thread (packed FP32
+    instructions, variants 4-7) give the bits of the one-line tiles, including
+    grids whose half-spectrum rows end in a padding element and 2D grids whose
+    synthesis runs along y."""
+    from specsim3d_b200 import _lib
+    L = _lib.lib()
+    sts = [(2, 0.8, 14.0, 9.0, 5.0, 35.0, 10.0, 5.0)]
+    sp = gpu.Spectrum(sts, 0.2, (1.0, 1.0, 1.0), n, ipad)
+    kinds = [(k, lg) for k, lg in _kinds_of(sp.np) if 5 <= lg <= 10]
+    if not kinds:
+        pytest.skip("no tuned column length on this grid")
+    ref = sp.realize(4321, 3, igauss, gpu.FP32, dtype=np.float32)
+    try:
+        for v in (4, 5, 6, 7):
+            for kind, lg in kinds:
+                assert L.ss3d_set_variant(kind, gpu.FP32, lg, v) == 0
+            got = sp.realize(4321, 3, igauss, gpu.FP32, dtype=np.float32)
+            assert np.array_equal(got, ref), (v, float(np.max(np.abs(got - ref))))
+        # mixed: synthesis on two lines, middle pass on one, and the reverse
+        for vs, vm in ((4, 0), (0, 6)):
+            for kind, lg in kinds:
+                L.ss3d_set_variant(kind, gpu.FP32, lg, vs if kind == 1 else vm)
+            assert np.array_equal(sp.realize(4321, 3, igauss, gpu.FP32, dtype=np.float32), ref)
+    finally:
+        for kind, lg in kinds:
+            L.ss3d_set_variant(kind, gpu.FP32, lg, 0)
+    assert L.ss3d_set_variant(2, gpu.FP32, 6, 4) != 0      # the row pass has no two-line tiles
 
 
 @pytest.mark.parametrize("case", [0, 1, 2])
