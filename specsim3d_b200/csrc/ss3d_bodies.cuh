@@ -122,6 +122,60 @@ __device__ __forceinline__ cpx_t<R> coef_from_state(uint32_t s1, R am, bool self
   }
 }
 
+// The coefficients of the two lanes of a pair (states s0, s1 of their first
+// draws, amplitudes am): the operations of coef_from_state<float, GAUSS> lane
+// by lane, with the products and the logarithm's series on packed FP32
+// instructions and the hardware functions and integer steps per lane.
+__device__ __forceinline__ float2 m2log_f2(uint32_t s0, uint32_t s1) {
+  const float2 a = make_float2((float)(PM_M - s0), (float)(PM_M - s1));
+  const float2 b = ksub(kconst<float2>(4294967294.0), a);
+  const float2 z = make_float2(-__fdividef(a.x, b.x), -__fdividef(a.y, b.y));
+  const float2 z2 = kmul(z, z);
+  float2 p = kfma(z2, kconst<float2>(1.0f / 7.0f), kconst<float2>(1.0f / 5.0f));
+  p = kfma(z2, p, kconst<float2>(1.0f / 3.0f));
+  p = kfma(z2, p, kconst<float2>(1.0));
+  const float2 near1 = kmul(kconst<float2>(-4.0), kmul(p, z));
+  const float2 u = kmul(make_float2((float)s0, (float)s1), kconst<float2>(1.0f / 2147483647.0f));
+  const float2 far = kmul(kconst<float2>(-1.3862944f), make_float2(__log2f(u.x), __log2f(u.y)));
+  return make_float2(s0 >= 1610612736u ? near1.x : far.x, s1 >= 1610612736u ? near1.y : far.y);
+}
+__device__ __forceinline__ void phasor_f2(uint32_t s0, uint32_t s1, float2& c, float2& sn) {
+  const float2 q = kmul(make_float2((float)s0, (float)s1), kconst<float2>(4.0f / 2147483647.0f));
+  const int n0 = __float2int_rn(q.x), n1 = __float2int_rn(q.y);
+  const int rem0 = (int)(4u * s0 - (uint32_t)n0 * PM_M), rem1 = (int)(4u * s1 - (uint32_t)n1 * PM_M);
+  const float2 x = kmul(make_float2((float)rem0, (float)rem1), kconst<float2>(7.3145904e-10f));
+  float sp0, cp0, sp1, cp1;
+  __sincosf(x.x, &sp0, &cp0);
+  __sincosf(x.y, &sp1, &cp1);
+  const float c00 = (n0 & 1) ? sp0 : cp0, s00 = (n0 & 1) ? cp0 : sp0;
+  const float c01 = (n1 & 1) ? sp1 : cp1, s01 = (n1 & 1) ? cp1 : sp1;
+  c = make_float2(((n0 + 1) & 2) ? -c00 : c00, ((n1 + 1) & 2) ? -c01 : c01);
+  sn = make_float2((n0 & 2) ? -s00 : s00, (n1 & 2) ? -s01 : s01);
+}
+template <int GAUSS>
+__device__ __forceinline__ cpair coef_pair(uint32_t s0, uint32_t s1, float2 am, bool self0, bool self1, bool conj) {
+  if constexpr (GAUSS) {
+    const float2 L = m2log_f2(s0, s1);
+    const float2 rr = kmul(L, make_float2(rsqrtf(L.x), rsqrtf(L.y)));
+    float2 cs, sn;
+    phasor_f2(pm_mulmod(s0, PM_A), pm_mulmod(s1, PM_A), cs, sn);
+    const float2 ah = kmul(am, kconst<float2>(0.70710678118654752f));
+    const float2 a = make_float2(self0 ? am.x : ah.x, self1 ? am.y : ah.y);
+    const float2 re = kmul(a, kmul(rr, cs));
+    const float2 im = kmul(conj ? kneg(a) : a, kmul(rr, sn));
+    return cpair{re, make_float2(self0 ? 0.f : im.x, self1 ? 0.f : im.y)};
+  } else {
+    float2 cs, sn;
+    phasor_f2(s0, s1, cs, sn);
+    const float2 re = kmul(am, cs);
+    const float2 im0 = kmul(am, sn);
+    const float2 im = conj ? kneg(im0) : im0;
+    const float sg0 = (2ull * s0) < (uint64_t)PM_M ? am.x : -am.x, sg1 = (2ull * s1) < (uint64_t)PM_M ? am.y : -am.y;
+    return cpair{make_float2(self0 ? sg0 : re.x, self1 ? sg1 : re.y),
+                 make_float2(self0 ? 0.f : im.x, self1 ? 0.f : im.y)};
+  }
+}
+
 // First inverse pass with the coefficient synthesis fused into the loader.
 // axis 2: columns are (i, j) plane offsets, positions k;  axis 1 (npz = 1):
 // columns are i, positions j.  Along the transformed axis (length N) the
@@ -323,12 +377,9 @@ __device__ __forceinline__ void colgen_body_pair(const AxisArgs& a, const Geo& g
         }
         const int pp = (N - p) & (N - 1);
         const uint32_t st = __ldg(greater ? rs_par + pp * rowstride : rs_own + p * rowstride);
-        const float2 c0 = coef_from_state<float, GAUSS>(pm_mulmod(st, greater ? aip0 : ai0), am.x, mid && self0,
-                                                        greater);
-        const float2 c1 = coef_from_state<float, GAUSS>(pm_mulmod(st, greater ? aip1 : ai1), am.y, mid && self1,
-                                                        greater);
-        return valid ? cpair{make_float2(c0.x, c1.x), make_float2(c0.y, c1.y)}
-                     : cpair{make_float2(0.f, 0.f), make_float2(0.f, 0.f)};
+        const cpair c = coef_pair<GAUSS>(pm_mulmod(st, greater ? aip0 : ai0), pm_mulmod(st, greater ? aip1 : ai1),
+                                         am, mid && self0, mid && self1, greater);
+        return valid ? c : cpair{make_float2(0.f, 0.f), make_float2(0.f, 0.f)};
       },
       [&](int pos, cpair v) {
         if (valid && pos < nout) dst[pos * S2] = quad_of(v);
