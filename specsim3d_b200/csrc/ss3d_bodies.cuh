@@ -69,7 +69,9 @@ __device__ __forceinline__ void col_body(const AxisArgs& a, const Geo& g, const 
   const int line0 = (tile % a.tpg) * TX;
   const int t = threadIdx.x % TX;
   const bool valid = line_valid(g, line0 + t, a.lines);
-  const C* src = in + ((long long)grp * a.gstride + line0 + t + (long long)r * a.rstride);
+  // a line past the grid reads line 0 (in range) and stores nothing: the
+  // columns of a tile are independent transforms, so no select in the loader
+  const C* src = in + ((long long)grp * a.gstride + (valid ? line0 + t : 0) + (long long)r * a.rstride);
   C* dst = out + ((long long)grp * a.gstride + line0 + t + (long long)r * a.rstride);
   const int S = (int)a.S;   // offsets inside one realization's grid fit in 32 bits
   const int nout = a.nout;
@@ -77,7 +79,7 @@ __device__ __forceinline__ void col_body(const AxisArgs& a, const Geo& g, const 
   for (int q = threadIdx.x; q < N; q += NTH) stw[q] = twtab<R>(tw)[N - 1 + q];
   __syncthreads();
   fft_tile<LOGN, TX, TPC, SIGN>(
-      s, stw, [&](int jb, int r) { return valid ? src[(jb + r * NR0) * S] : cmk<C>(R(0), R(0)); },
+      s, stw, [&](int jb, int r) { return src[(jb + r * NR0) * S]; },
       [&](int pos, C v) {
         if (valid && pos < nout) dst[pos * S] = v;
       });
@@ -95,7 +97,7 @@ __device__ __forceinline__ cpx_t<R> coef_from_state(uint32_t s1, R am, bool self
     const uint32_t s2 = pm_mulmod(s1, PM_A);
     if constexpr (sizeof(R) == 4) {
       const float L = m2log_f(s1);
-      const float rr = L * rsqrtf(L);
+      const float rr = L * rsqrt_hw(L);
       float cs, sn;
       phasor_f(s2, cs, sn);
       const float a = self ? am : am * 0.70710678118654752f;
@@ -129,34 +131,31 @@ __device__ __forceinline__ cpx_t<R> coef_from_state(uint32_t s1, R am, bool self
 __device__ __forceinline__ float2 m2log_f2(uint32_t s0, uint32_t s1) {
   const float2 a = make_float2((float)(PM_M - s0), (float)(PM_M - s1));
   const float2 b = ksub(kconst<float2>(4294967294.0), a);
-  const float2 z = make_float2(-__fdividef(a.x, b.x), -__fdividef(a.y, b.y));
+  const float2 q = kmul(a, make_float2(rcp_hw(b.x), rcp_hw(b.y)));
+  const float2 z = kneg(q);
   const float2 z2 = kmul(z, z);
   float2 p = kfma(z2, kconst<float2>(1.0f / 7.0f), kconst<float2>(1.0f / 5.0f));
   p = kfma(z2, p, kconst<float2>(1.0f / 3.0f));
   p = kfma(z2, p, kconst<float2>(1.0));
   const float2 near1 = kmul(kconst<float2>(-4.0), kmul(p, z));
   const float2 u = kmul(make_float2((float)s0, (float)s1), kconst<float2>(1.0f / 2147483647.0f));
-  const float2 far = kmul(kconst<float2>(-1.3862944f), make_float2(__log2f(u.x), __log2f(u.y)));
+  const float2 far = kmul(kconst<float2>(-1.3862944f), make_float2(lg2_hw(u.x), lg2_hw(u.y)));
   return make_float2(s0 >= 1610612736u ? near1.x : far.x, s1 >= 1610612736u ? near1.y : far.y);
 }
 __device__ __forceinline__ void phasor_f2(uint32_t s0, uint32_t s1, float2& c, float2& sn) {
-  const float2 q = kmul(make_float2((float)s0, (float)s1), kconst<float2>(4.0f / 2147483647.0f));
+  const float2 q = kmul(make_float2((float)s0, (float)s1), kconst<float2>(2.0f / 2147483647.0f));
   const int n0 = __float2int_rn(q.x), n1 = __float2int_rn(q.y);
-  const int rem0 = (int)(4u * s0 - (uint32_t)n0 * PM_M), rem1 = (int)(4u * s1 - (uint32_t)n1 * PM_M);
-  const float2 x = kmul(make_float2((float)rem0, (float)rem1), kconst<float2>(7.3145904e-10f));
-  float sp0, cp0, sp1, cp1;
-  __sincosf(x.x, &sp0, &cp0);
-  __sincosf(x.y, &sp1, &cp1);
-  const float c00 = (n0 & 1) ? sp0 : cp0, s00 = (n0 & 1) ? cp0 : sp0;
-  const float c01 = (n1 & 1) ? sp1 : cp1, s01 = (n1 & 1) ? cp1 : sp1;
-  c = make_float2(((n0 + 1) & 2) ? -c00 : c00, ((n1 + 1) & 2) ? -c01 : c01);
-  sn = make_float2((n0 & 2) ? -s00 : s00, (n1 & 2) ? -s01 : s01);
+  const int rem0 = (int)(2u * s0 - (uint32_t)n0 * PM_M), rem1 = (int)(2u * s1 - (uint32_t)n1 * PM_M);
+  const float2 x = kmul(make_float2((float)rem0, (float)rem1), kconst<float2>(1.4629181e-9f));
+  const float sp0 = sin_hw(x.x), cp0 = cos_hw(x.x), sp1 = sin_hw(x.y), cp1 = cos_hw(x.y);
+  c = make_float2((n0 & 1) ? -cp0 : cp0, (n1 & 1) ? -cp1 : cp1);
+  sn = make_float2((n0 & 1) ? -sp0 : sp0, (n1 & 1) ? -sp1 : sp1);
 }
 template <int GAUSS>
 __device__ __forceinline__ cpair coef_pair(uint32_t s0, uint32_t s1, float2 am, bool self0, bool self1, bool conj) {
   if constexpr (GAUSS) {
     const float2 L = m2log_f2(s0, s1);
-    const float2 rr = kmul(L, make_float2(rsqrtf(L.x), rsqrtf(L.y)));
+    const float2 rr = kmul(L, make_float2(rsqrt_hw(L.x), rsqrt_hw(L.y)));
     float2 cs, sn;
     phasor_f2(pm_mulmod(s0, PM_A), pm_mulmod(s1, PM_A), cs, sn);
     const float2 ah = kmul(am, kconst<float2>(0.70710678118654752f));
@@ -205,7 +204,7 @@ __device__ __forceinline__ void colgen_body(const AxisArgs& a, const Geo& g, con
   const int line = line0 + t;
   const bool valid = line_valid(g, line, a.lines);
   // lines past the grid or in the row padding compute with line 0's indices
-  // (in range) and contribute zeros: no branch in the loader
+  // (in range) and store nothing: no branch or select in the loader
   const int lsafe = valid ? line : 0;
   const bool zaxis = a.axis == 2;
   const int i = zaxis ? lsafe % g.HP : lsafe;
@@ -246,8 +245,7 @@ __device__ __forceinline__ void colgen_body(const AxisArgs& a, const Geo& g, con
         const int pp = (N - p) & (N - 1);
         const uint32_t st = __ldg(greater ? rs_par + pp * rowstride : rs_own + p * rowstride);
         const uint32_t s1 = pm_mulmod(st, greater ? aip : ai);
-        const C v = coef_from_state<R, GAUSS>(s1, am, mid && selfcol, greater);
-        return valid ? v : cmk<C>(R(0), R(0));
+        return coef_from_state<R, GAUSS>(s1, am, mid && selfcol, greater);
       },
       [&](int pos, C v) {
         if (valid && pos < nout) dst[pos * S] = v;
@@ -299,7 +297,8 @@ __device__ __forceinline__ void col_body_pair(const AxisArgs& a, const Geo& g, c
   const int line = ((tile % a.tpg) * TX + (int)threadIdx.x % TX) * 2;
   const bool valid = line_valid(g, line, a.lines);
   const long long off = (long long)grp * a.gstride + line + (long long)r * a.rstride;
-  const float4* src = reinterpret_cast<const float4*>(in + off);
+  const long long off0 = (long long)grp * a.gstride + (valid ? line : 0) + (long long)r * a.rstride;
+  const float4* src = reinterpret_cast<const float4*>(in + off0);   // past the grid: line 0, nothing stored
   float4* dst = reinterpret_cast<float4*>(out + off);
   const int S2 = (int)(a.S / 2);   // stride in pairs: S is a multiple of the even row pitch
   const int nout = a.nout;
@@ -308,12 +307,73 @@ __device__ __forceinline__ void col_body_pair(const AxisArgs& a, const Geo& g, c
   __syncthreads();
   fft_tile<LOGN, TX, TPC, SIGN>(
       s, stw,
-      [&](int jb, int rr) {
-        return valid ? pair_of(src[(jb + rr * NR0) * S2]) : cpair{make_float2(0.f, 0.f), make_float2(0.f, 0.f)};
-      },
+      [&](int jb, int rr) { return pair_of(src[(jb + rr * NR0) * S2]); },
       [&](int pos, cpair v) {
         if (valid && pos < nout) dst[pos * S2] = quad_of(v);
       });
+}
+
+// Streamed two-line column pass: a persistent CTA walks tiles t = blockIdx.x,
+// blockIdx.x + gridDim.x, ...; the columns of tile t + gridDim.x are copied
+// into the second stage buffer (cp.async, no registers) while tile t is
+// transformed in place in the first.  Tile order: column block fastest, then
+// group, then realization, so the CTAs at work cover whole rows.  Same
+// operations per element as col_body_pair.
+template <int LOGN> struct StreamCfg {
+  static constexpr int N = 1 << LOGN;
+  static constexpr int ET = N < 8 ? N : 8;          // pairs per thread
+  static constexpr int TPC = N / ET;
+  static constexpr int TX0 = 4096 / N;
+  static constexpr int TX = TX0 > 64 ? 64 : (TX0 < 2 ? 2 : TX0);   // pairs of lines per tile
+  static constexpr int NTH = TX * TPC;
+  static constexpr size_t SMEM = (size_t)(N + 2 * N * TX) * sizeof(cpair);   // twiddles + two stages
+};
+
+template <int LOGN, int SIGN>
+__device__ __forceinline__ void col_stream_pair(const AxisArgs& a, const Geo& g, const float2* in, float2* out,
+                                                const Tw& tw, int ntiles, unsigned char* smraw) {
+  using SC = StreamCfg<LOGN>;
+  constexpr int N = SC::N, TX = SC::TX, TPC = SC::TPC, NTH = SC::NTH;
+  constexpr int NR0 = N / Sched<LOGN>::radix(0);
+  cpair* stw = reinterpret_cast<cpair*>(smraw);
+  cpair* stage[2] = {stw + N, stw + N + N * TX};
+  load_tw_pair<N, NTH>(stw, tw);
+  const int S = (int)a.S, S2 = S / 2;
+  const int tp = (int)threadIdx.x % TX;
+  auto issue = [&](cpair* st, int tile) {
+    const int cb = tile % a.tpg;
+    const int rest = tile / a.tpg;
+    const int grp = rest % a.ngroups, r = rest / a.ngroups;
+    const float2* src = in + (long long)grp * a.gstride + 2 * cb * TX + (long long)r * a.rstride;
+    for (int c = threadIdx.x; c < N * TX; c += NTH) {
+      const int row = c / TX, q = c % TX;
+      if (line_valid(g, 2 * (cb * TX + q), a.lines)) cp_async16(st + c, src + row * S + 2 * q);
+    }
+  };
+  int tile = blockIdx.x;
+  if (tile < ntiles) issue(stage[0], tile);
+  cp_async_commit();
+  for (int it = 0; tile < ntiles; ++it, tile += gridDim.x) {
+    cpair* cur = stage[it & 1];
+    if (tile + (int)gridDim.x < ntiles) issue(stage[(it + 1) & 1], tile + gridDim.x);
+    cp_async_commit();
+    cp_async_wait<1>();   // this thread's copies of the current tile have landed
+    __syncthreads();      // and everyone's (also: the twiddles)
+    const int cb = tile % a.tpg;
+    const int rest = tile / a.tpg;
+    const int grp = rest % a.ngroups, r = rest / a.ngroups;
+    const int line = 2 * (cb * TX + tp);
+    const bool valid = line_valid(g, line, a.lines);
+    float4* dst = reinterpret_cast<float4*>(out + (long long)grp * a.gstride + line + (long long)r * a.rstride);
+    const int nout = a.nout;
+    fft_tile<LOGN, TX, TPC, SIGN, TX, true>(
+        cur, stw, [&](int jb, int rr) { return pair_of(reinterpret_cast<const float4*>(cur)[(jb + rr * NR0) * TX + tp]); },
+        [&](int pos, cpair v) {
+          if (valid && pos < nout) dst[pos * S2] = quad_of(v);
+        });
+    __syncthreads();      // cur is refilled by the copies issued next iteration
+  }
+  cp_async_wait<0>();
 }
 
 // synthesis + first inverse pass for two lines (indices i0 = even, i1 = i0 + 1
@@ -377,9 +437,8 @@ __device__ __forceinline__ void colgen_body_pair(const AxisArgs& a, const Geo& g
         }
         const int pp = (N - p) & (N - 1);
         const uint32_t st = __ldg(greater ? rs_par + pp * rowstride : rs_own + p * rowstride);
-        const cpair c = coef_pair<GAUSS>(pm_mulmod(st, greater ? aip0 : ai0), pm_mulmod(st, greater ? aip1 : ai1),
-                                         am, mid && self0, mid && self1, greater);
-        return valid ? c : cpair{make_float2(0.f, 0.f), make_float2(0.f, 0.f)};
+        return coef_pair<GAUSS>(pm_mulmod(st, greater ? aip0 : ai0), pm_mulmod(st, greater ? aip1 : ai1), am,
+                                mid && self0, mid && self1, greater);
       },
       [&](int pos, cpair v) {
         if (valid && pos < nout) dst[pos * S2] = quad_of(v);

@@ -90,6 +90,19 @@ template <int SIGN, typename C> __device__ __forceinline__ C cmul_si(C a) {
   return SIGN > 0 ? cmk<C>(kneg(a.y), a.x) : cmk<C>(a.y, kneg(a.x));
 }
 
+// ---------------------------------------------------------------- asynchronous copies
+// 16-byte global -> shared copy that bypasses the registers (cached in L2
+// only); completion per thread by commit groups, visibility to the block by a
+// barrier after the wait.  Waits are the hardware's own (no spinning).
+__device__ __forceinline__ void cp_async16(void* smem, const void* gmem) {
+  const unsigned sa = (unsigned)__cvta_generic_to_shared(smem);
+  asm volatile("cp.async.cg.shared.global [%0], [%1], 16;\n" ::"r"(sa), "l"(gmem) : "memory");
+}
+__device__ __forceinline__ void cp_async_commit() { asm volatile("cp.async.commit_group;\n" ::: "memory"); }
+template <int PENDING> __device__ __forceinline__ void cp_async_wait() {
+  asm volatile("cp.async.wait_group %0;\n" ::"n"(PENDING) : "memory");
+}
+
 // ---------------------------------------------------------------- Park-Miller
 __host__ __device__ __forceinline__ uint32_t pm_mulmod(uint32_t a, uint32_t b) {
   // a, b < 2^31: p = a b < 2^62 = hi 2^32 + lo;  p mod (2^31 - 1) = (p & m) + (p >> 31) folded once
@@ -165,26 +178,31 @@ __host__ __device__ __forceinline__ int row_class(const Geo& g, int j, int k) {
 }
 
 // ---------------------------------------------------------------- coefficient synthesis
-// Unit phasor e^{2 pi i s/m} in float.  The nearest quarter turn n is taken
-// in integers (exact); the remainder |x| <= pi/4 (argument error below 5e-8:
-// one float rounding of the exact integer remainder) goes through the hardware
-// sine and cosine (__sincosf, absolute error about 4e-7), and the quarter turns
-// are applied by exchanging and negating the two.  Reducing to the quarter
-// also keeps the small systematic error of the hardware functions from adding
-// up coherently: the four quadrants use it with opposite signs, whereas a
-// reduction to [-pi, pi] alone left a bias that summed to 4e-5 sqrt(C0) at the
-// cell where every phase is 1 (the origin) on a 512^3 spectrum.
+// Hardware approximations of the PTX ISA (sin.approx, cos.approx, lg2.approx,
+// rsqrt.approx, rcp.approx; .ftz: every argument below is a normal number),
+// issued directly so that no range or subnormal handling is added around them.
+__device__ __forceinline__ float sin_hw(float x) { float r; asm("sin.approx.ftz.f32 %0, %1;" : "=f"(r) : "f"(x)); return r; }
+__device__ __forceinline__ float cos_hw(float x) { float r; asm("cos.approx.ftz.f32 %0, %1;" : "=f"(r) : "f"(x)); return r; }
+__device__ __forceinline__ float lg2_hw(float x) { float r; asm("lg2.approx.ftz.f32 %0, %1;" : "=f"(r) : "f"(x)); return r; }
+__device__ __forceinline__ float rsqrt_hw(float x) { float r; asm("rsqrt.approx.ftz.f32 %0, %1;" : "=f"(r) : "f"(x)); return r; }
+__device__ __forceinline__ float rcp_hw(float x) { float r; asm("rcp.approx.ftz.f32 %0, %1;" : "=f"(r) : "f"(x)); return r; }
+
+// Unit phasor e^{2 pi i s/m} in float.  The nearest half turn n (0, 1 or 2)
+// is taken in integers (exact); the remainder |x| <= pi/2 (argument error
+// about 1e-7: one float rounding of the exact integer remainder) goes through
+// the hardware sine and cosine (absolute error about 2^-21), and odd half
+// turns negate both.  Half of the phases use the hardware values with each
+// sign, so their small systematic error averages out over a spectrum instead
+// of adding up coherently: a reduction to [-pi, pi] without the alternating
+// sign left a bias that summed to 4e-5 sqrt(C0) at the cell where every phase
+// is 1 (the origin) on a 512^3 spectrum.
 __device__ __forceinline__ void phasor_f(uint32_t s, float& c, float& sn) {
-  const int n = __float2int_rn((float)s * (4.0f / 2147483647.0f));   // nearest quarter (off by one at most)
-  const int rem = (int)(4u * s - (uint32_t)n * PM_M);                // exact 4s - n m, |.| <= m/2 + 2^11
-  const float x = (float)rem * 7.3145904e-10f;                         // (pi/2) / (2^31-1)
-  float sp, cp;
-  __sincosf(x, &sp, &cp);
-  // rotate by n quarter turns: (c, s) -> (cp, sp), (-sp, cp), (-cp, -sp), (sp, -cp)
-  const bool odd = n & 1;
-  const float c0 = odd ? sp : cp, s0 = odd ? cp : sp;
-  c = ((n + 1) & 2) ? -c0 : c0;
-  sn = (n & 2) ? -s0 : s0;
+  const int n = __float2int_rn((float)s * (2.0f / 2147483647.0f));   // nearest half turn (off by one at most)
+  const int rem = (int)(2u * s - (uint32_t)n * PM_M);                // exact 2s - n m, |.| <= m/2 + 2^10
+  const float x = (float)rem * 1.4629181e-9f;                          // pi / (2^31-1)
+  const float sp = sin_hw(x), cp = cos_hw(x);
+  c = (n & 1) ? -cp : cp;
+  sn = (n & 1) ? -sp : sp;
 }
 __device__ __forceinline__ void phasor_d(uint32_t s, double& c, double& sn) {
   double u = (double)s / 2147483647.0;
@@ -192,18 +210,19 @@ __device__ __forceinline__ void phasor_d(uint32_t s, double& c, double& sn) {
 }
 // -2 ln(s/m) in float for s in [1, m-1].  For u = s/m >= 3/4 the logarithm is
 // 2 atanh(z), z = (u-1)/(u+1) = -(m-s)/(m+s) with |z| <= 1/7, from the exact
-// integer difference m-s (odd series to z^7, truncation below 2e-8 relative);
+// integer difference m-s (odd series to z^7, truncation below 2e-8 relative;
+// the quotient by the hardware reciprocal, relative error about 2^-23);
 // below 3/4 |ln u| >= 0.28 and the hardware log2 (absolute error ~2^-22) is
 // accurate to a few 1e-7 relative.
 __device__ __forceinline__ float m2log_f(uint32_t s) {
   const float a = (float)(PM_M - s);
-  const float z = -__fdividef(a, 4294967294.0f - a);        // (u-1)/(u+1), m + s = 2m - (m - s)
+  const float z = -(a * rcp_hw(4294967294.0f - a));        // (u-1)/(u+1), m + s = 2m - (m - s)
   const float z2 = z * z;
   float p = fmaf(z2, 1.0f / 7.0f, 1.0f / 5.0f);
   p = fmaf(z2, p, 1.0f / 3.0f);
   p = fmaf(z2, p, 1.0f);
   const float near1 = -4.0f * (p * z);
-  const float far = -1.3862944f * __log2f((float)s * (1.0f / 2147483647.0f));   // -2 ln 2 * log2(u)
+  const float far = -1.3862944f * lg2_hw((float)s * (1.0f / 2147483647.0f));   // -2 ln 2 * log2(u)
   return s >= 1610612736u ? near1 : far;                    // u >= 3/4
 }
 __device__ __forceinline__ double m2log_d(uint32_t s) {
@@ -248,7 +267,7 @@ __device__ __forceinline__ cpx_t<R> coefficient(const Geo& g, int i, int j, int 
     uint32_t s2 = pm_mulmod(s1, PM_A);
     if constexpr (sizeof(R) == 4) {
       const float L = m2log_f(s1);
-      float rr = L * rsqrtf(L);
+      float rr = L * rsqrt_hw(L);
       float cs, sn;
       phasor_f(s2, cs, sn);
       if (self) return cmk<C>(amp * (rr * cs), 0.f);
@@ -293,7 +312,7 @@ __device__ __forceinline__ cpx_t<R> coef_col(const Geo& g, int j, int k, R amp, 
     const uint32_t s2 = pm_mulmod(s1, PM_A);
     if constexpr (sizeof(R) == 4) {
       const float L = m2log_f(s1);
-      const float rr = L * rsqrtf(L);
+      const float rr = L * rsqrt_hw(L);
       float cs, sn;
       phasor_f(s2, cs, sn);
       if (self) return cmk<C>(amp * (rr * cs), 0.f);
