@@ -864,10 +864,9 @@ extern "C" int ss3d_autotune(const ss3d_spectrum* sp, int igauss, int precision,
   double best[3] = {1e30, 1e30, 1e30};
   int bestv[3] = {0, 0, 0};
   int rc = SS3D_OK;
-  // variants per kind: 0-3 everywhere; FP32 column passes also 4-7 (two
-  // lines per thread) and the FP32 middle pass 8 (streamed); a kind without
-  // variant v runs its variant v mod 4 meanwhile
-  const int nvk[3] = {precision == SS3D_FP32 ? 9 : 4, precision == SS3D_FP32 ? 8 : 4, 4};
+  // variants per kind: 0-3 everywhere, FP32 column passes also 4-7 (two
+  // lines per thread); the row pass runs its variant v mod 4 meanwhile
+  const int nvk[3] = {precision == SS3D_FP32 ? 8 : 4, precision == SS3D_FP32 ? 8 : 4, 4};
   auto vk = [&](int k, int v) { return v < nvk[k] ? v : v % 4; };
   for (int v = 0; v < nvk[0] && rc == SS3D_OK; v++) {
     for (int k = 0; k < 3; k++)
@@ -897,8 +896,7 @@ extern "C" int ss3d_autotune(const ss3d_spectrum* sp, int igauss, int precision,
 }
 
 extern "C" int ss3d_set_variant(int kind, int precision, int logn, int variant) {
-  // 4-7: FP32 two-line column tiles; 8: FP32 streamed middle pass
-  const int vmax = precision != SS3D_FP32 ? 3 : kind == 0 ? 8 : kind == 1 ? 7 : 3;
+  const int vmax = (precision == SS3D_FP32 && kind < 2) ? 7 : 3;   // 4-7: FP32 two-line column tiles
   if (kind < 0 || kind > 2 || (precision != SS3D_FP64 && precision != SS3D_FP32) || logn < 0 || logn > 15 ||
       variant < 0 || variant > vmax)
     return fail(SS3D_EINVAL, "invalid variant selection");

@@ -313,69 +313,6 @@ __device__ __forceinline__ void col_body_pair(const AxisArgs& a, const Geo& g, c
       });
 }
 
-// Streamed two-line column pass: a persistent CTA walks tiles t = blockIdx.x,
-// blockIdx.x + gridDim.x, ...; the columns of tile t + gridDim.x are copied
-// into the second stage buffer (cp.async, no registers) while tile t is
-// transformed in place in the first.  Tile order: column block fastest, then
-// group, then realization, so the CTAs at work cover whole rows.  Same
-// operations per element as col_body_pair.
-template <int LOGN> struct StreamCfg {
-  static constexpr int N = 1 << LOGN;
-  static constexpr int ET = N < 8 ? N : 8;          // pairs per thread
-  static constexpr int TPC = N / ET;
-  static constexpr int TX0 = 4096 / N;
-  static constexpr int TX = TX0 > 64 ? 64 : (TX0 < 2 ? 2 : TX0);   // pairs of lines per tile
-  static constexpr int NTH = TX * TPC;
-  static constexpr size_t SMEM = (size_t)(N + 2 * N * TX) * sizeof(cpair);   // twiddles + two stages
-};
-
-template <int LOGN, int SIGN>
-__device__ __forceinline__ void col_stream_pair(const AxisArgs& a, const Geo& g, const float2* in, float2* out,
-                                                const Tw& tw, int ntiles, unsigned char* smraw) {
-  using SC = StreamCfg<LOGN>;
-  constexpr int N = SC::N, TX = SC::TX, TPC = SC::TPC, NTH = SC::NTH;
-  constexpr int NR0 = N / Sched<LOGN>::radix(0);
-  cpair* stw = reinterpret_cast<cpair*>(smraw);
-  cpair* stage[2] = {stw + N, stw + N + N * TX};
-  load_tw_pair<N, NTH>(stw, tw);
-  const int S = (int)a.S, S2 = S / 2;
-  const int tp = (int)threadIdx.x % TX;
-  auto issue = [&](cpair* st, int tile) {
-    const int cb = tile % a.tpg;
-    const int rest = tile / a.tpg;
-    const int grp = rest % a.ngroups, r = rest / a.ngroups;
-    const float2* src = in + (long long)grp * a.gstride + 2 * cb * TX + (long long)r * a.rstride;
-    for (int c = threadIdx.x; c < N * TX; c += NTH) {
-      const int row = c / TX, q = c % TX;
-      if (line_valid(g, 2 * (cb * TX + q), a.lines)) cp_async16(st + c, src + row * S + 2 * q);
-    }
-  };
-  int tile = blockIdx.x;
-  if (tile < ntiles) issue(stage[0], tile);
-  cp_async_commit();
-  for (int it = 0; tile < ntiles; ++it, tile += gridDim.x) {
-    cpair* cur = stage[it & 1];
-    if (tile + (int)gridDim.x < ntiles) issue(stage[(it + 1) & 1], tile + gridDim.x);
-    cp_async_commit();
-    cp_async_wait<1>();   // this thread's copies of the current tile have landed
-    __syncthreads();      // and everyone's (also: the twiddles)
-    const int cb = tile % a.tpg;
-    const int rest = tile / a.tpg;
-    const int grp = rest % a.ngroups, r = rest / a.ngroups;
-    const int line = 2 * (cb * TX + tp);
-    const bool valid = line_valid(g, line, a.lines);
-    float4* dst = reinterpret_cast<float4*>(out + (long long)grp * a.gstride + line + (long long)r * a.rstride);
-    const int nout = a.nout;
-    fft_tile<LOGN, TX, TPC, SIGN, TX, true>(
-        cur, stw, [&](int jb, int rr) { return pair_of(reinterpret_cast<const float4*>(cur)[(jb + rr * NR0) * TX + tp]); },
-        [&](int pos, cpair v) {
-          if (valid && pos < nout) dst[pos * S2] = quad_of(v);
-        });
-    __syncthreads();      // cur is refilled by the copies issued next iteration
-  }
-  cp_async_wait<0>();
-}
-
 // synthesis + first inverse pass for two lines (indices i0 = even, i1 = i0 + 1
 // of one row); the row state of a position serves both, the two amplitudes
 // are one 8-byte load.  Decisions as in colgen_body.

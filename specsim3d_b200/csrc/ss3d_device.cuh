@@ -90,19 +90,6 @@ template <int SIGN, typename C> __device__ __forceinline__ C cmul_si(C a) {
   return SIGN > 0 ? cmk<C>(kneg(a.y), a.x) : cmk<C>(a.y, kneg(a.x));
 }
 
-// ---------------------------------------------------------------- asynchronous copies
-// 16-byte global -> shared copy that bypasses the registers (cached in L2
-// only); completion per thread by commit groups, visibility to the block by a
-// barrier after the wait.  Waits are the hardware's own (no spinning).
-__device__ __forceinline__ void cp_async16(void* smem, const void* gmem) {
-  const unsigned sa = (unsigned)__cvta_generic_to_shared(smem);
-  asm volatile("cp.async.cg.shared.global [%0], [%1], 16;\n" ::"r"(sa), "l"(gmem) : "memory");
-}
-__device__ __forceinline__ void cp_async_commit() { asm volatile("cp.async.commit_group;\n" ::: "memory"); }
-template <int PENDING> __device__ __forceinline__ void cp_async_wait() {
-  asm volatile("cp.async.wait_group %0;\n" ::"n"(PENDING) : "memory");
-}
-
 // ---------------------------------------------------------------- Park-Miller
 __host__ __device__ __forceinline__ uint32_t pm_mulmod(uint32_t a, uint32_t b) {
   // a, b < 2^31: p = a b < 2^62 = hi 2^32 + lo;  p mod (2^31 - 1) = (p & m) + (p >> 31) folded once

@@ -13,12 +13,30 @@
 // w^(k*r), k = jb mod Ns, w = e^{SIGN 2 pi i/(Ns*R)}, applies the radix-R DFT
 // and writes positions (jb/Ns)*Ns*R + k + r*Ns.  After the last pass the data
 // are in natural order.
+//
+// Exchange layout: position p of column t sits at s[sw(p) * PITCH + t] with
+// sw(p) = p ^ ((p >> 3) & SWM), a permutation inside each block of 8
+// positions.  When a shared-memory row (PITCH elements) is narrower than the
+// 128 bytes of the banks, the radix-8 stores of pass 0 (positions 8 jb + r,
+// lanes differing in jb) would otherwise all fall into the same part of each
+// bank row; the XOR spreads them over the whole row.  Reads, whose lanes take
+// consecutive positions, keep touching the same addresses in another order.
 #pragma once
 #include "ss3d_device.cuh"
 
 namespace ss3d {
 
-template <int LOGN, int TX, int TPC, int SIGN, int P, int PITCH, bool STORE_SYNC, typename C, class Store>
+template <int SWM> __device__ __forceinline__ int sw(int p) { return SWM ? p ^ ((p >> 3) & SWM) : p; }
+
+// SWM of a row of PITCH elements of EB bytes: 128 / row - 1 for a row of a
+// power-of-two size below 128 bytes, else 0
+template <int PITCH, int EB> struct Swizzle {
+  static constexpr int row = PITCH * EB;
+  static constexpr bool pow2 = (row & (row - 1)) == 0;
+  static constexpr int M = (pow2 && row < 128) ? (128 / row > 8 ? 7 : 128 / row - 1) : 0;
+};
+
+template <int LOGN, int TX, int TPC, int SIGN, int P, int PITCH, bool STORE_SYNC, int SWM, typename C, class Store>
 __device__ __forceinline__ void fft_tile_rest(C* __restrict__ s, const C* __restrict__ tw, C* v, int t, int c,
                                               Store&& store) {
   constexpr int N = 1 << LOGN;
@@ -32,7 +50,7 @@ __device__ __forceinline__ void fft_tile_rest(C* __restrict__ s, const C* __rest
     for (int m = 0; m < NBT; ++m) {
       const int jb = c + TPC * m;
 #pragma unroll
-      for (int r = 0; r < R; ++r) v[m * R + r] = s[(jb + r * (N / R)) * PITCH + t];
+      for (int r = 0; r < R; ++r) v[m * R + r] = s[sw<SWM>(jb + r * (N / R)) * PITCH + t];
     }
 #pragma unroll
     for (int m = 0; m < NBT; ++m) {
@@ -60,10 +78,10 @@ __device__ __forceinline__ void fft_tile_rest(C* __restrict__ s, const C* __rest
         const int k = jb % NS;
         const int idxD = (jb / NS) * NS * R + k;
 #pragma unroll
-        for (int r = 0; r < R; ++r) s[(idxD + r * NS) * PITCH + t] = v[m * R + r];
+        for (int r = 0; r < R; ++r) s[sw<SWM>(idxD + r * NS) * PITCH + t] = v[m * R + r];
       }
       __syncthreads();
-      fft_tile_rest<LOGN, TX, TPC, SIGN, P + 1, PITCH, STORE_SYNC>(s, tw, v, t, c, store);
+      fft_tile_rest<LOGN, TX, TPC, SIGN, P + 1, PITCH, STORE_SYNC, SWM>(s, tw, v, t, c, store);
     }
   }
 }
@@ -82,6 +100,7 @@ __device__ __forceinline__ void fft_tile(C* __restrict__ s, const C* __restrict_
   constexpr int N = 1 << LOGN;
   constexpr int ET = N / TPC;
   constexpr int NP = Sched<LOGN>::npass;
+  constexpr int SWM = Swizzle<PITCH, (int)sizeof(C)>::M;
   static_assert(ET % 8 == 0 || N < 8, "each thread must own whole radix-8 butterflies");
   const int t = threadIdx.x % TX;
   const int c = threadIdx.x / TX;
@@ -113,13 +132,13 @@ __device__ __forceinline__ void fft_tile(C* __restrict__ s, const C* __restrict_
       for (int m = 0; m < NBT; ++m) {
         const int jb = c + TPC * m;
 #pragma unroll
-        for (int r = 0; r < R; ++r) s[(jb * R + r) * PITCH + t] = v[m * R + r];
+        for (int r = 0; r < R; ++r) s[sw<SWM>(jb * R + r) * PITCH + t] = v[m * R + r];
       }
       __syncthreads();
     }
   }
   // ---- passes 1 .. NP-1
-  fft_tile_rest<LOGN, TX, TPC, SIGN, 1, PITCH, STORE_SYNC>(s, tw, v, t, c, store);
+  fft_tile_rest<LOGN, TX, TPC, SIGN, 1, PITCH, STORE_SYNC, SWM>(s, tw, v, t, c, store);
 }
 
 }  // namespace ss3d

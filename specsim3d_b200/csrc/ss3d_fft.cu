@@ -71,10 +71,13 @@ template <typename R, int LOGN, int V> struct AxisCfg<R, LOGN, V, true> : PairCf
 };
 
 // c2c transform along a strided axis (in place allowed), unscaled, pruned store.
-// The one-line FP32 tiles are held to 64 registers (two 512-thread CTAs per SM).
+// FP32 tiles of lengths up to 512 with 8 elements (or pairs) per thread are
+// held to 64 registers (two 512-thread CTAs per SM).
 template <typename R, int LOGN, int V>
 constexpr int col_min_blocks() {
-  return (sizeof(R) == 4 && V < 4 && AxisCfg<R, LOGN, V>::NTH <= 1024) ? 1024 / AxisCfg<R, LOGN, V>::NTH : 1;
+  return (sizeof(R) == 4 && LOGN <= 9 && (V < 4 || (V & 1) == 0) && AxisCfg<R, LOGN, V>::NTH <= 1024)
+             ? 1024 / AxisCfg<R, LOGN, V>::NTH
+             : 1;
 }
 template <typename R, int LOGN, int SIGN, int V>
 __global__ void __launch_bounds__(AxisCfg<R, LOGN, V>::NTH, (col_min_blocks<R, LOGN, V>()))
@@ -85,14 +88,6 @@ __global__ void __launch_bounds__(AxisCfg<R, LOGN, V>::NTH, (col_min_blocks<R, L
     col_body_pair<LOGN, CF::TX, CF::TPC, SIGN>(a, g, in, out, tw, blockIdx.x, smraw);
   else
     col_body<R, LOGN, CF::TX, CF::TPC, SIGN>(a, g, in, out, tw, blockIdx.x, smraw);
-}
-
-// streamed two-line column pass (variant 8 of the FP32 middle pass)
-template <int LOGN, int SIGN>
-__global__ void __launch_bounds__(StreamCfg<LOGN>::NTH) k_col_stream(AxisArgs a, Geo g, const float2* in,
-                                                                     float2* out, Tw tw, int ntiles) {
-  extern __shared__ __align__(16) unsigned char smraw[];
-  col_stream_pair<LOGN, SIGN>(a, g, in, out, tw, ntiles, smraw);
 }
 
 // first inverse pass with the coefficient synthesis fused into the loader
@@ -423,36 +418,6 @@ static cudaError_t run_axis_c2c_v(const AxisArgs& a, const Geo& g, const cpx_t<R
   }
 }
 
-static int device_sms() {
-  static int sms[64] = {};
-  int dev = 0;
-  if (cudaGetDevice(&dev) != cudaSuccess || dev < 0 || dev >= 64) return 148;
-  if (!sms[dev]) {
-    int v = 0;
-    if (cudaDeviceGetAttribute(&v, cudaDevAttrMultiProcessorCount, dev) != cudaSuccess || v <= 0) v = 148;
-    sms[dev] = v;
-  }
-  return sms[dev];
-}
-
-template <int L, int SIGN>
-static cudaError_t run_axis_stream(const AxisArgs& a, const Geo& g, const float2* in, float2* out, Tw tw,
-                                   cudaStream_t st) {
-  using SC = StreamCfg<L>;
-  cudaError_t e = set_smem(k_col_stream<L, SIGN>, SC::SMEM);
-  if (e != cudaSuccess) return e;
-  AxisArgs b = a;
-  b.tpg = (a.lines + 2 * SC::TX - 1) / (2 * SC::TX);
-  const long long ntiles = (long long)b.tpg * a.ngroups * a.nreal;
-  if (ntiles <= 0) return cudaSuccess;
-  if (ntiles >= (1ll << 31)) return cudaErrorInvalidValue;
-  const int per_sm = SC::SMEM * 2 <= 227 * 1024 ? 2 : 1;
-  const unsigned blocks = (unsigned)std::min<long long>(ntiles, (long long)device_sms() * per_sm);
-  k_col_stream<L, SIGN><<<blocks, SC::NTH, SC::SMEM, st>>>(b, g, in, out, tw, (int)ntiles);
-  ++g_launch_count;
-  return cudaGetLastError();
-}
-
 template <typename R, int L, int V>
 static cudaError_t run_axis_gen_v(const AxisArgs& a, const Geo& g, const R* amp, const uint32_t* rs,
                                   const uint32_t* apow, cpx_t<R>* out, Tw tw, cudaStream_t st) {
@@ -505,7 +470,6 @@ static cudaError_t run_axis_c2c(const AxisArgs& a, const Geo& g, const cpx_t<R>*
     }
     if constexpr (sizeof(R) == 4) {
       switch (g_variant[0][1][L]) {
-        case 8: return run_axis_stream<L, SIGN>(a, g, in, out, tw, st);
         case 4: return run_axis_c2c_v<R, L, SIGN, 4>(a, g, in, out, tw, st);
         case 5: return run_axis_c2c_v<R, L, SIGN, 5>(a, g, in, out, tw, st);
         case 6: return run_axis_c2c_v<R, L, SIGN, 6>(a, g, in, out, tw, st);
