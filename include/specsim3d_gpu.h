@@ -202,6 +202,13 @@ int ss3d_batch_time(ss3d_batch *b, float ms[4]);
  * CTAs per SM (0: occupancy limit). */
 int ss3d_batch_schedule(const ss3d_batch *b, int *sched, int etv[3], int mode[3], int cps[3]);
 int ss3d_batch_set_schedule(ss3d_batch *b, int sched, int pass, int etv, int mode, int cps);
+/* Chains schedule: each job's realizations run as `split` consecutive
+ * sub-chains on separate branches, sub-chain q starting when the synthesis of
+ * sub-chain q-1 has ended, so that syntheses overlap the middle and row passes
+ * of earlier sub-chains (1: one chain per job; chosen by ss3d_batch_autotune).
+ * Results do not depend on it. */
+int ss3d_batch_split(const ss3d_batch *b, int *split);
+int ss3d_batch_set_split(ss3d_batch *b, int split);
 void ss3d_batch_free(ss3d_batch *b);
 
 /* ---------------------------------------------------------------- variogram */

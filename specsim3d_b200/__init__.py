@@ -254,13 +254,19 @@ class Batch:
         sched = ctypes.c_int()
         etv, mode, cps = ((ctypes.c_int * 3)() for _ in range(3))
         L.check(L.lib().ss3d_batch_schedule(self._h, ctypes.byref(sched), etv, mode, cps))
+        split = ctypes.c_int()
+        L.check(L.lib().ss3d_batch_split(self._h, ctypes.byref(split)))
         return {"schedule": "persistent" if sched.value == 1 else "chains",
                 "elements_per_thread": [16 if v == 0 else 8 for v in etv], "mode": list(mode),
-                "ctas_per_sm": list(cps)}
+                "ctas_per_sm": list(cps), "split": int(split.value)}
 
     def set_schedule(self, sched, pass_=0, elements_per_thread=8, mode=2, ctas_per_sm=0):
         L.check(L.lib().ss3d_batch_set_schedule(self._h, int(sched), int(pass_),
                                                 0 if elements_per_thread == 16 else 1, int(mode), int(ctas_per_sm)))
+
+    def set_split(self, split):
+        """Chains schedule: run each job's realizations as `split` staggered sub-chains."""
+        L.check(L.lib().ss3d_batch_set_split(self._h, int(split)))
 
     def close(self):
         if self._h:

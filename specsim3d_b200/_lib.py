@@ -26,7 +26,7 @@ EXPORTS = (
     "ss3d_set_stream", "ss3d_last_error", "ss3d_version", "ss3d_profile", "ss3d_profile_read", "ss3d_autotune", "ss3d_set_variant",
     "ss3d_realize_workspace_bytes", "ss3d_release_workspace", "ss3d_trim_pool",
     "ss3d_batch_create", "ss3d_batch_run", "ss3d_batch_autotune", "ss3d_batch_info", "ss3d_batch_time",
-    "ss3d_batch_schedule", "ss3d_batch_set_schedule", "ss3d_batch_free",
+    "ss3d_batch_schedule", "ss3d_batch_set_schedule", "ss3d_batch_split", "ss3d_batch_set_split", "ss3d_batch_free",
     "ss3d_server_create", "ss3d_server_submit", "ss3d_server_wait", "ss3d_server_stats", "ss3d_server_clock",
     "ss3d_server_free",
 )
@@ -150,6 +150,8 @@ def lib():
         "ss3d_batch_time": (I, [P, P]),
         "ss3d_batch_schedule": (I, [P, P, P, P, P]),
         "ss3d_batch_set_schedule": (I, [P, I, I, I, I, I]),
+        "ss3d_batch_split": (I, [P, P]),
+        "ss3d_batch_set_split": (I, [P, I]),
         "ss3d_batch_free": (None, [P]),
         "ss3d_server_create": (I, [P, P]),
         "ss3d_server_submit": (I, [P, P, P]),

@@ -186,6 +186,10 @@ struct ss3d_batch {
   std::vector<cudaStream_t> branch;
   std::vector<cudaEvent_t> joins;
   cudaEvent_t fork = nullptr;
+  // chains: realizations of a job split into this many consecutive sub-chains,
+  // each starting its synthesis when the previous one's synthesis has ended
+  int split = 1;
+  std::vector<cudaEvent_t> stag;   // synthesis-done events of the sub-chains
   // persistent: per pass
   int etv[3] = {0, 0, 0};    // tile variant
   int mode[3] = {0, 0, 0};   // 0 strided items, 1 contiguous items, 2 one CTA per item
@@ -290,9 +294,14 @@ cudaError_t enqueue_persistent(ss3d_batch* b, cudaStream_t st, cudaEvent_t* ev) 
   return e;
 }
 
-// Chains schedule: job j on branch stream j mod B, forked from and joined
-// back into st.  The per-call launchers pick their tile from g_variant, set to
-// the batch's choice for the duration of the enqueue.
+// Chains schedule: sub-chain c (realizations r0..r1 of one job: row states,
+// synthesis, middle and row passes) on branch stream c mod B, forked from and
+// joined back into st.  With split S a job's realizations form S consecutive
+// sub-chains, and sub-chain q starts only when the synthesis of sub-chain q-1
+// has ended: the syntheses, bound by instruction issue, then run one after
+// the other while the memory-bound middle and row passes of the earlier
+// sub-chains run beside them.  The per-call launchers pick their tile from
+// g_variant, set to the batch's choice for the duration of the enqueue.
 cudaError_t enqueue_chains(ss3d_batch* b, cudaStream_t st) {
   int saved[3][16];
   for (int k = 0; k < 3; k++)
@@ -301,16 +310,38 @@ cudaError_t enqueue_chains(ss3d_batch* b, cudaStream_t st) {
       g_variant[k][1][L] = b->var[k][L];
     }
   const int nb = (int)b->branch.size();
-  cudaError_t e = cudaEventRecord(b->fork, st);
+  cudaError_t e = cudaSuccess;
+  size_t nstag = 0;
+  for (const BJob& J : b->jobs) nstag += (size_t)std::max(0, std::min(b->split, J.nreal) - 1);
+  while (b->stag.size() < nstag && e == cudaSuccess) {
+    cudaEvent_t ev = nullptr;
+    e = cudaEventCreateWithFlags(&ev, cudaEventDisableTiming);
+    if (e == cudaSuccess) b->stag.push_back(ev);
+  }
+  if (e == cudaSuccess) e = cudaEventRecord(b->fork, st);
   for (int q = 0; q < nb && e == cudaSuccess; q++) e = cudaStreamWaitEvent(b->branch[q], b->fork, 0);
+  int chain = 0;
+  size_t ist = 0;
   for (size_t j = 0; j < b->jobs.size() && e == cudaSuccess; j++) {
     const BJob& J = b->jobs[j];
-    cudaStream_t s = b->branch[j % nb];
-    e = launch_rowstates(J.g, b->s0[j], b->r_first[j], J.nreal, b->ptab, const_cast<uint32_t*>(J.rs),
-                         const_cast<uint32_t*>(J.apow), s);
-    if (e == cudaSuccess)
-      e = launch_realize<float>(J.g, J.amp, J.rs, J.apow, J.work, J.wstride, J.nreal, J.out, 0, nullptr, nullptr,
-                                b->tw, true, s);
+    const int S = std::min(b->split, J.nreal);
+    const long long rows = (long long)J.g.npy * J.g.npz, M = (long long)J.g.nx * J.g.ny * J.g.nz;
+    cudaEvent_t prev = nullptr;
+    for (int q = 0; q < S && e == cudaSuccess; q++, chain++) {
+      const int r0 = (int)((long long)J.nreal * q / S), r1 = (int)((long long)J.nreal * (q + 1) / S);
+      cudaStream_t s = b->branch[chain % nb];
+      cudaEvent_t done = q + 1 < S ? b->stag[ist++] : nullptr;
+      if (prev) e = cudaStreamWaitEvent(s, prev, 0);
+      // the column offsets a^(d i) are written once, by the first sub-chain
+      if (e == cudaSuccess)
+        e = launch_rowstates(J.g, b->s0[j], b->r_first[j] + r0, r1 - r0, b->ptab,
+                             const_cast<uint32_t*>(J.rs) + r0 * rows, q == 0 ? const_cast<uint32_t*>(J.apow) : nullptr,
+                             s);
+      if (e == cudaSuccess)
+        e = launch_realize<float>(J.g, J.amp, J.rs + r0 * rows, J.apow, J.work + r0 * J.wstride, J.wstride, r1 - r0,
+                                  J.out + r0 * M, 0, nullptr, nullptr, b->tw, true, s, nullptr, done);
+      prev = done;
+    }
   }
   for (int q = 0; q < nb && e == cudaSuccess; q++) {
     e = cudaEventRecord(b->joins[q], b->branch[q]);
@@ -401,6 +432,7 @@ extern "C" void ss3d_batch_free(ss3d_batch* b) {
   if (b->graph) cudaGraphDestroy(b->graph);
   for (cudaStream_t s : b->branch) cudaStreamDestroy(s);
   for (cudaEvent_t ev : b->joins) cudaEventDestroy(ev);
+  for (cudaEvent_t ev : b->stag) cudaEventDestroy(ev);
   if (b->fork) cudaEventDestroy(b->fork);
   for (void* p : b->bufs) cudaFree(p);
   if (b->djobs) cudaFree(b->djobs);
@@ -499,7 +531,9 @@ extern "C" int ss3d_batch_create(const ss3d_batch_job* jobs, int njobs, ss3d_bat
     b->r_first.push_back(q.r_first);
     b->cells += (long long)g.nx * g.ny * g.nz * q.nreal;
   }
-  const int nbranch = std::min(njobs, 16);
+  long long nchains = 0;
+  for (const BJob& J : b->jobs) nchains += J.nreal;
+  const int nbranch = (int)std::min<long long>(nchains, 16);
   if (e == cudaSuccess) e = cudaEventCreateWithFlags(&b->fork, cudaEventDisableTiming);
   for (int q = 0; q < nbranch && e == cudaSuccess; q++) {
     cudaStream_t s = nullptr;
@@ -562,6 +596,18 @@ extern "C" int ss3d_batch_schedule(const ss3d_batch* b, int* sched, int etv[3], 
   return SS3D_OK;
 }
 
+extern "C" int ss3d_batch_split(const ss3d_batch* b, int* split) {
+  if (!b || !split) return set_error(SS3D_EINVAL, "NULL argument");
+  *split = b->split;
+  return SS3D_OK;
+}
+
+extern "C" int ss3d_batch_set_split(ss3d_batch* b, int split) {
+  if (!b || split < 1) return set_error(SS3D_EINVAL, "invalid batch split");
+  b->split = split;
+  return capture(b);
+}
+
 extern "C" int ss3d_batch_set_schedule(ss3d_batch* b, int sched, int pass, int etv, int mode, int cps) {
   if (!b || sched < 0 || sched > 1 || pass < 0 || pass > 2 || etv < 0 || etv >= NETV || mode < 0 || mode > 2 ||
       cps < 0)
@@ -618,6 +664,22 @@ extern "C" int ss3d_batch_autotune(ss3d_batch* b) {
     for (int L = 0; L < 16; L++)
       if (used[k][L]) b->var[k][L] = bestv;
     best_chain = bestk;
+  }
+  // chains: split of each job's realizations into staggered sub-chains
+  {
+    int maxr = 1;
+    for (const BJob& J : b->jobs) maxr = std::max(maxr, J.nreal);
+    int bests = b->split;
+    for (int sp : {1, 2, 4, 8}) {
+      if (sp > maxr || e != cudaSuccess) break;
+      b->split = sp;
+      e = time_run(b, st, ms, true);
+      if (e == cudaSuccess && ms[3] < best_chain) {
+        best_chain = ms[3];
+        bests = sp;
+      }
+    }
+    b->split = bests;
   }
   // persistent
   float best_pers = 1e30f;

@@ -624,10 +624,12 @@ cudaError_t launch_gen(const Geo& g, const R* amp, const uint32_t* rowstates, co
 template <typename R>
 cudaError_t launch_realize(const Geo& g, const R* amp, const uint32_t* rowstates, const uint32_t* apow,
                            cpx_t<R>* work, long long wstride, int nreal, void* out, int out_kind, double* part,
-                           int* nblk_per_r, Tw tw, bool fused, cudaStream_t st, Marks* marks) {
+                           int* nblk_per_r, Tw tw, bool fused, cudaStream_t st, Marks* marks,
+                           cudaEvent_t first_done) {
   constexpr int ML = MaxL<R>::v;
   cudaError_t e = cudaSuccess;
   mark(marks, 1, st);
+  auto first_pass_done = [&]() { return first_done ? cudaEventRecord(first_done, st) : cudaSuccess; };
   // first inverse axis: z if present, else y, else only x
   if (g.npz > 1) {
     AxisArgs a{};
@@ -649,6 +651,7 @@ cudaError_t launch_realize(const Geo& g, const R* amp, const uint32_t* rowstates
       e = cudaErrorInvalidValue;
       SS3D_LOGN_SWITCH(L, ML, e = (run_axis_c2c<R, L, +1>(a, g, work, work, tw, st)));
     }
+    if (e == cudaSuccess) e = first_pass_done();
     if (e != cudaSuccess) return e;
     if (g.npy > 1) {
       mark(marks, 2, st);
@@ -686,9 +689,11 @@ cudaError_t launch_realize(const Geo& g, const R* amp, const uint32_t* rowstates
       e = cudaErrorInvalidValue;
       SS3D_LOGN_SWITCH(Ly, ML, e = (run_axis_c2c<R, L, +1>(b, g, work, work, tw, st)));
     }
+    if (e == cudaSuccess) e = first_pass_done();
     if (e != cudaSuccess) return e;
   } else {
     e = launch_gen<R>(g, amp, rowstates, apow, work, wstride, nreal, st);
+    if (e == cudaSuccess) e = first_pass_done();
     if (e != cudaSuccess) return e;
   }
   // x pass
@@ -736,10 +741,10 @@ cudaError_t launch_reduce_zstats(const double* part, int nblk_per_r, int nreal, 
 
 template cudaError_t launch_realize<float>(const Geo&, const float*, const uint32_t*, const uint32_t*, float2*,
                                            long long, int, void*, int, double*, int*, Tw, bool, cudaStream_t,
-                                           Marks*);
+                                           Marks*, cudaEvent_t);
 template cudaError_t launch_realize<double>(const Geo&, const double*, const uint32_t*, const uint32_t*, double2*,
                                             long long, int, void*, int, double*, int*, Tw, bool, cudaStream_t,
-                                            Marks*);
+                                            Marks*, cudaEvent_t);
 template cudaError_t launch_gen<float>(const Geo&, const float*, const uint32_t*, const uint32_t*, float2*,
                                        long long, int, cudaStream_t);
 template cudaError_t launch_gen<double>(const Geo&, const double*, const uint32_t*, const uint32_t*, double2*,

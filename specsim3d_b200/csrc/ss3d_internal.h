@@ -81,12 +81,13 @@ cudaError_t launch_spectrum(const Model& m, const double d[3], const Geo& g, dou
                             cudaStream_t st);
 cudaError_t launch_rowstates(const Geo& g, uint32_t s0, long long r_first, int nreal, const uint32_t* ptab,
                              uint32_t* rowstates, uint32_t* apow, cudaStream_t st);
-// out_kind: 0 float output, 1 double output
+// out_kind: 0 float output, 1 double output; first_done (may be NULL) is
+// recorded on st once the first pass (synthesis) has been enqueued
 template <typename R>
 cudaError_t launch_realize(const Geo& g, const R* amp, const uint32_t* rowstates, const uint32_t* apow,
                            cpx_t<R>* work, long long wstride, int nreal, void* out, int out_kind,
                            double* part, int* nblk_per_r, Tw tw, bool fused, cudaStream_t st,
-                           Marks* marks = nullptr);
+                           Marks* marks = nullptr, cudaEvent_t first_done = nullptr);
 template <typename R>
 cudaError_t launch_gen(const Geo& g, const R* amp, const uint32_t* rowstates, const uint32_t* apow,
                        cpx_t<R>* work, long long wstride, int nreal, cudaStream_t st);

@@ -73,6 +73,22 @@ def test_batch_equals_per_call(gpu, sched):
     b.close()
 
 
+@pytest.mark.parametrize("split", [2, 3, 8])
+def test_batch_split_sub_chains(gpu, split):
+    """Realizations of each job split into staggered sub-chains: same bits as
+    one chain per job (and as the per-call path)."""
+    jobs = _build(gpu, _specs_small())
+    b = gpu.Batch(jobs)
+    b.set_split(split)
+    assert b.schedule()["split"] == split and b.schedule()["schedule"] == "chains"
+    b.run()
+    _check_against_per_call(gpu, jobs)
+    _clear(jobs)
+    b.run()
+    _check_against_per_call(gpu, jobs)
+    b.close()
+
+
 def test_batch_persistent_variants_identical(gpu):
     jobs = _build(gpu, _specs_small()[:5])
     b = gpu.Batch(jobs)
