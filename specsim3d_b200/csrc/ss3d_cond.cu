@@ -30,14 +30,19 @@
 
 namespace ss3d {
 
+// Leading dimension of the kriging matrices in shared memory: odd, so that the
+// lanes of a warp walking down a column (stride ld elements) hit distinct banks
+// (an even ld such as ndmax = 24 put 16 lanes on the same bank pair).
+__host__ __device__ inline int cond_ld(int ndmax) { return ndmax | 1; }
+
 // shared memory of one kriging warp.  FP64 solves (prec 0): the covariance
-// matrix, factored in place (ndmax^2 doubles), four ndmax vectors of doubles
+// matrix, factored in place (ndmax x ld doubles), four ndmax vectors of doubles
 // and the neighbour ids.  FP32 solves (prec 1): the FP64 matrix (kept for the
-// refinement residual), its FP32 factor (ndmax^2 floats), three ndmax vectors
+// refinement residual), its FP32 factor (ndmax x ld floats), three ndmax vectors
 // of doubles, four of floats and the ids.  Rounded up to 16 bytes.
 __host__ __device__ inline size_t cond_warp_bytes(int ndmax, int prec) {
-  const size_t n = (size_t)ndmax;
-  const size_t b = prec == 0 ? n * n * 8 + n * 32 + n * 4 : n * n * 12 + n * 24 + n * 16 + n * 4;
+  const size_t n = (size_t)ndmax, m = n * (size_t)cond_ld(ndmax);
+  const size_t b = prec == 0 ? m * 8 + n * 32 + n * 4 : m * 12 + n * 24 + n * 16 + n * 4;
   return (b + 15) & ~(size_t)15;
 }
 
@@ -209,14 +214,14 @@ __global__ void k_cond_krige(CondGeo G, Model mdl, long long node0, int count, c
   const int lane = threadIdx.x & 31, wib = threadIdx.x >> 5;
   const int nwb = blockDim.x >> 5;
   const int ndmax = G.ndmax;
-  const int ld = ndmax;
+  const int ld = cond_ld(ndmax);
   uint8_t* tri = smc;
   fill_tri(tri, ndmax);
   if (threadIdx.x < 4) bcount[threadIdx.x] = 0;
   __syncthreads();
   const size_t per = cond_warp_bytes(ndmax, PREC);
   unsigned char* mine = smc + cond_tri_bytes(ndmax) + per * wib;
-  const int n2 = ndmax * ndmax;
+  const int n2 = ndmax * ld;
   double* A = (double*)mine;     // covariance matrix (PREC 0: factored in place)
   double* b = A + n2;
   double* w = b + ndmax;
