@@ -94,7 +94,7 @@ template <typename R, int GAUSS>
 __device__ __forceinline__ cpx_t<R> coef_from_state(uint32_t s1, R am, bool self, bool conj) {
   using C = cpx_t<R>;
   if constexpr (GAUSS) {
-    const uint32_t s2 = pm_mulmod(s1, PM_A);
+    const uint32_t s2 = sizeof(R) == 4 ? pm_mulmod_lazy(s1, PM_A) : pm_mulmod(s1, PM_A);
     if constexpr (sizeof(R) == 4) {
       const float L = m2log_f(s1);
       const float rr = L * rsqrt_hw(L);
@@ -143,10 +143,9 @@ __device__ __forceinline__ float2 m2log_f2(uint32_t s0, uint32_t s1) {
   return make_float2(s0 >= 1610612736u ? near1.x : far.x, s1 >= 1610612736u ? near1.y : far.y);
 }
 __device__ __forceinline__ void phasor_f2(uint32_t s0, uint32_t s1, float2& c, float2& sn) {
-  const float2 q = kmul(make_float2((float)s0, (float)s1), kconst<float2>(2.0f / 2147483647.0f));
-  const int n0 = __float2int_rn(q.x), n1 = __float2int_rn(q.y);
-  const int rem0 = (int)(2u * s0 - (uint32_t)n0 * PM_M), rem1 = (int)(2u * s1 - (uint32_t)n1 * PM_M);
-  const float2 x = kmul(make_float2((float)rem0, (float)rem1), kconst<float2>(1.4629181e-9f));
+  const int n0 = half_turns(s0), n1 = half_turns(s1);
+  const float2 x = kmul(make_float2((float)half_turn_rem(s0, n0), (float)half_turn_rem(s1, n1)),
+                        kconst<float2>(1.4629181e-9f));
   const float sp0 = sin_hw(x.x), cp0 = cos_hw(x.x), sp1 = sin_hw(x.y), cp1 = cos_hw(x.y);
   c = make_float2((n0 & 1) ? -cp0 : cp0, (n1 & 1) ? -cp1 : cp1);
   sn = make_float2((n0 & 1) ? -sp0 : sp0, (n1 & 1) ? -sp1 : sp1);
@@ -157,7 +156,7 @@ __device__ __forceinline__ cpair coef_pair(uint32_t s0, uint32_t s1, float2 am, 
     const float2 L = m2log_f2(s0, s1);
     const float2 rr = kmul(L, make_float2(rsqrt_hw(L.x), rsqrt_hw(L.y)));
     float2 cs, sn;
-    phasor_f2(pm_mulmod(s0, PM_A), pm_mulmod(s1, PM_A), cs, sn);
+    phasor_f2(pm_mulmod_lazy(s0, PM_A), pm_mulmod_lazy(s1, PM_A), cs, sn);
     const float2 ah = kmul(am, kconst<float2>(0.70710678118654752f));
     const float2 a = make_float2(self0 ? am.x : ah.x, self1 ? am.y : ah.y);
     const float2 re = kmul(a, kmul(rr, cs));

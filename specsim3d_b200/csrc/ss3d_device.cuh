@@ -103,6 +103,19 @@ __host__ __device__ __forceinline__ uint32_t pm_mulmod(uint32_t a, uint32_t b) {
   return r >= PM_M ? r - PM_M : r;
 }
 
+// the same product without the final conditional subtraction: a value in
+// [0, 2m) congruent to a b (mod m), for consumers that accept either
+// representative (the FP32 phase reduction below)
+__host__ __device__ __forceinline__ uint32_t pm_mulmod_lazy(uint32_t a, uint32_t b) {
+#ifdef __CUDA_ARCH__
+  const uint32_t lo = a * b, hi = __umulhi(a, b);
+#else
+  const uint64_t p = (uint64_t)a * (uint64_t)b;
+  const uint32_t lo = (uint32_t)p, hi = (uint32_t)(p >> 32);
+#endif
+  return (lo & PM_M) + ((hi << 1) | (lo >> 31));
+}
+
 // 16807^e mod (2^31-1) from the three 11-bit power tables
 // tab[l*2048 + v] = 16807^(v * 2048^l) mod m, e < 2^31 (reduced mod m-1).
 __device__ __forceinline__ uint32_t pm_pow(const uint32_t* __restrict__ tab, uint64_t e) {
@@ -174,19 +187,26 @@ __device__ __forceinline__ float lg2_hw(float x) { float r; asm("lg2.approx.ftz.
 __device__ __forceinline__ float rsqrt_hw(float x) { float r; asm("rsqrt.approx.ftz.f32 %0, %1;" : "=f"(r) : "f"(x)); return r; }
 __device__ __forceinline__ float rcp_hw(float x) { float r; asm("rcp.approx.ftz.f32 %0, %1;" : "=f"(r) : "f"(x)); return r; }
 
-// Unit phasor e^{2 pi i s/m} in float.  The nearest half turn n (0, 1 or 2)
-// is taken in integers (exact); the remainder |x| <= pi/2 (argument error
-// about 1e-7: one float rounding of the exact integer remainder) goes through
-// the hardware sine and cosine (absolute error about 2^-21), and odd half
-// turns negate both.  Half of the phases use the hardware values with each
-// sign, so their small systematic error averages out over a spectrum instead
-// of adding up coherently: a reduction to [-pi, pi] without the alternating
-// sign left a bias that summed to 4e-5 sqrt(C0) at the cell where every phase
-// is 1 (the origin) on a 512^3 spectrum.
+// Unit phasor e^{2 pi i s/m} in float, for any s < 2m congruent to the state
+// (mod m).  The nearest half turn n of 2s/m is taken in integers from
+// s / 2^30 (which differs from 2s/m by less than 2^-29 relative, so n is the
+// nearest half turn or, at a boundary, its neighbour), and the remainder
+// 2s - n m is exact in 32-bit modular arithmetic; |x| <= pi/2 + 1e-8 (argument
+// error about 1e-7: one float rounding of the exact integer remainder) goes
+// through the hardware sine and cosine (absolute error about 2^-21), and odd
+// half turns negate both (s and s - m give half turns of the same parity).
+// Half of the phases use the hardware values with each sign, so their small
+// systematic error averages out over a spectrum instead of adding up
+// coherently: a reduction to [-pi, pi] without the alternating sign left a
+// bias that summed to 4e-5 sqrt(C0) at the cell where every phase is 1 (the
+// origin) on a 512^3 spectrum.
+__device__ __forceinline__ int half_turns(uint32_t s) { return (int)((s >> 30) + ((s >> 29) & 1u)); }
+__device__ __forceinline__ int half_turn_rem(uint32_t s, int n) {
+  return (int)(2u * s - ((uint32_t)n << 31) + (uint32_t)n);   // 2s - n (2^31 - 1)  (mod 2^32)
+}
 __device__ __forceinline__ void phasor_f(uint32_t s, float& c, float& sn) {
-  const int n = __float2int_rn((float)s * (2.0f / 2147483647.0f));   // nearest half turn (off by one at most)
-  const int rem = (int)(2u * s - (uint32_t)n * PM_M);                // exact 2s - n m, |.| <= m/2 + 2^10
-  const float x = (float)rem * 1.4629181e-9f;                          // pi / (2^31-1)
+  const int n = half_turns(s);
+  const float x = (float)half_turn_rem(s, n) * 1.4629181e-9f;   // pi / (2^31-1)
   const float sp = sin_hw(x), cp = cos_hw(x);
   c = (n & 1) ? -cp : cp;
   sn = (n & 1) ? -sp : sp;
@@ -251,7 +271,7 @@ __device__ __forceinline__ cpx_t<R> coefficient(const Geo& g, int i, int j, int 
   bool conj, self;
   uint32_t s1 = first_state(g, i, j, k, rs, apow, conj, self);
   if (g.d == 2) {
-    uint32_t s2 = pm_mulmod(s1, PM_A);
+    const uint32_t s2 = sizeof(R) == 4 ? pm_mulmod_lazy(s1, PM_A) : pm_mulmod(s1, PM_A);
     if constexpr (sizeof(R) == 4) {
       const float L = m2log_f(s1);
       float rr = L * rsqrt_hw(L);
@@ -296,7 +316,7 @@ __device__ __forceinline__ cpx_t<R> coef_col(const Geo& g, int j, int k, R amp, 
   const uint32_t s1 = pm_mulmod(__ldg(rs + row), greater ? aip : ai);
   const bool self = !less && !greater && iedge;
   if (g.d == 2) {
-    const uint32_t s2 = pm_mulmod(s1, PM_A);
+    const uint32_t s2 = sizeof(R) == 4 ? pm_mulmod_lazy(s1, PM_A) : pm_mulmod(s1, PM_A);
     if constexpr (sizeof(R) == 4) {
       const float L = m2log_f(s1);
       const float rr = L * rsqrt_hw(L);
