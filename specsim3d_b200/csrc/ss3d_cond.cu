@@ -58,6 +58,54 @@ struct CondGeo {
 
 __device__ __forceinline__ int clampi(int v, int lo, int hi) { return v < lo ? lo : (v > hi ? hi : v); }
 
+// The covariance model of the kriging systems (f90:153-178) with each
+// structure's rotation divided by its range, so that h / a takes no division
+// per evaluation; the same value as covariance() up to the rounding of the
+// scaled rotation.
+struct KModel {
+  int nst;
+  double nugget;
+  int itype[MAXST];
+  double sill[MAXST];
+  double rots[MAXST][9];
+};
+__device__ __forceinline__ double cov_k(const KModel& m, double dx, double dy, double dz) {
+  double c = (dx == 0.0 && dy == 0.0 && dz == 0.0) ? m.nugget : 0.0;
+  for (int i = 0; i < m.nst; i++) {
+    const double* r = m.rots[i];
+    const double rx = r[0] * dx + r[1] * dy + r[2] * dz;
+    const double ry = r[3] * dx + r[4] * dy + r[5] * dz;
+    const double rz = r[6] * dx + r[7] * dy + r[8] * dz;
+    const double hr = sqrt(rx * rx + ry * ry + rz * rz);
+    if (m.itype[i] == 1) {
+      if (hr < 1.0) c = c + m.sill[i] * (1.0 - 1.5 * hr + 0.5 * (hr * hr * hr));
+    } else if (m.itype[i] == 2) {
+      c = c + m.sill[i] * exp(-3.0 * hr);
+    } else {
+      c = c + m.sill[i] * exp(-(3.0 * hr * hr));
+    }
+  }
+  return c;
+}
+
+// 1/sqrt(x) for a positive normal x: the hardware approximation (PTX
+// rsqrt.approx) refined by Newton's iteration r <- r + r (1 - x r^2) / 2,
+// twice in FP64 (about 2^-23 -> 2^-46 -> full precision) and once in FP32.
+__device__ __forceinline__ double rsqrt_nr(double x) {
+  double r;
+  asm("rsqrt.approx.ftz.f64 %0, %1;" : "=d"(r) : "d"(x));
+  double e = fma(-x * r, r, 1.0);
+  r = fma(0.5 * r, e, r);
+  e = fma(-x * r, r, 1.0);
+  return fma(0.5 * r, e, r);
+}
+__device__ __forceinline__ float rsqrt_nr(float x) {
+  float r;
+  asm("rsqrt.approx.ftz.f32 %0, %1;" : "=f"(r) : "f"(x));
+  const float e = fmaf(-x * r, r, 1.0f);
+  return fmaf(0.5f * r, e, r);
+}
+
 // neighbour search of nodes [node0, node0 + count): writes nn and the
 // neighbour ids (0-based data index) and flags the exact data nodes
 __global__ void k_cond_search(CondGeo G, long long node0, int count, const double* __restrict__ dxs,
@@ -180,8 +228,8 @@ __device__ bool warp_cholesky(T* L, T* rinv, int ld, int n, T ridge, const uint8
   for (int c = 0; c < n; ++c) {
     const T piv = L[c * ld + c];
     if (!(piv > T(0))) return false;   // uniform: every lane reads the same value
-    const T dgl = sqrt(piv);
-    const T inv = T(1) / dgl;
+    const T inv = rsqrt_nr(piv);       // 1 / sqrt(pivot)
+    const T dgl = piv * inv;
     __syncwarp();
     for (int r = c + 1 + lane; r < n; r += 32) L[r * ld + c] *= inv;
     if (lane == 0) {
@@ -204,7 +252,7 @@ __device__ bool warp_cholesky(T* L, T* rinv, int ld, int n, T ridge, const uint8
 // refinement step with the residual b - A w formed in FP64.
 // Dynamic shared memory: the pair table, then one region per warp.
 template <int PREC>
-__global__ void k_cond_krige(CondGeo G, Model mdl, long long node0, int count, const int* __restrict__ nbr,
+__global__ void k_cond_krige(CondGeo G, KModel mdl, long long node0, int count, const int* __restrict__ nbr,
                              const int* __restrict__ nnb, const double* __restrict__ dxs,
                              const double* __restrict__ dys, const double* __restrict__ dzs,
                              const double* __restrict__ dg, const double* __restrict__ simd, double* __restrict__ res,
@@ -250,7 +298,9 @@ __global__ void k_cond_krige(CondGeo G, Model mdl, long long node0, int count, c
       if (lane == 0) atomicAdd_block(&bcount[3], 1ull);
       continue;
     }
-    const int i = (int)(node % G.nx), j = (int)((node / G.nx) % G.ny), k = (int)(node / ((long long)G.nx * G.ny));
+    // a conditioned grid has at most 2^27 nodes: 32-bit index arithmetic
+    const uint32_t nu = (uint32_t)node, row = nu / (uint32_t)G.nx;
+    const int i = (int)(nu - row * (uint32_t)G.nx), j = (int)(row % (uint32_t)G.ny), k = (int)(row / (uint32_t)G.ny);
     const double x = G.xmin + (double)i * G.dx, y = G.ymin + (double)j * G.dy, z = G.zmin + (double)k * G.dz;
     for (int p = lane; p < nn; p += 32) id[p] = nl[p];
     __syncwarp();
@@ -259,7 +309,7 @@ __global__ void k_cond_krige(CondGeo G, Model mdl, long long node0, int count, c
       for (int e = lane; e < ntri; e += 32) {
         const int p = tri[2 * e], qq = tri[2 * e + 1];
         const int cp = id[p], cq = id[qq];
-        const double v = covariance(mdl, dxs[cp] - dxs[cq], dys[cp] - dys[cq], dzs[cp] - dzs[cq]);
+        const double v = cov_k(mdl, dxs[cp] - dxs[cq], dys[cp] - dys[cq], dzs[cp] - dzs[cq]);
         A[p * ld + qq] = v;
         A[qq * ld + p] = v;
       }
@@ -267,7 +317,7 @@ __global__ void k_cond_krige(CondGeo G, Model mdl, long long node0, int count, c
     fill_matrix();
     for (int p = lane; p < nn; p += 32) {
       const int cp = id[p];
-      b[p] = covariance(mdl, dxs[cp] - x, dys[cp] - y, dzs[cp] - z);
+      b[p] = cov_k(mdl, dxs[cp] - x, dys[cp] - y, dzs[cp] - z);
     }
     __syncwarp();
     double ridge = 1.0e-10 * G.c0;
@@ -314,8 +364,10 @@ __global__ void k_cond_krige(CondGeo G, Model mdl, long long node0, int count, c
       continue;
     }
     if (tries > 1 && lane == 0) atomicAdd_block(&bcount[1], 1ull);
-    double zk = 0.0;
-    for (int p = 0; p < nn; ++p) zk += w[p] * dg[id[p]];
+    double zk = 0.0;   // sum of w dg over the neighbours: lanes, then a butterfly
+    for (int p = lane; p < nn; p += 32) zk += w[p] * dg[id[p]];
+#pragma unroll
+    for (int off = 16; off > 0; off >>= 1) zk += __shfl_xor_sync(0xffffffffu, zk, off);
     for (int l = lane; l < G.nreal; l += 32) {
       double sks = 0.0;
       for (int p = 0; p < nn; ++p) sks += w[p] * simd[id[p] + (long long)G.nd * l];
@@ -605,6 +657,14 @@ extern "C" int ss3d_condition(double* res, const int n[3], int nreal, const doub
   }
   Model mdl;
   model_public(st, nst, nugget, mdl);
+  KModel kmdl{};
+  kmdl.nst = mdl.nst;
+  kmdl.nugget = mdl.nugget;
+  for (int q = 0; q < mdl.nst; q++) {
+    kmdl.itype[q] = mdl.itype[q];
+    kmdl.sill[q] = mdl.sill[q];
+    for (int e = 0; e < 9; e++) kmdl.rots[q][e] = mdl.rot[q][e] / mdl.ahmax[q];
+  }
   CondGeo G{};
   G.nx = nx;
   G.ny = ny;
@@ -707,10 +767,10 @@ extern "C" int ss3d_condition(double* res, const int n[3], int nreal, const doub
     // serving loop's higher-priority requests, gets SMs as blocks finish
     const int nblk = (int)(((long long)count + wpb - 1) / wpb);
     if (precision == SS3D_FP64)
-      k_cond_krige<0><<<nblk, 32 * wpb, cond_tri_bytes(cp->ndmax) + per * wpb, stm>>>(G, mdl, node0, count, dnbr, dnnb, ddx, ddy, ddz, ddg,
+      k_cond_krige<0><<<nblk, 32 * wpb, cond_tri_bytes(cp->ndmax) + per * wpb, stm>>>(G, kmdl, node0, count, dnbr, dnnb, ddx, ddy, ddz, ddg,
                                                           dsimd, dres, dcnt);
     else
-      k_cond_krige<1><<<nblk, 32 * wpb, cond_tri_bytes(cp->ndmax) + per * wpb, stm>>>(G, mdl, node0, count, dnbr, dnnb, ddx, ddy, ddz, ddg,
+      k_cond_krige<1><<<nblk, 32 * wpb, cond_tri_bytes(cp->ndmax) + per * wpb, stm>>>(G, kmdl, node0, count, dnbr, dnnb, ddx, ddy, ddz, ddg,
                                                           dsimd, dres, dcnt);
     ++g_launch_count;
     e = cudaGetLastError();
