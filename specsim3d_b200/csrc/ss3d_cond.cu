@@ -36,12 +36,14 @@ namespace ss3d {
 __host__ __device__ inline int cond_ld(int ndmax) { return ndmax | 1; }
 
 // shared memory of one kriging warp.  FP64 solves (prec 0): the covariance
-// matrix, factored in place (ndmax x ld doubles), four ndmax vectors of doubles
-// and the neighbour ids.  FP32 solves (prec 1): the FP64 matrix (kept for the
-// refinement residual), its FP32 factor (ndmax x ld floats), three ndmax vectors
-// of doubles, four of floats and the ids.  Rounded up to 16 bytes.
+// matrix with the right-hand side as an extra row, factored in place
+// ((ndmax + 1) x ld doubles), four ndmax vectors of doubles and the neighbour
+// ids.  FP32 solves (prec 1): the FP64 matrix (kept for the refinement
+// residual), its FP32 factor with the extra row ((ndmax + 1) x ld floats),
+// three ndmax vectors of doubles, four of floats and the ids.  Rounded up to 16
+// bytes.
 __host__ __device__ inline size_t cond_warp_bytes(int ndmax, int prec) {
-  const size_t n = (size_t)ndmax, m = n * (size_t)cond_ld(ndmax);
+  const size_t n = (size_t)ndmax, m = (n + 1) * (size_t)cond_ld(ndmax);
   const size_t b = prec == 0 ? m * 8 + n * 32 + n * 4 : m * 12 + n * 24 + n * 16 + n * 4;
   return (b + 15) & ~(size_t)15;
 }
@@ -215,23 +217,41 @@ __device__ void warp_tri_solve(const T* L, const T* rinv, int ld, int n, T* w, c
   }
 }
 
+// back substitution L^T w = y with the factor L (diagonal reciprocals rinv);
+// tmp is n scratch values
+template <typename T>
+__device__ void warp_tri_back(const T* L, const T* rinv, int ld, int n, T* w, const T* y, T* tmp, int lane) {
+  for (int p = lane; p < n; p += 32) tmp[p] = y[p];
+  __syncwarp();
+  for (int p = n - 1; p >= 0; --p) {
+    const T wp = tmp[p] * rinv[p];
+    for (int r = lane; r < p; r += 32) tmp[r] -= L[p * ld + r] * wp;
+    if (lane == 0) w[p] = wp;
+    __syncwarp();
+  }
+}
+
 // Cholesky factor of L + ridge I in place (lower triangle; L holds the matrix
 // on entry), warp-cooperative and right-looking: the trailing update of each
 // column goes over the lanes by the pair table (each element receives its
 // updates in column order, as in the serial algorithm); the column is scaled
-// by the reciprocal of its pivot, kept in rinv for the solves.  Returns false
-// on a non-positive pivot (the reference's chol_solve failure, f90:1040-1079).
+// by the reciprocal of its pivot, kept in rinv for the solves.  Row n holds a
+// right-hand side b and is carried through the same scalings and updates, so
+// that it ends as y = L^-1 b, the forward substitution done on the way.
+// Returns false on a non-positive pivot (the reference's chol_solve failure,
+// f90:1040-1079).
 template <typename T>
 __device__ bool warp_cholesky(T* L, T* rinv, int ld, int n, T ridge, const uint8_t* __restrict__ tri, int lane) {
   for (int p = lane; p < n; p += 32) L[p * ld + p] += ridge;
   __syncwarp();
+  T* y = L + (size_t)n * ld;
   for (int c = 0; c < n; ++c) {
     const T piv = L[c * ld + c];
     if (!(piv > T(0))) return false;   // uniform: every lane reads the same value
     const T inv = rsqrt_nr(piv);       // 1 / sqrt(pivot)
     const T dgl = piv * inv;
     __syncwarp();
-    for (int r = c + 1 + lane; r < n; r += 32) L[r * ld + c] *= inv;
+    for (int r = c + 1 + lane; r <= n; r += 32) L[r * ld + c] *= inv;   // row n: y_c
     if (lane == 0) {
       L[c * ld + c] = dgl;
       rinv[c] = inv;
@@ -242,6 +262,7 @@ __device__ bool warp_cholesky(T* L, T* rinv, int ld, int n, T ridge, const uint8
       const int r = c + 1 + tri[2 * e], cc = c + 1 + tri[2 * e + 1];
       L[r * ld + cc] -= L[r * ld + c] * L[cc * ld + c];
     }
+    for (int cc = c + 1 + lane; cc < n; cc += 32) y[cc] -= y[c] * L[cc * ld + c];
     __syncwarp();
   }
   return true;
@@ -269,7 +290,7 @@ __global__ void k_cond_krige(CondGeo G, KModel mdl, long long node0, int count, 
   __syncthreads();
   const size_t per = cond_warp_bytes(ndmax, PREC);
   unsigned char* mine = smc + cond_tri_bytes(ndmax) + per * wib;
-  const int n2 = ndmax * ld;
+  const int n2 = (ndmax + 1) * ld;   // matrix rows and the right-hand-side row
   double* A = (double*)mine;     // covariance matrix (PREC 0: factored in place)
   double* b = A + n2;
   double* w = b + ndmax;
@@ -327,18 +348,19 @@ __global__ void k_cond_krige(CondGeo G, KModel mdl, long long node0, int count, 
       if (PREC == 0) {
         if (tries > 1) {   // the failed factorization overwrote the matrix
           fill_matrix();
-          __syncwarp();
         }
+        for (int p = lane; p < nn; p += 32) A[nn * ld + p] = b[p];   // right-hand side row
+        __syncwarp();
         ok = warp_cholesky<double>(A, rinv, ld, nn, ridge, tri, lane);
-        if (ok) warp_tri_solve<double>(A, rinv, ld, nn, w, b, tmp, lane);
+        if (ok) warp_tri_back<double>(A, rinv, ld, nn, w, A + nn * ld, tmp, lane);
       } else {
-        // FP32 copies of A and b; the factor is built in place in Lf
-        for (int p = lane; p < nn; p += 32) bf[p] = (float)b[p];
+        // FP32 copies of A and b; the factor is built in place in Lf, b as its row nn
         for (int e = lane; e < nn * ld; e += 32) Lf[e] = (float)A[e];
+        for (int p = lane; p < nn; p += 32) Lf[nn * ld + p] = (float)b[p];
         __syncwarp();
         ok = warp_cholesky<float>(Lf, rinvf, ld, nn, (float)ridge, tri, lane);
         if (ok) {
-          warp_tri_solve<float>(Lf, rinvf, ld, nn, wf, bf, tf, lane);
+          warp_tri_back<float>(Lf, rinvf, ld, nn, wf, Lf + nn * ld, tf, lane);
           // one refinement: res = b - (A + ridge I) w in FP64 (to tmp), solve
           // L L^T d = res in FP32, w += d
           for (int p = lane; p < nn; p += 32) w[p] = (double)wf[p];
