@@ -291,6 +291,10 @@ typedef struct ss3d_server_config {
                                     them back when the queue head does not fit */
     double dry_run_ns_per_cell;  /* > 0: no GPU work, sleeps of this many ns per cell
                                     (scheduler tests); needs an explicit hbm_budget */
+    int64_t premap_bytes;        /* device bytes mapped into the stream-ordered pool at
+                                    creation (best effort, at most the budget; 0: none):
+                                    mapping pages while requests run stalls the device
+                                    for all of them */
 } ss3d_server_config;
 
 typedef struct ss3d_request {

@@ -350,13 +350,15 @@ class Server:
     ``slots`` requests run on the GPU at once, each on its own stream; queued
     requests are admitted in arrival order as slots and HBM free up (budget
     ``hbm_budget`` bytes, 0 = 80 % of free memory); spectra of seen models stay
-    resident (LRU, ``cache_budget`` bytes of idle spectra).  ``dry_run_ns_per_cell``
-    > 0 replaces the GPU work by sleeps (scheduler tests without a GPU)."""
+    resident (LRU, ``cache_budget`` bytes of idle spectra).  ``premap_bytes`` of
+    device memory are mapped into the stream-ordered pool at creation, so that
+    requests do not stall on page mapping.  ``dry_run_ns_per_cell`` > 0 replaces
+    the GPU work by sleeps (scheduler tests without a GPU)."""
 
     def __init__(self, slots=4, hbm_budget=0, cache_budget=0, retain_bytes=0, max_bypass=0, max_cond=0,
-                 dry_run_ns_per_cell=0.0):
+                 dry_run_ns_per_cell=0.0, premap_bytes=0):
         cfg = L.ServerConfig(int(slots), int(max_bypass), int(max_cond), int(hbm_budget), int(cache_budget),
-                             int(retain_bytes), float(dry_run_ns_per_cell))
+                             int(retain_bytes), float(dry_run_ns_per_cell), int(premap_bytes))
         h = ctypes.c_void_p()
         L.check(L.lib().ss3d_server_create(ctypes.byref(cfg), ctypes.byref(h)))
         self._h = h

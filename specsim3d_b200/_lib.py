@@ -60,7 +60,7 @@ class ServerConfig(ctypes.Structure):
     _fields_ = [("slots", ctypes.c_int), ("max_bypass", ctypes.c_int), ("max_cond", ctypes.c_int),
                 ("hbm_budget", ctypes.c_int64),
                 ("cache_budget", ctypes.c_int64), ("retain_bytes", ctypes.c_int64),
-                ("dry_run_ns_per_cell", ctypes.c_double)]
+                ("dry_run_ns_per_cell", ctypes.c_double), ("premap_bytes", ctypes.c_int64)]
 
 
 class Request(ctypes.Structure):

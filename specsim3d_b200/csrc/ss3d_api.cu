@@ -580,6 +580,25 @@ extern "C" int ss3d_release_workspace(void) {
   return SS3D_OK;
 }
 
+size_t ss3d::pool_premap(size_t bytes) {
+  DevCtx* ctx;
+  if (get_ctx(&ctx)) return 0;   // also sets the pool's release threshold
+  cudaStream_t st = nullptr;
+  if (cudaStreamCreateWithFlags(&st, cudaStreamNonBlocking) != cudaSuccess) return 0;
+  size_t done = 0;
+  for (size_t b = bytes; b >= ((size_t)256 << 20) && !done; b /= 2) {
+    void* p = nullptr;
+    if (cudaMallocAsync(&p, b, st) == cudaSuccess) {
+      cudaFreeAsync(p, st);
+      done = b;
+    }
+    cudaGetLastError();
+  }
+  cudaStreamSynchronize(st);
+  cudaStreamDestroy(st);
+  return done;
+}
+
 extern "C" int ss3d_trim_pool(void) {
   int dev = 0;
   CK(cudaGetDevice(&dev));

@@ -112,6 +112,11 @@ namespace ss3d {
 int spectrum_view(const ss3d_spectrum* sp, NoallocView* v);
 int64_t realize_bytes_for(const int np[3], const int n[3], int nreal, int precision, int host_out);
 int batch_ctx(int dev, Tw* tw, const uint32_t** ptab);   // twiddle and jump tables of the current device
+// Maps up to `bytes` of device memory into the stream-ordered pool of the
+// current device (one allocation, freed at once; the pool keeps it mapped), so
+// that later allocations up to that total find mapped pages; best effort:
+// halves the request on failure.  Returns the bytes mapped.
+size_t pool_premap(size_t bytes);
 // geometry of a spectrum for igauss and its FP32 amplitudes; 1 if the handle is
 // invalid or lives on another device than the current one
 int batch_geo(const ss3d_spectrum* sp, int igauss, Geo* g, const float** amp32);

@@ -370,6 +370,11 @@ extern "C" int ss3d_server_create(const ss3d_server_config* cfg, ss3d_server** o
       return set_error(SS3D_ECUDA, "server: no CUDA device");
     }
     if (s->cfg.hbm_budget <= 0) s->cfg.hbm_budget = (int64_t)(0.8 * (double)fr);
+    // map pages into the stream-ordered pool now if asked: mapping pages while
+    // requests run stalls the device for all of them (about a millisecond per
+    // few MB)
+    if (s->cfg.premap_bytes > 0)
+      pool_premap((size_t)std::min<int64_t>(s->cfg.premap_bytes, s->cfg.hbm_budget));
   } else if (s->cfg.hbm_budget <= 0) {
     delete s;
     return set_error(SS3D_EINVAL, "dry run needs an explicit hbm_budget");
