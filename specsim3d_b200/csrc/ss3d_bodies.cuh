@@ -100,9 +100,9 @@ __device__ __forceinline__ cpx_t<R> coef_from_state(uint32_t s1, R am, bool self
       const float rr = L * rsqrt_hw(L);
       float cs, sn;
       phasor_f(s2, cs, sn);
-      const float a = self ? am : am * 0.70710678118654752f;
-      const float re = a * (rr * cs);
-      const float im = (conj ? -a : a) * (rr * sn);
+      const float t = (self ? am : am * 0.70710678118654752f) * rr;
+      const float re = t * cs;
+      const float im = (conj ? -t : t) * sn;
       return cmk<C>(re, self ? 0.f : im);
     } else {
       const double rr = sqrt(m2log_d(s1));
@@ -134,12 +134,12 @@ __device__ __forceinline__ float2 m2log_f2(uint32_t s0, uint32_t s1) {
   const float2 q = kmul(a, make_float2(rcp_hw(b.x), rcp_hw(b.y)));
   const float2 z = kneg(q);
   const float2 z2 = kmul(z, z);
-  float2 p = kfma(z2, kconst<float2>(1.0f / 7.0f), kconst<float2>(1.0f / 5.0f));
-  p = kfma(z2, p, kconst<float2>(1.0f / 3.0f));
-  p = kfma(z2, p, kconst<float2>(1.0));
-  const float2 near1 = kmul(kconst<float2>(-4.0), kmul(p, z));
-  const float2 u = kmul(make_float2((float)s0, (float)s1), kconst<float2>(1.0f / 2147483647.0f));
-  const float2 far = kmul(kconst<float2>(-1.3862944f), make_float2(lg2_hw(u.x), lg2_hw(u.y)));
+  float2 p = kfma(z2, kconst<float2>(-4.0f / 7.0f), kconst<float2>(-4.0f / 5.0f));
+  p = kfma(z2, p, kconst<float2>(-4.0f / 3.0f));
+  p = kfma(z2, p, kconst<float2>(-4.0));
+  const float2 near1 = kmul(p, z);
+  const float2 far = kfma(kconst<float2>(-1.3862944f), make_float2(lg2_hw((float)s0), lg2_hw((float)s1)),
+                          kconst<float2>(M2LOG_C31));
   return make_float2(s0 >= 1610612736u ? near1.x : far.x, s1 >= 1610612736u ? near1.y : far.y);
 }
 __device__ __forceinline__ void phasor_f2(uint32_t s0, uint32_t s1, float2& c, float2& sn) {
@@ -158,9 +158,9 @@ __device__ __forceinline__ cpair coef_pair(uint32_t s0, uint32_t s1, float2 am, 
     float2 cs, sn;
     phasor_f2(pm_mulmod_lazy(s0, PM_A), pm_mulmod_lazy(s1, PM_A), cs, sn);
     const float2 ah = kmul(am, kconst<float2>(0.70710678118654752f));
-    const float2 a = make_float2(self0 ? am.x : ah.x, self1 ? am.y : ah.y);
-    const float2 re = kmul(a, kmul(rr, cs));
-    const float2 im = kmul(conj ? kneg(a) : a, kmul(rr, sn));
+    const float2 t = kmul(make_float2(self0 ? am.x : ah.x, self1 ? am.y : ah.y), rr);
+    const float2 re = kmul(t, cs);
+    const float2 im = kmul(conj ? kneg(t) : t, sn);
     return cpair{re, make_float2(self0 ? 0.f : im.x, self1 ? 0.f : im.y)};
   } else {
     float2 cs, sn;

@@ -221,15 +221,18 @@ __device__ __forceinline__ void phasor_d(uint32_t s, double& c, double& sn) {
 // the quotient by the hardware reciprocal, relative error about 2^-23);
 // below 3/4 |ln u| >= 0.28 and the hardware log2 (absolute error ~2^-22) is
 // accurate to a few 1e-7 relative.
+// The series is evaluated as z (-4 - 4/3 z^2 - 4/5 z^4 - 4/7 z^6); the far
+// branch as -2 ln 2 (log2 s - 31), u = s 2^-31 (the float of 1/(2^31 - 1)).
+constexpr float M2LOG_C31 = 42.975124f;   // 2 ln 2 * 31
 __device__ __forceinline__ float m2log_f(uint32_t s) {
   const float a = (float)(PM_M - s);
   const float z = -(a * rcp_hw(4294967294.0f - a));        // (u-1)/(u+1), m + s = 2m - (m - s)
   const float z2 = z * z;
-  float p = fmaf(z2, 1.0f / 7.0f, 1.0f / 5.0f);
-  p = fmaf(z2, p, 1.0f / 3.0f);
-  p = fmaf(z2, p, 1.0f);
-  const float near1 = -4.0f * (p * z);
-  const float far = -1.3862944f * lg2_hw((float)s * (1.0f / 2147483647.0f));   // -2 ln 2 * log2(u)
+  float p = fmaf(z2, -4.0f / 7.0f, -4.0f / 5.0f);
+  p = fmaf(z2, p, -4.0f / 3.0f);
+  p = fmaf(z2, p, -4.0f);
+  const float near1 = p * z;
+  const float far = fmaf(-1.3862944f, lg2_hw((float)s), M2LOG_C31);
   return s >= 1610612736u ? near1 : far;                    // u >= 3/4
 }
 __device__ __forceinline__ double m2log_d(uint32_t s) {
@@ -277,10 +280,9 @@ __device__ __forceinline__ cpx_t<R> coefficient(const Geo& g, int i, int j, int 
       float rr = L * rsqrt_hw(L);
       float cs, sn;
       phasor_f(s2, cs, sn);
-      if (self) return cmk<C>(amp * (rr * cs), 0.f);
-      const float h = 0.70710678118654752f;
-      float a = amp * h;
-      return cmk<C>(a * (rr * cs), (conj ? -a : a) * (rr * sn));
+      const float t = (self ? amp : amp * 0.70710678118654752f) * rr;
+      if (self) return cmk<C>(t * cs, 0.f);
+      return cmk<C>(t * cs, (conj ? -t : t) * sn);
     } else {
       double rr = sqrt(m2log_d(s1));
       double cs, sn;
@@ -322,9 +324,9 @@ __device__ __forceinline__ cpx_t<R> coef_col(const Geo& g, int j, int k, R amp, 
       const float rr = L * rsqrt_hw(L);
       float cs, sn;
       phasor_f(s2, cs, sn);
-      if (self) return cmk<C>(amp * (rr * cs), 0.f);
-      const float a = amp * 0.70710678118654752f;
-      return cmk<C>(a * (rr * cs), (greater ? -a : a) * (rr * sn));
+      const float t = (self ? amp : amp * 0.70710678118654752f) * rr;
+      if (self) return cmk<C>(t * cs, 0.f);
+      return cmk<C>(t * cs, (greater ? -t : t) * sn);
     } else {
       const double rr = sqrt(m2log_d(s1));
       double cs, sn;
