@@ -99,8 +99,9 @@ __device__ __forceinline__ cpx_t<R> coef_from_state(uint32_t s1, R am, bool self
       const float L = m2log_f(s1);
       const float rr = L * rsqrt_hw(L);
       float cs, sn;
-      phasor_f(s2, cs, sn);
-      const float t = (self ? am : am * 0.70710678118654752f) * rr;
+      const bool odd = phasor_half_f(s2, cs, sn);
+      const float t0 = (self ? am : am * 0.70710678118654752f) * rr;
+      const float t = odd ? -t0 : t0;
       const float re = t * cs;
       const float im = (conj ? -t : t) * sn;
       return cmk<C>(re, self ? 0.f : im);
@@ -115,11 +116,15 @@ __device__ __forceinline__ cpx_t<R> coef_from_state(uint32_t s1, R am, bool self
       return cmk<C>(re, self ? 0.0 : im);
     }
   } else {
-    R cs, sn;
-    if constexpr (sizeof(R) == 4) phasor_f(s1, cs, sn); else phasor_d(s1, cs, sn);
+    R cs, sn, a = am;
+    if constexpr (sizeof(R) == 4) {
+      if (phasor_half_f(s1, cs, sn)) a = -a;
+    } else {
+      phasor_d(s1, cs, sn);
+    }
     const R sgn = (2ull * s1) < (uint64_t)PM_M ? am : -am;   // urand() < 0.5
-    const R re = self ? sgn : am * cs;
-    const R im = conj ? -(am * sn) : am * sn;
+    const R re = self ? sgn : a * cs;
+    const R im = conj ? -(a * sn) : a * sn;
     return cmk<C>(re, self ? R(0) : im);
   }
 }
@@ -132,23 +137,25 @@ __device__ __forceinline__ float2 m2log_f2(uint32_t s0, uint32_t s1) {
   const float2 a = make_float2((float)(PM_M - s0), (float)(PM_M - s1));
   const float2 b = ksub(kconst<float2>(4294967294.0), a);
   const float2 q = kmul(a, make_float2(rcp_hw(b.x), rcp_hw(b.y)));
-  const float2 z = kneg(q);
-  const float2 z2 = kmul(z, z);
-  float2 p = kfma(z2, kconst<float2>(-4.0f / 7.0f), kconst<float2>(-4.0f / 5.0f));
-  p = kfma(z2, p, kconst<float2>(-4.0f / 3.0f));
-  p = kfma(z2, p, kconst<float2>(-4.0));
-  const float2 near1 = kmul(p, z);
+  const float2 z2 = kmul(q, q);
+  float2 p = kfma(z2, kconst<float2>(4.0f / 7.0f), kconst<float2>(4.0f / 5.0f));
+  p = kfma(z2, p, kconst<float2>(4.0f / 3.0f));
+  p = kfma(z2, p, kconst<float2>(4.0));
+  const float2 near1 = kmul(p, q);
   const float2 far = kfma(kconst<float2>(-1.3862944f), make_float2(lg2_hw((float)s0), lg2_hw((float)s1)),
                           kconst<float2>(M2LOG_C31));
   return make_float2(s0 >= 1610612736u ? near1.x : far.x, s1 >= 1610612736u ? near1.y : far.y);
 }
-__device__ __forceinline__ void phasor_f2(uint32_t s0, uint32_t s1, float2& c, float2& sn) {
+// cos and sin of the two remainders; odd0/odd1 as phasor_half_f returns them
+__device__ __forceinline__ void phasor_half_f2(uint32_t s0, uint32_t s1, float2& c, float2& sn, bool& odd0,
+                                               bool& odd1) {
   const int n0 = half_turns(s0), n1 = half_turns(s1);
   const float2 x = kmul(make_float2((float)half_turn_rem(s0, n0), (float)half_turn_rem(s1, n1)),
                         kconst<float2>(1.4629181e-9f));
-  const float sp0 = sin_hw(x.x), cp0 = cos_hw(x.x), sp1 = sin_hw(x.y), cp1 = cos_hw(x.y);
-  c = make_float2((n0 & 1) ? -cp0 : cp0, (n1 & 1) ? -cp1 : cp1);
-  sn = make_float2((n0 & 1) ? -sp0 : sp0, (n1 & 1) ? -sp1 : sp1);
+  sn = make_float2(sin_hw(x.x), sin_hw(x.y));
+  c = make_float2(cos_hw(x.x), cos_hw(x.y));
+  odd0 = n0 & 1;
+  odd1 = n1 & 1;
 }
 template <int GAUSS>
 __device__ __forceinline__ cpair coef_pair(uint32_t s0, uint32_t s1, float2 am, bool self0, bool self1, bool conj) {
@@ -156,17 +163,21 @@ __device__ __forceinline__ cpair coef_pair(uint32_t s0, uint32_t s1, float2 am, 
     const float2 L = m2log_f2(s0, s1);
     const float2 rr = kmul(L, make_float2(rsqrt_hw(L.x), rsqrt_hw(L.y)));
     float2 cs, sn;
-    phasor_f2(pm_mulmod_lazy(s0, PM_A), pm_mulmod_lazy(s1, PM_A), cs, sn);
+    bool odd0, odd1;
+    phasor_half_f2(pm_mulmod_lazy(s0, PM_A), pm_mulmod_lazy(s1, PM_A), cs, sn, odd0, odd1);
     const float2 ah = kmul(am, kconst<float2>(0.70710678118654752f));
-    const float2 t = kmul(make_float2(self0 ? am.x : ah.x, self1 ? am.y : ah.y), rr);
+    const float2 t0 = kmul(make_float2(self0 ? am.x : ah.x, self1 ? am.y : ah.y), rr);
+    const float2 t = make_float2(odd0 ? -t0.x : t0.x, odd1 ? -t0.y : t0.y);
     const float2 re = kmul(t, cs);
     const float2 im = kmul(conj ? kneg(t) : t, sn);
     return cpair{re, make_float2(self0 ? 0.f : im.x, self1 ? 0.f : im.y)};
   } else {
     float2 cs, sn;
-    phasor_f2(s0, s1, cs, sn);
-    const float2 re = kmul(am, cs);
-    const float2 im0 = kmul(am, sn);
+    bool odd0, odd1;
+    phasor_half_f2(s0, s1, cs, sn, odd0, odd1);
+    const float2 a = make_float2(odd0 ? -am.x : am.x, odd1 ? -am.y : am.y);
+    const float2 re = kmul(a, cs);
+    const float2 im0 = kmul(a, sn);
     const float2 im = conj ? kneg(im0) : im0;
     const float sg0 = (2ull * s0) < (uint64_t)PM_M ? am.x : -am.x, sg1 = (2ull * s1) < (uint64_t)PM_M ? am.y : -am.y;
     return cpair{make_float2(self0 ? sg0 : re.x, self1 ? sg1 : re.y),

@@ -204,12 +204,14 @@ __device__ __forceinline__ int half_turns(uint32_t s) { return (int)((s >> 30) +
 __device__ __forceinline__ int half_turn_rem(uint32_t s, int n) {
   return (int)(2u * s - ((uint32_t)n << 31) + (uint32_t)n);   // 2s - n (2^31 - 1)  (mod 2^32)
 }
-__device__ __forceinline__ void phasor_f(uint32_t s, float& c, float& sn) {
+// cos and sin of the remainder; returns true for an odd half-turn count, when
+// the phasor is (-c, -sn): callers fold that sign into their scale factor
+__device__ __forceinline__ bool phasor_half_f(uint32_t s, float& c, float& sn) {
   const int n = half_turns(s);
   const float x = (float)half_turn_rem(s, n) * 1.4629181e-9f;   // pi / (2^31-1)
-  const float sp = sin_hw(x), cp = cos_hw(x);
-  c = (n & 1) ? -cp : cp;
-  sn = (n & 1) ? -sp : sp;
+  sn = sin_hw(x);
+  c = cos_hw(x);
+  return n & 1;
 }
 __device__ __forceinline__ void phasor_d(uint32_t s, double& c, double& sn) {
   double u = (double)s / 2147483647.0;
@@ -221,17 +223,17 @@ __device__ __forceinline__ void phasor_d(uint32_t s, double& c, double& sn) {
 // the quotient by the hardware reciprocal, relative error about 2^-23);
 // below 3/4 |ln u| >= 0.28 and the hardware log2 (absolute error ~2^-22) is
 // accurate to a few 1e-7 relative.
-// The series is evaluated as z (-4 - 4/3 z^2 - 4/5 z^4 - 4/7 z^6); the far
+// The series is evaluated as q (4 + 4/3 q^2 + 4/5 q^4 + 4/7 q^6), q = -z; the far
 // branch as -2 ln 2 (log2 s - 31), u = s 2^-31 (the float of 1/(2^31 - 1)).
 constexpr float M2LOG_C31 = 42.975124f;   // 2 ln 2 * 31
 __device__ __forceinline__ float m2log_f(uint32_t s) {
   const float a = (float)(PM_M - s);
-  const float z = -(a * rcp_hw(4294967294.0f - a));        // (u-1)/(u+1), m + s = 2m - (m - s)
-  const float z2 = z * z;
-  float p = fmaf(z2, -4.0f / 7.0f, -4.0f / 5.0f);
-  p = fmaf(z2, p, -4.0f / 3.0f);
-  p = fmaf(z2, p, -4.0f);
-  const float near1 = p * z;
+  const float q = a * rcp_hw(4294967294.0f - a);           // -z = (1-u)/(1+u), m + s = 2m - (m - s)
+  const float z2 = q * q;
+  float p = fmaf(z2, 4.0f / 7.0f, 4.0f / 5.0f);
+  p = fmaf(z2, p, 4.0f / 3.0f);
+  p = fmaf(z2, p, 4.0f);
+  const float near1 = p * q;
   const float far = fmaf(-1.3862944f, lg2_hw((float)s), M2LOG_C31);
   return s >= 1610612736u ? near1 : far;                    // u >= 3/4
 }
@@ -279,8 +281,9 @@ __device__ __forceinline__ cpx_t<R> coefficient(const Geo& g, int i, int j, int 
       const float L = m2log_f(s1);
       float rr = L * rsqrt_hw(L);
       float cs, sn;
-      phasor_f(s2, cs, sn);
-      const float t = (self ? amp : amp * 0.70710678118654752f) * rr;
+      const bool odd = phasor_half_f(s2, cs, sn);
+      const float t0 = (self ? amp : amp * 0.70710678118654752f) * rr;
+      const float t = odd ? -t0 : t0;
       if (self) return cmk<C>(t * cs, 0.f);
       return cmk<C>(t * cs, (conj ? -t : t) * sn);
     } else {
@@ -298,9 +301,13 @@ __device__ __forceinline__ cpx_t<R> coefficient(const Geo& g, int i, int j, int 
       bool pos = (2ull * s1) < (uint64_t)PM_M;
       return cmk<C>(pos ? amp : -amp, R(0));
     }
-    R cs, sn;
-    if constexpr (sizeof(R) == 4) phasor_f(s1, cs, sn); else phasor_d(s1, cs, sn);
-    return cmk<C>(amp * cs, conj ? -(amp * sn) : amp * sn);
+    R cs, sn, a = amp;
+    if constexpr (sizeof(R) == 4) {
+      if (phasor_half_f(s1, cs, sn)) a = -a;
+    } else {
+      phasor_d(s1, cs, sn);
+    }
+    return cmk<C>(a * cs, conj ? -(a * sn) : a * sn);
   }
 }
 
@@ -323,8 +330,9 @@ __device__ __forceinline__ cpx_t<R> coef_col(const Geo& g, int j, int k, R amp, 
       const float L = m2log_f(s1);
       const float rr = L * rsqrt_hw(L);
       float cs, sn;
-      phasor_f(s2, cs, sn);
-      const float t = (self ? amp : amp * 0.70710678118654752f) * rr;
+      const bool odd = phasor_half_f(s2, cs, sn);
+      const float t0 = (self ? amp : amp * 0.70710678118654752f) * rr;
+      const float t = odd ? -t0 : t0;
       if (self) return cmk<C>(t * cs, 0.f);
       return cmk<C>(t * cs, (greater ? -t : t) * sn);
     } else {
@@ -338,9 +346,13 @@ __device__ __forceinline__ cpx_t<R> coef_col(const Geo& g, int j, int k, R amp, 
     }
   } else {
     if (self) return cmk<C>((2ull * s1) < (uint64_t)PM_M ? amp : -amp, R(0));
-    R cs, sn;
-    if constexpr (sizeof(R) == 4) phasor_f(s1, cs, sn); else phasor_d(s1, cs, sn);
-    return cmk<C>(amp * cs, greater ? -(amp * sn) : amp * sn);
+    R cs, sn, a = amp;
+    if constexpr (sizeof(R) == 4) {
+      if (phasor_half_f(s1, cs, sn)) a = -a;
+    } else {
+      phasor_d(s1, cs, sn);
+    }
+    return cmk<C>(a * cs, greater ? -(a * sn) : a * sn);
   }
 }
 
