@@ -157,8 +157,10 @@ int ss3d_autotune(const ss3d_spectrum *sp, int igauss, int precision, int nreal,
 /* Explicit variant of kernel kind 0 middle pass, 1 synthesis pass, 2 row
  * pass, for one precision and transform length 2^logn: 0..3 one line per
  * thread; for the FP32 column passes (kinds 0, 1) also 4..7, two adjacent
- * lines per thread on the packed FP32 instructions.  Every variant computes
- * the same values; they differ in tile shape and instruction form only. */
+ * lines per thread on the packed FP32 instructions; for the row pass also 4,
+ * each row held in the registers of one warp (row lengths 8..512 in FP32,
+ * 8..256 in FP64; other lengths run variant 0).  Every variant computes the
+ * same values; they differ in tile shape and instruction form only. */
 int ss3d_set_variant(int kind, int precision, int logn, int variant);
 
 /* ---------------------------------------------------------------- batched form */

@@ -884,10 +884,12 @@ extern "C" int ss3d_autotune(const ss3d_spectrum* sp, int igauss, int precision,
   int bestv[3] = {0, 0, 0};
   int rc = SS3D_OK;
   // variants per kind: 0-3 everywhere, FP32 column passes also 4-7 (two
-  // lines per thread); the row pass runs its variant v mod 4 meanwhile
-  const int nvk[3] = {precision == SS3D_FP32 ? 8 : 4, precision == SS3D_FP32 ? 8 : 4, 4};
+  // lines per thread), the row pass also 4 (rows held in warps); a kind with
+  // fewer variants runs its variant v mod 4 meanwhile
+  const int nvk[3] = {precision == SS3D_FP32 ? 8 : 4, precision == SS3D_FP32 ? 8 : 4, 5};
+  const int nv = std::max(nvk[0], nvk[2]);
   auto vk = [&](int k, int v) { return v < nvk[k] ? v : v % 4; };
-  for (int v = 0; v < nvk[0] && rc == SS3D_OK; v++) {
+  for (int v = 0; v < nv && rc == SS3D_OK; v++) {
     for (int k = 0; k < 3; k++)
       if (L[k] >= 0) g_variant[k][p][L[k]] = vk(k, v);
     rc = ss3d_realize(sp, 1, 0, nreal, igauss, precision, out, SS3D_OUT_F32, nullptr);   // warm up
@@ -915,7 +917,8 @@ extern "C" int ss3d_autotune(const ss3d_spectrum* sp, int igauss, int precision,
 }
 
 extern "C" int ss3d_set_variant(int kind, int precision, int logn, int variant) {
-  const int vmax = (precision == SS3D_FP32 && kind < 2) ? 7 : 3;   // 4-7: FP32 two-line column tiles
+  // 4-7: FP32 two-line column tiles; 4 of the row pass: rows held in warps
+  const int vmax = kind == 2 ? 4 : (precision == SS3D_FP32 ? 7 : 3);
   if (kind < 0 || kind > 2 || (precision != SS3D_FP64 && precision != SS3D_FP32) || logn < 0 || logn > 15 ||
       variant < 0 || variant > vmax)
     return fail(SS3D_EINVAL, "invalid variant selection");

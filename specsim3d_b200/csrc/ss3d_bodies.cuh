@@ -558,4 +558,124 @@ __device__ __forceinline__ void rows_body(const Geo& g, const cpx_t<R>* __restri
   }
 }
 
+// ---------------------------------------------------------------- x pass, rows in warps
+// The same C2R + crop with each row held by TPC lanes of one warp (RPW = 32 /
+// TPC rows per warp): the N+1 inputs go from global memory straight into
+// registers (lane rank c holds positions c + TPC i, coalesced), the packing
+// takes X[N-q] from the mirrored lane by a shuffle, the transform runs on the
+// warp's own shared-memory slice with warp barriers, and the last pass stores
+// the cropped row.  Shared memory sees only the exchanges between radix passes
+// (rows_body also stages the rows, packs in place and reads the result back).
+// The packing and the butterflies are the operations of rows_body, so the
+// values are the same bits.
+template <typename R, int LOGN> struct RowWarpCfg {
+  static constexpr int N = 1 << LOGN;
+  static constexpr int ET = N > 256 ? 16 : 8;   // elements per lane
+  static constexpr int TPC = N / ET;            // lanes per row
+  static constexpr int RPW = TPC >= 32 ? 1 : 32 / TPC;
+  static constexpr int NW = 8;                  // warps per block
+  static constexpr int NTH = 32 * NW;
+  static constexpr int ROWS = NW * RPW;         // rows per block
+  static constexpr int SLICE = N * RPW;         // exchange elements per warp
+  static constexpr bool ok = LOGN >= 3 && LOGN <= (sizeof(R) == 4 ? 9 : 8);
+  static constexpr size_t smem = (size_t)(2 * N + NW * SLICE) * sizeof(cpx_t<R>);
+};
+
+template <typename R, typename O, int LOGN>
+__device__ __forceinline__ void rows_warp_body(const Geo& g, const cpx_t<R>* __restrict__ in, long long rstride,
+                                               O* __restrict__ out, long long ostride, int nreal, int nblk_per_r,
+                                               double* __restrict__ part, const Tw& tw, int item,
+                                               unsigned char* smraw) {
+  using C = cpx_t<R>;
+  using W = RowWarpCfg<R, LOGN>;
+  constexpr int N = W::N, ET = W::ET, TPC = W::TPC, RPW = W::RPW;
+  static_assert(W::ok && TPC * RPW == 32, "rows of whole warps");
+  C* stw = reinterpret_cast<C*>(smraw);   // N entries e^{-2 pi i m/(2N)}
+  C* stwN = stw + N;                      // N entries e^{-2 pi i m/N}
+  const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
+  C* sx = stwN + N + warp * W::SLICE;
+  const int r = item % nreal;
+  const int blk = item / nreal;
+  for (int q = threadIdx.x; q < N; q += W::NTH) {
+    stw[q] = twtab<R>(tw)[2 * N - 1 + q];
+    stwN[q] = twtab<R>(tw)[N - 1 + q];
+  }
+  const int t = lane % RPW, c = lane / RPW;
+  const int nrows = g.ny * g.nz;
+  const int row = (blk * W::NW + warp) * RPW + t;
+  const bool ok = row < nrows;
+  const int j = ok ? row % g.ny : 0, k = ok ? row / g.ny : 0;
+  const C* rp = in + (long long)r * rstride + ((long long)k * g.npy + j) * g.HP;
+  C x[ET];
+#pragma unroll
+  for (int i = 0; i < ET; ++i) x[i] = rp[c + TPC * i];
+  const C xN = rp[N];
+  __syncthreads();
+  // Z[q] = (X[q] + conj X[N-q]) + i w^q (X[q] - conj X[N-q]), q = c + TPC i:
+  // rank (TPC - c) of the row holds X[N-q] in register ET-1-i; rank 0 holds
+  // X[N - TPC i] itself in register ET-i, and X[N]
+  const int mirror = ((TPC - c) % TPC) * RPW + t;
+  C z[ET];
+#pragma unroll
+  for (int i = 0; i < ET; ++i) {
+    C b;
+    b.x = __shfl_sync(0xffffffffu, x[ET - 1 - i].x, mirror);
+    b.y = __shfl_sync(0xffffffffu, x[ET - 1 - i].y, mirror);
+    if (c == 0) b = i == 0 ? xN : x[(ET - i) % ET];
+    C a = x[i];
+    const int q = c + TPC * i;
+    if (q == 0) {
+      a.y = R(0);
+      b.y = R(0);
+    }
+    C w = stw[q];
+    w.y = -w.y;
+    const C bc = cmk<C>(b.x, -b.y);
+    z[i] = cadd(cadd(a, bc), cmul_si<+1>(cmul(w, csub(a, bc))));
+  }
+  // pass-0 order of the engine: v[m R0 + r] = position c + TPC m + r N / R0
+  constexpr int R0 = Sched<LOGN>::radix(0), NBT = ET / R0;
+  C v[ET];
+#pragma unroll
+  for (int m = 0; m < NBT; ++m)
+#pragma unroll
+    for (int rr = 0; rr < R0; ++rr) v[m * R0 + rr] = z[m + rr * NBT];
+  double s1 = 0.0, s2 = 0.0;
+  const bool stats = part != nullptr;
+  O* orow = out + (long long)r * ostride + (long long)(ok ? row : 0) * g.nx;
+  const int nxh = (g.nx + 1) / 2;
+  const bool even = (g.nx & 1) == 0;
+  fft_tile_regs<LOGN, RPW, TPC, +1, RPW, false, false, -1>(sx, stwN, v, t, c, [&](int pos, C zz) {
+    if (ok && pos < nxh) {
+      const O a0 = (O)zz.x, a1 = (O)zz.y;
+      const bool second = even || 2 * pos + 1 < g.nx;
+      if (even) {
+        if constexpr (sizeof(O) == 4) {
+          reinterpret_cast<float2*>(orow)[pos] = make_float2((float)a0, (float)a1);
+        } else {
+          reinterpret_cast<double2*>(orow)[pos] = make_double2((double)a0, (double)a1);
+        }
+      } else {
+        orow[2 * pos] = a0;
+        if (second) orow[2 * pos + 1] = a1;
+      }
+      if (stats) {
+        s1 += (double)zz.x;
+        s2 += (double)zz.x * (double)zz.x;
+        if (second) {
+          s1 += (double)zz.y;
+          s2 += (double)zz.y * (double)zz.y;
+        }
+      }
+    }
+  });
+  if (part) {
+    block_sum2<W::NTH>(s1, s2);
+    if (threadIdx.x == 0) {
+      part[2 * ((long long)r * nblk_per_r + blk)] = s1;
+      part[2 * ((long long)r * nblk_per_r + blk) + 1] = s2;
+    }
+  }
+}
+
 }  // namespace ss3d

@@ -28,6 +28,29 @@ namespace ss3d {
 
 template <int SWM> __device__ __forceinline__ int sw(int p) { return SWM ? p ^ ((p >> 3) & SWM) : p; }
 
+// Exchange index of position p of column t.  SWM >= 0: sw(p) * PITCH + t.
+// SWM < 0 (tiles of one warp, PITCH = TX rows of one warp): a = p * PITCH + t
+// permuted as a ^ ((a >> 3) & 15), a bijection (bits 4-6 are kept, bits 0-3
+// take bits 3-6 in); every exchange of the Stockham schedule then uses the
+// minimum number of shared-memory wavefronts for transform lengths 32..512.
+template <int PITCH, int SWM> __device__ __forceinline__ int xidx(int p, int t) {
+  if constexpr (SWM < 0) {
+    const int a = p * PITCH + t;
+    return a ^ ((a >> 3) & 15);
+  } else {
+    return sw<SWM>(p) * PITCH + t;
+  }
+}
+
+// barrier among the NTH threads of a tile: a warp barrier when the tile is
+// one warp (the tiles of the warps of a block are then independent)
+template <int NTH> __device__ __forceinline__ void tile_sync() {
+  if constexpr (NTH <= 32)
+    __syncwarp();
+  else
+    __syncthreads();
+}
+
 // SWM of a row of PITCH elements of EB bytes: 128 / row - 1 for a row of a
 // power-of-two size below 128 bytes, else 0
 template <int PITCH, int EB> struct Swizzle {
@@ -50,7 +73,7 @@ __device__ __forceinline__ void fft_tile_rest(C* __restrict__ s, const C* __rest
     for (int m = 0; m < NBT; ++m) {
       const int jb = c + TPC * m;
 #pragma unroll
-      for (int r = 0; r < R; ++r) v[m * R + r] = s[sw<SWM>(jb + r * (N / R)) * PITCH + t];
+      for (int r = 0; r < R; ++r) v[m * R + r] = s[xidx<PITCH, SWM>(jb + r * (N / R), t)];
     }
 #pragma unroll
     for (int m = 0; m < NBT; ++m) {
@@ -61,7 +84,7 @@ __device__ __forceinline__ void fft_tile_rest(C* __restrict__ s, const C* __rest
       dftR<R, SIGN>(&v[m * R]);
     }
     if constexpr (P == NP - 1) {
-      if constexpr (STORE_SYNC) __syncthreads();
+      if constexpr (STORE_SYNC) tile_sync<TX * TPC>();
 #pragma unroll
       for (int m = 0; m < NBT; ++m) {
         const int jb = c + TPC * m;
@@ -71,21 +94,57 @@ __device__ __forceinline__ void fft_tile_rest(C* __restrict__ s, const C* __rest
         for (int r = 0; r < R; ++r) store(idxD + r * NS, v[m * R + r]);
       }
     } else {
-      __syncthreads();
+      tile_sync<TX * TPC>();
 #pragma unroll
       for (int m = 0; m < NBT; ++m) {
         const int jb = c + TPC * m;
         const int k = jb % NS;
         const int idxD = (jb / NS) * NS * R + k;
 #pragma unroll
-        for (int r = 0; r < R; ++r) s[sw<SWM>(idxD + r * NS) * PITCH + t] = v[m * R + r];
+        for (int r = 0; r < R; ++r) s[xidx<PITCH, SWM>(idxD + r * NS, t)] = v[m * R + r];
       }
-      __syncthreads();
+      tile_sync<TX * TPC>();
       fft_tile_rest<LOGN, TX, TPC, SIGN, P + 1, PITCH, STORE_SYNC, SWM>(s, tw, v, t, c, store);
     }
   }
 }
 
+
+// Passes of the tile from pass-0 inputs already in registers: v[m * R0 + r]
+// holds position jb + r * N / R0, jb = c + TPC * m (R0 the radix of pass 0).
+// t = column, c = rank of the thread in its column.  SWM: exchange layout
+// (xidx).  LOAD_SYNC / STORE_SYNC as for fft_tile.
+template <int LOGN, int TX, int TPC, int SIGN, int PITCH, bool LOAD_SYNC, bool STORE_SYNC, int SWM, typename C,
+          class Store>
+__device__ __forceinline__ void fft_tile_regs(C* __restrict__ s, const C* __restrict__ tw, C* v, int t, int c,
+                                              Store&& store) {
+  constexpr int N = 1 << LOGN;
+  constexpr int ET = N / TPC;
+  constexpr int NP = Sched<LOGN>::npass;
+  static_assert(ET % 8 == 0 || N < 8, "each thread must own whole radix-8 butterflies");
+  constexpr int R = Sched<LOGN>::radix(0);
+  constexpr int NBT = ET / R;
+#pragma unroll
+  for (int m = 0; m < NBT; ++m) dftR<R, SIGN>(&v[m * R]);
+  if constexpr (LOAD_SYNC) tile_sync<TX * TPC>();
+  if constexpr (NP == 1) {
+#pragma unroll
+    for (int m = 0; m < NBT; ++m) {
+      const int jb = c + TPC * m;
+#pragma unroll
+      for (int r = 0; r < R; ++r) store(jb * R + r, v[m * R + r]);
+    }
+  } else {
+#pragma unroll
+    for (int m = 0; m < NBT; ++m) {
+      const int jb = c + TPC * m;
+#pragma unroll
+      for (int r = 0; r < R; ++r) s[xidx<PITCH, SWM>(jb * R + r, t)] = v[m * R + r];
+    }
+    tile_sync<TX * TPC>();
+    fft_tile_rest<LOGN, TX, TPC, SIGN, 1, PITCH, STORE_SYNC, SWM>(s, tw, v, t, c, store);
+  }
+}
 
 // load(jb, r) returns the input at position jb + r * N / R0 (R0 the radix of
 // pass 0); r is a constant after unrolling, so a loader can resolve anything
@@ -99,46 +158,19 @@ template <int LOGN, int TX, int TPC, int SIGN, int PITCH = TX, bool LOAD_SYNC = 
 __device__ __forceinline__ void fft_tile(C* __restrict__ s, const C* __restrict__ tw, Load&& load, Store&& store) {
   constexpr int N = 1 << LOGN;
   constexpr int ET = N / TPC;
-  constexpr int NP = Sched<LOGN>::npass;
   constexpr int SWM = Swizzle<PITCH, (int)sizeof(C)>::M;
-  static_assert(ET % 8 == 0 || N < 8, "each thread must own whole radix-8 butterflies");
   const int t = threadIdx.x % TX;
   const int c = threadIdx.x / TX;
   C v[ET > 0 ? ET : 1];
-
-  // ---- pass 0 (Ns = 1): inputs from the loader
-  {
-    constexpr int R = Sched<LOGN>::radix(0);
-    constexpr int NBT = ET / R;
+  constexpr int R = Sched<LOGN>::radix(0);
+  constexpr int NBT = ET / R;
 #pragma unroll
-    for (int m = 0; m < NBT; ++m) {
-      const int jb = c + TPC * m;
+  for (int m = 0; m < NBT; ++m) {
+    const int jb = c + TPC * m;
 #pragma unroll
-      for (int r = 0; r < R; ++r) v[m * R + r] = load(jb, r);   // position jb + r * N / R
-    }
-#pragma unroll
-    for (int m = 0; m < NBT; ++m) dftR<R, SIGN>(&v[m * R]);
-    if constexpr (LOAD_SYNC) __syncthreads();
-    if constexpr (NP == 1) {
-#pragma unroll
-      for (int m = 0; m < NBT; ++m) {
-        const int jb = c + TPC * m;
-#pragma unroll
-        for (int r = 0; r < R; ++r) store(jb * R + r, v[m * R + r]);
-      }
-      return;
-    } else {
-#pragma unroll
-      for (int m = 0; m < NBT; ++m) {
-        const int jb = c + TPC * m;
-#pragma unroll
-        for (int r = 0; r < R; ++r) s[sw<SWM>(jb * R + r) * PITCH + t] = v[m * R + r];
-      }
-      __syncthreads();
-    }
+    for (int r = 0; r < R; ++r) v[m * R + r] = load(jb, r);   // position jb + r * N / R
   }
-  // ---- passes 1 .. NP-1
-  fft_tile_rest<LOGN, TX, TPC, SIGN, 1, PITCH, STORE_SYNC, SWM>(s, tw, v, t, c, store);
+  fft_tile_regs<LOGN, TX, TPC, SIGN, PITCH, LOAD_SYNC, STORE_SYNC, SWM>(s, tw, v, t, c, store);
 }
 
 }  // namespace ss3d

@@ -178,6 +178,15 @@ __global__ void __launch_bounds__(RowCfg<R, LOGN, V>::NTH) k_rows_c2r(Geo g, con
                                          smraw);
 }
 
+// x pass with the rows held in warps (rows_warp_body)
+template <typename R, typename O, int LOGN>
+__global__ void __launch_bounds__(RowWarpCfg<R, LOGN>::NTH)
+    k_rows_warp(Geo g, const cpx_t<R>* __restrict__ in, long long rstride, O* __restrict__ out, long long ostride,
+                int nreal, int nblk_per_r, double* __restrict__ part, Tw tw) {
+  extern __shared__ __align__(16) unsigned char smraw[];
+  rows_warp_body<R, O, LOGN>(g, in, rstride, out, ostride, nreal, nblk_per_r, part, tw, blockIdx.x, smraw);
+}
+
 // npx == 1: the x axis is trivial, x[0] = Re X[0]
 template <typename R, typename O>
 __global__ void k_rows_copy(Geo g, const cpx_t<R>* __restrict__ in, long long rstride, O* __restrict__ out,
@@ -454,6 +463,25 @@ static cudaError_t run_rows_c2r_v(const Geo& g, const cpx_t<R>* in, long long rs
   return cudaGetLastError();
 }
 
+// row pass variant 4: rows held in warps, for the lengths RowWarpCfg covers
+template <typename R, typename O, int L>
+static cudaError_t run_rows_warp(const Geo& g, const cpx_t<R>* in, long long rstride, O* out, long long ostride,
+                                 int nreal, double* part, int* nblk_out, Tw tw, cudaStream_t st) {
+  using W = RowWarpCfg<R, L>;
+  if constexpr (!W::ok) {
+    return run_rows_c2r_v<R, O, L, 0>(g, in, rstride, out, ostride, nreal, part, nblk_out, tw, st);
+  } else {
+    cudaError_t e = set_smem(k_rows_warp<R, O, L>, W::smem);
+    if (e != cudaSuccess) return e;
+    int nblk = (g.ny * g.nz + W::ROWS - 1) / W::ROWS;
+    if (nblk_out) *nblk_out = nblk;
+    k_rows_warp<R, O, L><<<(unsigned)((long long)nblk * nreal), W::NTH, W::smem, st>>>(g, in, rstride, out, ostride,
+                                                                                    nreal, nblk, part, tw);
+    ++g_launch_count;
+    return cudaGetLastError();
+  }
+}
+
 // variants are compiled for transform lengths 32..1024; other lengths use variant 0
 constexpr bool tuned_len(int L) { return L >= 5 && L <= 10; }
 template <typename R> constexpr int prec_index() { return sizeof(R) == 4 ? 1 : 0; }
@@ -512,6 +540,7 @@ static cudaError_t run_rows_c2r(const Geo& g, const cpx_t<R>* in, long long rstr
       case 1: return run_rows_c2r_v<R, O, L, 1>(g, in, rstride, out, ostride, nreal, part, nblk_out, tw, st);
       case 2: return run_rows_c2r_v<R, O, L, 2>(g, in, rstride, out, ostride, nreal, part, nblk_out, tw, st);
       case 3: return run_rows_c2r_v<R, O, L, 3>(g, in, rstride, out, ostride, nreal, part, nblk_out, tw, st);
+      case 4: return run_rows_warp<R, O, L>(g, in, rstride, out, ostride, nreal, part, nblk_out, tw, st);
       default: break;
     }
   }
@@ -537,6 +566,12 @@ int realize_part_blocks(const Geo& g, bool dbl) {
   if (g.npx == 1) return (g.ny * g.nz + NT - 1) / NT;
   int L = ilog2(g.npx) - 1;
   int v = tuned_len(L) ? g_variant[2][dbl ? 0 : 1][L] : 0;
+  if (v == 4 && L >= 3 && L <= (dbl ? 8 : 9)) {   // RowWarpCfg
+    const int tpc = (1 << L) / (L > 8 ? 16 : 8);      // lanes per row
+    const int rows = 8 * (tpc >= 32 ? 1 : 32 / tpc);  // rows per block
+    return (g.ny * g.nz + rows - 1) / rows;
+  }
+  if (v == 4) v = 0;
   int E = (dbl ? 4096 : 8192) >> ((v >> 1) & 1);
   int tx = std::min(64, std::max(1, E >> L));
   return (g.ny * g.nz + tx - 1) / tx;

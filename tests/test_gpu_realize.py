@@ -154,14 +154,14 @@ def test_tile_variants_give_identical_results(gpu):
     sp = gpu.Spectrum(sts, nug, d, n, ipad)
     for prec in (gpu.FP32, gpu.FP64):
         ref = sp.realize(77, 2, 1, prec)
-        for v in (1, 2, 3):
+        for v in (1, 2, 3, 4):
             for kind, logn in ((0, 7), (1, 5), (2, 6)):
-                assert L.ss3d_set_variant(kind, prec, logn, v) == 0
+                assert L.ss3d_set_variant(kind, prec, logn, v if kind == 2 or v < 4 else 0) == 0
             assert np.array_equal(sp.realize(77, 2, 1, prec), ref)
         for kind, logn in ((0, 7), (1, 5), (2, 6)):
             L.ss3d_set_variant(kind, prec, logn, 0)
     chosen = gpu.autotune(sp, 1, gpu.FP32, 2)
-    assert chosen["row_pass"] in {0, 1, 2, 3} and set(chosen.values()) <= set(range(8))
+    assert chosen["row_pass"] in {0, 1, 2, 3, 4} and set(chosen.values()) <= set(range(8))
     assert np.array_equal(sp.realize(77, 2, 1, gpu.FP32), sp.realize(77, 2, 1, gpu.FP32))
 
 
@@ -203,8 +203,34 @@ def test_two_line_variants_identical(gpu, n, ipad, igauss):
     finally:
         for kind, lg in kinds:
             L.ss3d_set_variant(kind, gpu.FP32, lg, 0)
-    assert L.ss3d_set_variant(2, gpu.FP32, 6, 4) != 0      # the row pass has no two-line tiles
+    assert L.ss3d_set_variant(2, gpu.FP32, 6, 5) != 0      # the row pass has no two-line tiles
     assert L.ss3d_set_variant(0, gpu.FP32, 6, 8) != 0
+
+
+@pytest.mark.parametrize("prec", ["FP32", "FP64"])
+@pytest.mark.parametrize("n", [(40, 36, 20), (256, 3, 2), (33, 17, 1), (100, 1, 30), (101, 3, 5), (200, 9, 7),
+                               (600, 2, 1)])
+def test_row_warp_variant_identical(gpu, n, prec):
+    """Row pass variant 4 (each row in the registers of one warp, packing by
+    shuffles) gives the bits of the shared-memory row tiles, for odd and even
+    nx, row counts that leave a block partly empty, row lengths 32..512, and
+    the same mean / variance table."""
+    from specsim3d_b200 import _lib
+    L = _lib.lib()
+    P = getattr(gpu, prec)
+    sts = [(1, 0.9, 12.0, 7.0, 4.0, 20.0, 0.0, 0.0)]
+    sp = gpu.Spectrum(sts, 0.1, (1.0, 1.0, 1.0), n, 1)
+    lg = int(sp.np[0]).bit_length() - 2                 # log2 of the row transform length npx/2
+    if not 5 <= lg <= 10:
+        pytest.skip("row length outside the tuned range")
+    ref, zref = sp.realize(99, 3, 1, P, dtype=np.float32, zstats=True)
+    try:
+        assert L.ss3d_set_variant(2, P, lg, 4) == 0
+        got, zgot = sp.realize(99, 3, 1, P, dtype=np.float32, zstats=True)
+    finally:
+        L.ss3d_set_variant(2, P, lg, 0)
+    assert np.array_equal(got, ref), float(np.max(np.abs(got - ref)))
+    assert np.allclose(zgot, zref, rtol=1e-12, atol=1e-12)
 
 
 @pytest.mark.parametrize("case", [0, 1, 2])
