@@ -652,7 +652,8 @@ extern "C" int ss3d_batch_autotune(ss3d_batch* b) {
   for (int k : {1, 0, 2}) {
     int bestv = 0;
     float bestk = 1e30f;
-    for (int v = 0; v < (k == 2 ? 4 : 8) && e == cudaSuccess; v++) {   // 4-7: two-line column tiles
+    // column passes 4-7: two-line tiles; row pass 4: rows held in warps
+    for (int v = 0; v < (k == 2 ? 5 : 8) && e == cudaSuccess; v++) {
       for (int L = 0; L < 16; L++)
         if (used[k][L]) b->var[k][L] = v;
       e = time_run(b, st, ms, true);
