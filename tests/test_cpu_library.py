@@ -117,3 +117,29 @@ def test_gpu_calls_without_gpu_report_cuda_error():
     import specsim3d_b200 as ss
     with pytest.raises(ss.SpecsimError):
         ss.Spectrum([(1, 1.0, 5, 5, 5, 0, 0, 0)], 0.0, (1, 1, 1), (8, 8, 8), 1)
+
+
+def test_variant_selection_ranges():
+    """ss3d_set_variant (host only): 0-3 for every pass; 4-7 for the FP32 column
+    passes (two lines per thread); 4 for the row pass in both precisions (rows
+    held in warps); anything else is refused."""
+    from specsim3d_b200 import _lib
+    import specsim3d_b200 as ss
+    L = _lib.lib()
+    try:
+        for prec in (ss.FP32, ss.FP64):
+            for kind in (0, 1, 2):
+                for v in range(4):
+                    assert L.ss3d_set_variant(kind, prec, 8, v) == 0
+            assert L.ss3d_set_variant(2, prec, 8, 4) == 0
+            assert L.ss3d_set_variant(2, prec, 8, 5) != 0
+            assert L.ss3d_set_variant(0, prec, 8, -1) != 0
+            assert L.ss3d_set_variant(3, prec, 8, 0) != 0
+        for kind in (0, 1):
+            assert L.ss3d_set_variant(kind, ss.FP32, 8, 7) == 0
+            assert L.ss3d_set_variant(kind, ss.FP32, 8, 8) != 0
+            assert L.ss3d_set_variant(kind, ss.FP64, 8, 4) != 0
+    finally:
+        for prec in (ss.FP32, ss.FP64):
+            for kind in (0, 1, 2):
+                L.ss3d_set_variant(kind, prec, 8, 0)
