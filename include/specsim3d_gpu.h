@@ -110,6 +110,9 @@ int ss3d_spectrum_amp(const ss3d_spectrum *sp, double *amp);
  *   zstats     NULL or 3*nreal doubles: mean, variance, max|Im| per realization
  *              (the line printed at f90:1343-1344; max|Im| is 0 because the
  *              Hermitian half-spectrum inverse is real by construction). */
+/*   A device out must belong to the spectrum's device and, when nx is even,
+ *   start on a multiple of twice the element size (rows are stored as pairs);
+ *   otherwise SS3D_EINVAL before any work.  Host out has no alignment rule. */
 int ss3d_realize(const ss3d_spectrum *sp, int iseed, int64_t r_first, int nreal, int igauss, int precision,
                  void *out, int out_dtype, double *zstats);
 
@@ -137,11 +140,14 @@ int ss3d_debug_coefficients(const ss3d_spectrum *sp, int iseed, int64_t r, int i
  * lives in one fixed array of SS3D_NOALLOC_SCRATCH_BYTES that every GPU loading
  * the library holds until exit.  A call needs about nz * npy * (npx/2 + 2) * 8
  * bytes (FP32; 16 for FP64; nz is replaced by 1 when npz = 1) plus 0.5 MB of
- * tables: a 128^3 grid on its 256^3 periodic grid fits, the 256^3 grid on 512^3
- * does not.  Larger grids are rejected with SS3D_ETOOLARGE and a message giving
- * the bytes needed.  out must be device memory.  The first call on a device copies the
- * constant tables into the array: make it before any stream capture.  Every call
- * shares and overwrites the one array, so calls that overlap on the GPU race. */
+ * tables: a 128^3 grid on its 256^3 periodic grid fits in FP32 (34 MB) but is
+ * refused in FP64 (68 MB); the 256^3 grid on 512^3 is refused in both.  Refused
+ * grids return SS3D_ETOOLARGE and a message giving the bytes needed.  out must
+ * be device memory of the spectrum's device, which must be the current device
+ * (SS3D_EINVAL otherwise, before any work).  The first call on a device copies
+ * the constant tables into the array and synchronises the device: make that
+ * first call before any stream capture begins.  Every call shares and
+ * overwrites the one array, so calls that overlap on the GPU race. */
 #define SS3D_NOALLOC_SCRATCH_BYTES (64u << 20)
 int ss3d_realize_noalloc(const ss3d_spectrum *sp, int iseed, int64_t r_first, int nreal, int igauss, int precision,
                          void *out, int out_dtype);

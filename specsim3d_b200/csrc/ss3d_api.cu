@@ -160,6 +160,10 @@ int get_ctx(DevCtx** out) {
     CK(cudaMemcpy(c.twf, hf.data(), sizeof(float2) * ntw, cudaMemcpyHostToDevice));
     CK(cudaMemcpy(c.twd, hd.data(), sizeof(double2) * ntw, cudaMemcpyHostToDevice));
     CK(cudaMemcpy(c.ptab, ht.data(), sizeof(uint32_t) * 3 * 2048, cudaMemcpyHostToDevice));
+    // a copy from pageable memory may return before its DMA ends, and the
+    // kernels that read the tables can run on non-blocking streams that do not
+    // order behind the legacy stream: wait for the copies once, here
+    CK(cudaDeviceSynchronize());
     // Spectra, work spaces and temporaries come from the device's
     // stream-ordered pool.  Freed pool memory stays mapped (release threshold
     // unlimited): mapping device pages costs about a millisecond per few MB
@@ -178,14 +182,25 @@ int get_ctx(DevCtx** out) {
   return SS3D_OK;
 }
 
-bool is_device_ptr(const void* p) {
+}  // namespace
+
+int ss3d::check_ptr(const void* p, int dev, size_t align, const char* what, bool* is_dev) {
+  *is_dev = false;
   cudaPointerAttributes a;
   if (cudaPointerGetAttributes(&a, p) != cudaSuccess) {
     cudaGetLastError();
-    return false;
+    return SS3D_OK;   // memory CUDA does not know: ordinary host memory
   }
-  return a.type == cudaMemoryTypeDevice || a.type == cudaMemoryTypeManaged;
+  if (a.type != cudaMemoryTypeDevice && a.type != cudaMemoryTypeManaged) return SS3D_OK;
+  *is_dev = true;
+  if (a.type == cudaMemoryTypeDevice && a.device != dev)
+    return fail(SS3D_EINVAL, "%s is memory of device %d, the work runs on device %d", what, a.device, dev);
+  if (align > 1 && ((uintptr_t)p % align) != 0)
+    return fail(SS3D_EINVAL, "%s must start on a multiple of %zu bytes (device memory at %p)", what, align, p);
+  return SS3D_OK;
 }
+
+namespace {
 
 // ---------------------------------------------------------------- model
 const double PI = 3.14159265358979323846;  // f90:92
@@ -625,14 +640,16 @@ extern "C" int ss3d_realize(const ss3d_spectrum* csp, int iseed, int64_t r_first
   const char* ax = "";
   if (!supported_axes(g, dbl, &ax))
     return fail(SS3D_ETOOLARGE, "periodic axis %s longer than the supported transform length", ax);
+  // the tables of the spectrum's device: make it current before taking them
+  CK(cudaSetDevice(sp->dev));
   DevCtx* ctx;
   int rc;
   if ((rc = get_ctx(&ctx))) return rc;
-  CK(cudaSetDevice(sp->dev));
   cudaStream_t s = g_stream;
-  const bool dev_out = is_device_ptr(out);
   const size_t M = (size_t)g.nx * g.ny * g.nz;
   const size_t oel = out_dtype == SS3D_OUT_F32 ? 4 : 8;
+  bool dev_out = false;
+  if ((rc = check_ptr(out, sp->dev, (g.nx % 2 == 0 ? 2 : 1) * oel, "out", &dev_out))) return rc;
   const RealizeLayout lay = realize_layout(g, dbl, dev_out, nreal, oel);
   const int bt = lay.bt;
   void* wsp = nullptr;
@@ -828,6 +845,7 @@ int ss3d::set_error(int code, const char* msg) { return fail(code, "%s", msg); }
 cudaStream_t ss3d::current_stream() { return g_stream; }
 int ss3d::spectrum_view(const ss3d_spectrum* sp, NoallocView* v) {
   if (!sp || !sp->amp32 || !sp->amp64) return 1;
+  v->dev = sp->dev;
   v->geo = sp->geo;
   v->amp64 = sp->amp64;
   v->amp32 = sp->amp32;

@@ -466,6 +466,15 @@ extern "C" int ss3d_batch_create(const ss3d_batch_job* jobs, int njobs, ss3d_bat
                                     "igauss not 0/1, or spectrum of another device)");
     }
     const Geo& g = J.g;
+    bool dev_out = false;
+    if (int rc = check_ptr(q.out, b->dev, g.nx % 2 == 0 ? 8 : 4, "batch job output", &dev_out)) {
+      ss3d_batch_free(b);
+      return rc;
+    }
+    if (!dev_out) {
+      ss3d_batch_free(b);
+      return set_error(SS3D_EINVAL, "batch job output must be device memory");
+    }
     J.amp = amp32;
     J.nreal = q.nreal;
     J.out = q.out;

@@ -716,10 +716,10 @@ extern "C" int ss3d_condition(double* res, const int n[3], int nreal, const doub
   // ---- device work
   cudaStream_t stm = current_stream();
   const long long M = (long long)nx * ny * nz;
-  cudaPointerAttributes pa;
-  const bool dev_res = cudaPointerGetAttributes(&pa, res) == cudaSuccess &&
-                       (pa.type == cudaMemoryTypeDevice || pa.type == cudaMemoryTypeManaged);
-  cudaGetLastError();
+  int cur_dev = 0;
+  if (cudaGetDevice(&cur_dev) != cudaSuccess) return set_error(SS3D_ECUDA, "no current CUDA device");
+  bool dev_res = false;
+  if (int rc = check_ptr(res, cur_dev, sizeof(double), "res", &dev_res)) return rc;
   DevBuf bufs(stm);
   double* dres = res;
   cudaError_t e = cudaSuccess;

@@ -96,11 +96,19 @@ int realize_part_blocks(const Geo& g, bool dbl);
 
 // ---- helpers of the allocation-free entry point (ss3d_api.cu)
 struct NoallocView {
+  int dev;              // device that holds the amplitudes
   Geo geo;
   const double* amp64;
   const float* amp32;
 };
 int set_error(int code, const char* msg);     // sets the message returned by ss3d_last_error
+// Where caller memory p lives.  *is_dev becomes true for device (or managed)
+// memory, false for host memory (pageable or pinned), which the library only
+// reaches through copies.  Device memory must belong to device `dev` and start
+// on a multiple of `align` bytes (the kernels store 2-element vectors into
+// output rows of even length); otherwise SS3D_EINVAL with a message naming
+// `what`, before any work is issued.
+int check_ptr(const void* p, int dev, size_t align, const char* what, bool* is_dev);
 void setrot_public(const ss3d_struct& s, double rot[3][3], double axes[3][3]);
 void model_public(const ss3d_struct* st, int nst, double nugget, Model& m);
 cudaStream_t current_stream();                // stream selected with ss3d_set_stream

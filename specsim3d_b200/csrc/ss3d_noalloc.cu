@@ -15,13 +15,16 @@
 // Limits and rules:
 //  * the scratch array is SS3D_NOALLOC_SCRATCH_BYTES (64 MiB); one call needs
 //    about nz * npy * (npx/2 + 2) * 8 bytes (FP32, 16 for FP64) plus 0.5 MB of
-//    tables, so a 128^3 grid on its 256^3 periodic grid fits and the 256^3 grid
-//    on 512^3 does not; a grid that does not fit is rejected with
-//    SS3D_ETOOLARGE and a message giving the bytes it would need;
-//  * out must be device memory (host pointers are rejected);
+//    tables.  A 128^3 grid on its 256^3 periodic grid fits in FP32 (34 MB) but
+//    not in FP64 (68 MB), and the 256^3 grid on 512^3 fits in neither; a grid
+//    that does not fit is rejected with SS3D_ETOOLARGE and a message giving
+//    the bytes it would need;
+//  * out must be device memory of the device that holds the spectrum, which
+//    must also be the current device (host pointers and other devices are
+//    rejected with SS3D_EINVAL before any work is issued);
 //  * the first call on a device fills the twiddle and jump-ahead tables of the
-//    array for that device (a plain host-to-device copy); make that first call
-//    before any stream capture;
+//    array for that device (a host-to-device copy followed by a device
+//    synchronisation); make that first call before any stream capture begins;
 //  * every call shares the one array and overwrites it: calls that overlap on
 //    the GPU (two host threads, or two streams) race and corrupt each other.
 //    Nothing in the array needs to start at zero: every element a kernel reads
@@ -99,6 +102,10 @@ int setup(int dev, unsigned char** base) {
     e = cudaMemcpy(s + kOffTwF, hf.data(), sizeof(float2) * kTwCount, cudaMemcpyHostToDevice);
     if (e == cudaSuccess) e = cudaMemcpy(s + kOffTwD, hd.data(), sizeof(double2) * kTwCount, cudaMemcpyHostToDevice);
     if (e == cudaSuccess) e = cudaMemcpy(s + kOffPtab, ht.data(), sizeof(uint32_t) * 3 * 2048, cudaMemcpyHostToDevice);
+    // a copy from pageable memory may return before its DMA ends, and the
+    // kernels run on the caller's stream, which need not order behind the
+    // legacy stream: wait for the copies before the first launch
+    if (e == cudaSuccess) e = cudaDeviceSynchronize();
     if (e != cudaSuccess) return fail(SS3D_ECUDA, std::string("scratch table set-up: ") + cudaGetErrorString(e));
     d.base = s;
     d.ready = true;
@@ -120,16 +127,19 @@ extern "C" int ss3d_realize_noalloc(const ss3d_spectrum* sp, int iseed, int64_t 
   if (out_dtype != SS3D_OUT_F32 && out_dtype != SS3D_OUT_F64) return fail(SS3D_EINVAL, "unknown out_dtype");
   if (nreal == 0) return SS3D_OK;
   if (!out) return fail(SS3D_EINVAL, "out is NULL");
-  cudaPointerAttributes pa;
-  if (cudaPointerGetAttributes(&pa, out) != cudaSuccess ||
-      (pa.type != cudaMemoryTypeDevice && pa.type != cudaMemoryTypeManaged)) {
-    cudaGetLastError();
-    return fail(SS3D_EINVAL, "ss3d_realize_noalloc needs a device output pointer");
-  }
   int dev = 0;
   cudaError_t e = cudaGetDevice(&dev);
   if (e != cudaSuccess || dev < 0 || dev >= 64) return fail(SS3D_ECUDA, "no current CUDA device");
+  if (dev != v.dev) {
+    char buf[160];
+    snprintf(buf, sizeof buf, "the spectrum lives on device %d but device %d is current", v.dev, dev);
+    return fail(SS3D_EINVAL, buf);
+  }
   Geo g = v.geo;
+  const size_t oel = out_dtype == SS3D_OUT_F32 ? 4 : 8;
+  bool dev_out = false;
+  if (int rc = check_ptr(out, dev, (g.nx % 2 == 0 ? 2 : 1) * oel, "out", &dev_out)) return rc;
+  if (!dev_out) return fail(SS3D_EINVAL, "ss3d_realize_noalloc needs a device output pointer");
   const bool dbl = precision == SS3D_FP64;
   const int maxl = dbl ? MAX_LOGN_D : MAX_LOGN_F;
   auto lg = [](int n) { int l = 0; while ((1 << l) < n) ++l; return l; };
@@ -166,7 +176,6 @@ extern "C" int ss3d_realize_noalloc(const ss3d_spectrum* sp, int iseed, int64_t 
   int64_t a = iseed < 0 ? -(int64_t)iseed : (int64_t)iseed;
   const uint32_t s0 = (uint32_t)(a % 2147483646LL + 1);
   const size_t M = (size_t)g.nx * g.ny * g.nz;
-  const size_t oel = out_dtype == SS3D_OUT_F32 ? 4 : 8;
   cudaStream_t st = current_stream();
   for (int r = 0; r < nreal && e == cudaSuccess; ++r) {
     e = launch_rowstates(g, s0, r_first + r, 1, ptab, rs, r == 0 ? apow : nullptr, st);

@@ -404,6 +404,15 @@ extern "C" int ss3d_server_submit(ss3d_server* s, const ss3d_request* q, int64_t
     return set_error(SS3D_EINVAL, "conditional requests need cp, rows, nvar and a float64 output");
   int np[3];
   if (int rc = ss3d_grid_size(q->st, q->nst, q->d, q->n, q->ipad, np)) return rc;
+  bool host_out = false;
+  if (!s->dry) {
+    // rejected at submission, not when a slot reaches the request: device
+    // output on another device, or not aligned for the row stores
+    bool dev_out = false;
+    const size_t oel = q->out_dtype == SS3D_OUT_F32 ? 4 : 8;
+    if (int rc = check_ptr(q->out, s->dev, (q->n[0] % 2 == 0 ? 2 : 1) * oel, "out", &dev_out)) return rc;
+    host_out = !dev_out;
+  }
   Req* r = new Req();
   r->st.assign(q->st, q->st + q->nst);
   r->r = *q;
@@ -419,13 +428,6 @@ extern "C" int ss3d_server_submit(ss3d_server* s, const ss3d_request* q, int64_t
   const int64_t M = (int64_t)q->n[0] * q->n[1] * q->n[2];
   r->spec_bytes = nh * (int64_t)(sizeof(double) + sizeof(float)) + (1 << 20);
   r->build_bytes = nh * (int64_t)(2 * sizeof(double)) + (1 << 20);
-  bool host_out = false;
-  if (!s->dry) {
-    cudaPointerAttributes pa;
-    host_out = !(cudaPointerGetAttributes(&pa, q->out) == cudaSuccess &&
-                 (pa.type == cudaMemoryTypeDevice || pa.type == cudaMemoryTypeManaged));
-    cudaGetLastError();
-  }
   r->work_bytes = realize_bytes_for(np, q->n, q->nreal, q->precision, host_out ? 1 : 0);
   if (cond) {
     const int64_t per_node = 4LL * q->cp->ndmax + 4;

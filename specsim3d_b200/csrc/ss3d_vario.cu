@@ -245,13 +245,11 @@ extern "C" int ss3d_vario(const double* res, const int n[3], int nreal, int ndir
   const size_t ngam = (size_t)nlagmax * ndir * nreal;
   if (ngam == 0) return SS3D_OK;
   cudaStream_t st = current_stream();
-  cudaPointerAttributes pa;
-  bool dev_in = cudaPointerGetAttributes(&pa, res) == cudaSuccess &&
-                (pa.type == cudaMemoryTypeDevice || pa.type == cudaMemoryTypeManaged);
-  cudaGetLastError();
-  bool dev_gam = cudaPointerGetAttributes(&pa, gam) == cudaSuccess &&
-                 (pa.type == cudaMemoryTypeDevice || pa.type == cudaMemoryTypeManaged);
-  cudaGetLastError();
+  int cur_dev = 0;
+  if (cudaGetDevice(&cur_dev) != cudaSuccess) return set_error(SS3D_ECUDA, "no current CUDA device");
+  bool dev_in = false, dev_gam = false;
+  if (int rc = check_ptr(res, cur_dev, sizeof(double), "res", &dev_in)) return rc;
+  if (int rc = check_ptr(gam, cur_dev, sizeof(double), "gam", &dev_gam)) return rc;
   const double* fdev = res;
   double* fbuf = nullptr;
   double* gdev = nullptr;

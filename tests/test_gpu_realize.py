@@ -263,3 +263,28 @@ def test_fp32_error_at_full_size(gpu):
         torch.cuda.synchronize()
         err = float((o32.double() - o64).abs().amax().item()) / np.sqrt(sp.stats["c0"])
         assert err <= 1e-5, (igauss, err)
+
+
+def test_misaligned_device_output_is_refused(gpu):
+    """Rows of even length are stored as 2-element vectors: a device output that
+    starts off a pair boundary (a contiguous view at an odd element offset) is
+    refused by ss3d_realize and ss3d_batch_create before any kernel runs, and
+    the memory stays untouched.  Host outputs have no alignment rule."""
+    import torch
+    n, sts, nug, d, ipad = CASES[0]
+    sp = gpu.Spectrum(sts, nug, d, n, ipad)
+    M = n[0] * n[1] * n[2]
+    for dt in (torch.float32, torch.float64):
+        flat = torch.zeros(M + 1, dtype=dt, device="cuda")
+        view = flat[1:].view(1, n[2], n[1], n[0])
+        with pytest.raises(gpu.SpecsimError, match="multiple of"):
+            sp.realize(7, 1, 0, gpu.FP32, out=view)
+        torch.cuda.synchronize()
+        assert float(flat.abs().sum().item()) == 0.0
+    flat = torch.zeros(M + 1, dtype=torch.float32, device="cuda")
+    with pytest.raises(gpu.SpecsimError, match="multiple of"):
+        gpu.Batch([(sp, 7, 0, 0, 1, flat[1:].view(1, n[2], n[1], n[0]))])
+    host = np.zeros(M + 1, dtype=np.float32)
+    got = sp.realize(7, 1, 0, gpu.FP32, out=host[1:].reshape(1, n[2], n[1], n[0]))
+    assert np.array_equal(got, sp.realize(7, 1, 0, gpu.FP32, dtype=np.float32))
+    sp.close()
