@@ -413,6 +413,16 @@ void ora_fill_states(const int np[3], int igauss, int64_t *first_state)
 int ora_realize(const double *amp, const int np[3], const int n[3], int iseed, int nreal, int igauss,
                 double *res, double *zstats)
 {
+    return ora_realize_range(amp, np, n, iseed, 0, nreal, igauss, res, zstats);
+}
+
+/* Realizations r_first+1 .. r_first+nreal (1-based) of the run: the stream is
+ * seeded once (f90:1302-1303) and the fills of the first r_first realizations
+ * are drawn and discarded (f90:1300-1334 without their transforms), so the
+ * draws of every kept realization are those of the full serial run. */
+int ora_realize_range(const double *amp, const int np[3], const int n[3], int iseed, int r_first, int nreal,
+                      int igauss, double *res, double *zstats)
+{
     int npx = np[0], npy = np[1], npz = np[2];
     int nx = n[0], ny = n[1], nz = n[2];
     size_t ntot = (size_t)npx * npy * npz;
@@ -420,6 +430,7 @@ int ora_realize(const double *amp, const int np[3], const int n[3], int iseed, i
     double *c = malloc(sizeof(double) * 2 * ntot);
     if (!c) return 2;
     ora_rng_seed(iseed);
+    for (int r = 0; r < r_first; r++) ora_fill_coefficients(amp, np, igauss, c);
     for (int r = 0; r < nreal; r++) {
         ora_fill_coefficients(amp, np, igauss, c);
         ora_fft3d(c, npx, npy, npz, +1);

@@ -84,6 +84,9 @@ void ora_fill_states(const int np[3], int igauss, int64_t *first_state);
  * (mean, variance, max|Im|). */
 int ora_realize(const double *amp, const int np[3], const int n[3], int iseed, int nreal, int igauss,
                 double *res, double *zstats);
+/* the same for realizations r_first+1 .. r_first+nreal of the serial run */
+int ora_realize_range(const double *amp, const int np[3], const int n[3], int iseed, int r_first, int nreal,
+                      int igauss, double *res, double *zstats);
 
 /* Experimental variogram, f90:394-431 */
 int64_t ora_npair_count(int nx, int ny, int nz, int lx, int ly, int lz);

@@ -359,18 +359,44 @@ __global__ void k_spec_amp(Geo g, const double2* __restrict__ X, double* __restr
   }
 }
 
-__global__ void k_reduce_spec(const SpecPartial* part, int n, SpecPartial* out) {
-  if (threadIdx.x == 0 && blockIdx.x == 0) {
-    SpecPartial p{0, 0, 0, 0};
-    for (int q = 0; q < n; ++q) {
-      p.maximag = fmax(p.maximag, part[q].maximag);
-      p.maxreal = fmax(p.maxreal, part[q].maxreal);
-      p.spos += part[q].spos;
-      p.sneg += part[q].sneg;
-    }
-    *out = p;
+// Sum of the per-block partials in a fixed order, independent of scheduling:
+// one block of RS_NT threads; thread t combines partials t, t + RS_NT, ... in
+// index order, then each warp folds its lanes by halving distances, and warp 0
+// folds the warp results the same way.
+constexpr int RS_NT = 1024;
+__device__ __forceinline__ void spec_combine(SpecPartial& a, const SpecPartial& b) {
+  a.maximag = fmax(a.maximag, b.maximag);
+  a.maxreal = fmax(a.maxreal, b.maxreal);
+  a.spos += b.spos;
+  a.sneg += b.sneg;
+}
+__device__ __forceinline__ void spec_warp_fold(SpecPartial& p) {
+#pragma unroll
+  for (int off = 16; off > 0; off >>= 1) {
+    SpecPartial o;
+    o.maximag = __shfl_down_sync(0xffffffffu, p.maximag, off);
+    o.maxreal = __shfl_down_sync(0xffffffffu, p.maxreal, off);
+    o.spos = __shfl_down_sync(0xffffffffu, p.spos, off);
+    o.sneg = __shfl_down_sync(0xffffffffu, p.sneg, off);
+    spec_combine(p, o);
   }
 }
+__global__ void __launch_bounds__(RS_NT) k_reduce_spec(const SpecPartial* __restrict__ part, int n,
+                                                       SpecPartial* out) {
+  __shared__ SpecPartial red[RS_NT / 32];
+  SpecPartial p{0, 0, 0, 0};
+  for (int q = threadIdx.x; q < n; q += RS_NT) spec_combine(p, part[q]);
+  spec_warp_fold(p);
+  const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
+  if (lane == 0) red[warp] = p;
+  __syncthreads();
+  if (warp == 0) {
+    p = red[lane];   // RS_NT / 32 == 32 warp results
+    spec_warp_fold(p);
+    if (lane == 0) *out = p;
+  }
+}
+static_assert(RS_NT / 32 == 32, "warp 0 folds one result per warp");
 
 // ---------------------------------------------------------------- launch helpers
 static int ilog2(int n) {
@@ -628,7 +654,7 @@ cudaError_t launch_spectrum(const Model& m, const double d[3], const Geo& g, dou
   k_spec_amp<<<nb, NT, 0, st>>>(g, work, amp64, amp32, part);
   ++g_launch_count;
   if ((e = cudaGetLastError()) != cudaSuccess) return e;
-  k_reduce_spec<<<1, 32, 0, st>>>(part, nb, result);
+  k_reduce_spec<<<1, RS_NT, 0, st>>>(part, nb, result);
   ++g_launch_count;
   return cudaGetLastError();
 }

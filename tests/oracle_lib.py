@@ -109,6 +109,18 @@ def realize(amp, np3, n, iseed, nreal, igauss):
     return res, zs
 
 
+def realize_range(amp, np3, n, iseed, r_first, nreal, igauss):
+    """Realizations r_first..r_first+nreal-1 (0-based) of the serial run of seed
+    iseed: the earlier fills are drawn and discarded, as the serial stream does."""
+    res = np.zeros((nreal, n[2], n[1], n[0]))
+    zs = np.zeros((nreal, 3))
+    rc = lib().ora_realize_range(ctypes.c_void_p(amp.ctypes.data), _i3(np3), _i3(n), int(iseed), int(r_first),
+                                 int(nreal), int(igauss), ctypes.c_void_p(res.ctypes.data),
+                                 ctypes.c_void_p(zs.ctypes.data))
+    assert rc == 0
+    return res, zs
+
+
 def fill_states(np3, iseed, nreal, igauss):
     """First-draw states (nreal, npz, npy, npx) of the sequential stream (0 = no draw)."""
     lib().ora_rng_seed(ctypes.c_int(iseed))

@@ -117,3 +117,62 @@ def test_no_data_inside_grid(gpu):
     res = np.zeros((1, 4, 4, 4))
     with pytest.raises(gpu.SpecsimError, match="no conditioning data"):
         gpu.condition(res, (0, 0, 0), (1, 1, 1), [(1, 1.0, 5, 5, 5, 0, 0, 0)], 0.0, _gpu_params(_params()), rows)
+
+
+@pytest.mark.parametrize("precision", [0, 1])
+def test_conditional_tables_fig12_fig13_gpu(gpu, precision):
+    """The reference's seeded conditional tables (fig12 SPECSIM3D row, fig13)
+    through the CUDA path, to every printed digit: FP64 realizations, kriging
+    in FP64 or in the precision form (FP32 solves + one FP64 refinement)."""
+    import json
+    import os
+    import recipes
+    pins = json.load(open(os.path.join(os.path.dirname(__file__), "golden", "reference_pins.json")))
+    c = recipes.COND
+    sp = gpu.Spectrum(c["structs"], c["nugget"], c["d"], c["n"], c["ipad"])
+
+    def realize(seed, nreal):
+        return sp.realize(seed, nreal, 0, gpu.FP64)
+
+    def condition(res, p, rows):
+        st, _ = gpu.condition(res, (0.0, 0.0, 0.0), c["d"], c["structs"], c["nugget"], p, rows, precision=precision)
+        assert st["nd"] == len(rows)
+
+    got = recipes.conditional_tables(realize, condition)
+    sp.close()
+    want12 = {k: v for k, v in pins["fig12"].items() if k not in ("code", "nreal", "seconds_per_realization")}
+    assert got["fig12"] == want12
+    assert got["fig13"] == pins["fig13"]
+
+
+@pytest.mark.parametrize("precision,tol", [(0, 1e-9), (1, 1e-5)])
+def test_conditional_config_full_size(gpu, precision, tol):
+    """The conditional configuration at full size against the oracle:
+    128x128x64, exponential 40/20/8 N60E, nugget 0.05; truth = realization 1 of
+    seed 4242 (igauss 0); 2,000 data at default_rng(99) uniform locations with
+    values exp(0.5 z) of the truth; nscore + back transform (zmax = 2 max, linear
+    tails); search = the ranges, ndmax 24; 16 realizations of seed 4243.  The
+    search statistics (neighbours, exact data nodes, empty nodes, regularised
+    systems) are equal; the fields agree to 1e-9 (FP64) or 1e-5 of their
+    standard deviation (precision form).  On a lattice the integer distance
+    ties of the insertion rule are common: this is where they would show."""
+    n = (128, 128, 64)
+    sts = [(2, 1.0, 40.0, 20.0, 8.0, 60.0, 0.0, 0.0)]
+    sp = gpu.Spectrum(sts, 0.05, (1, 1, 1), n, 1)
+    truth = sp.realize(4242, 1, 0, gpu.FP64)[0]
+    rng = np.random.default_rng(99)
+    pts = np.stack([rng.uniform(0, n[a] - 1, 2000) for a in range(3)], axis=1)
+    ii = np.rint(pts).astype(int)
+    val = np.exp(0.5 * truth[ii[:, 2], ii[:, 1], ii[:, 0]])
+    rows = np.c_[pts, val]
+    p = _params(itrans=1, zlo=0.0, zhi=2 * float(val.max()), rmax=40.0, rmed=20.0, rvert=8.0, sa1=60.0, ndmax=24)
+    res = sp.realize(4243, 16, 0, gpu.FP64)
+    sp.close()
+    a = res.copy()
+    b = res.copy()
+    st_o, ex_o = ora.condition(a, (0, 0, 0), (1, 1, 1), sts, 0.05, p, rows)
+    st_g, ex_g = gpu.condition(b, (0, 0, 0), (1, 1, 1), sts, 0.05, _gpu_params(p), rows, precision=precision)
+    _check_stats(st_o, st_g)
+    assert np.array_equal(ex_o["vrt"], ex_g["vrt"])
+    err = np.max(np.abs(a - b)) / float(np.std(a))
+    assert err <= tol, err

@@ -133,3 +133,28 @@ def test_oracle_vario_matches_numpy():
     for k, (sx, sy, sz, nl) in enumerate(dirs):
         g, _ = recipes.vario_shift(fx, (sx, sy, sz), nl)
         assert np.allclose(gam[:, k, :g.shape[1]], g, rtol=1e-12, atol=1e-14)
+
+
+def test_conditional_tables_fig12_fig13():
+    """fig12_conditional_validation.csv (SPECSIM3D row) and
+    fig13_conditional_nscore.csv reproduced to every printed digit: the
+    reference's seeded conditional recipe (truth of seed 2024, 150 data nodes of
+    default_rng(7), 200 realizations of seed 777 kriged with itrans 0; 50 of
+    seed 99 through nscore and back transform) run through the oracle's
+    search, kriging and transforms."""
+    c = recipes.COND
+    np3, _ = ora.grid(c["structs"], c["d"], c["n"], c["ipad"])
+    amp, _ = ora.spectrum(c["structs"], c["nugget"], c["d"], np3)
+
+    def realize(seed, nreal):
+        return ora.realize(amp, np3, c["n"], seed, nreal, 0)[0]
+
+    def condition(res, p, rows):
+        st, _ = ora.condition(res, (0.0, 0.0, 0.0), c["d"], c["structs"], c["nugget"],
+                              recipes.oracle_cond_params(p), rows)
+        assert st["rc"] == 0 and st["nd"] == len(rows)
+
+    got = recipes.conditional_tables(realize, condition)
+    want12 = {k: v for k, v in PINS["fig12"].items() if k not in ("code", "nreal", "seconds_per_realization")}
+    assert got["fig12"] == want12
+    assert got["fig13"] == PINS["fig13"]
