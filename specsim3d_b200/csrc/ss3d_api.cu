@@ -380,6 +380,37 @@ struct Workspace {
 };
 thread_local Workspace g_ws[64];
 
+// Copy stream and events of the host-output path, per host thread and device,
+// created on first use and kept (creating them per call costs a few
+// microseconds each and serialises with other threads' launches).
+struct CopyCtx {
+  cudaStream_t cs = nullptr;
+  cudaEvent_t done[2] = {nullptr, nullptr};
+  cudaEvent_t ready = nullptr;
+  int dev = -1;
+  ~CopyCtx() {
+    if (dev < 0) return;
+    cudaSetDevice(dev);
+    if (cs) cudaStreamDestroy(cs);
+    for (cudaEvent_t ev : {done[0], done[1], ready})
+      if (ev) cudaEventDestroy(ev);
+  }
+};
+thread_local CopyCtx g_copy[64];
+
+int copy_ctx(int dev, CopyCtx** out) {
+  CopyCtx& c = g_copy[dev];
+  if (c.dev < 0) {
+    CK(cudaStreamCreateWithFlags(&c.cs, cudaStreamNonBlocking));
+    CK(cudaEventCreateWithFlags(&c.done[0], cudaEventDisableTiming));
+    CK(cudaEventCreateWithFlags(&c.done[1], cudaEventDisableTiming));
+    CK(cudaEventCreateWithFlags(&c.ready, cudaEventDisableTiming));
+    c.dev = dev;
+  }
+  *out = &c;
+  return SS3D_OK;
+}
+
 int ws_reserve(int dev, size_t bytes, void** ptr) {
   if (dev < 0 || dev >= 64) return fail(SS3D_EINVAL, "device ordinal %d out of range", dev);
   Workspace& w = g_ws[dev];
@@ -554,6 +585,13 @@ RealizeLayout realize_layout(const Geo& g, bool dbl, bool dev_out, int nreal, si
   const size_t per_real = L.per_work + (dev_out ? 0 : 2 * M * oel) + (size_t)g.npy * g.npz * 4 + (size_t)nbx * 16;
   L.bt = (int)std::min<size_t>((size_t)std::max(nreal, 1), std::max<size_t>(1, budget / per_real));
   L.bt = std::min(L.bt, 16);
+  if (!dev_out) {
+    // host output: chunks of about 32 MB, so that the copy of chunk b to the
+    // host (PCIe, several times slower than the kernels) overlaps the kernels
+    // of chunk b + 1 instead of waiting for the whole batch
+    const size_t chunk = std::max<size_t>(1, ((size_t)32 << 20) / std::max<size_t>(1, M * oel));
+    L.bt = (int)std::min<size_t>((size_t)L.bt, chunk);
+  }
   L.off_work = 0;
   L.off_rs = align256(L.off_work + L.per_work * L.bt);
   L.off_apow = align256(L.off_rs + (size_t)g.npy * g.npz * 4 * L.bt);
@@ -664,12 +702,19 @@ extern "C" int ss3d_realize(const ss3d_spectrum* csp, int iseed, int64_t r_first
   const long long wstride = (long long)work_planes(g) * g.npy * g.HP;
   const uint32_t s0 = seed0(iseed);
   Tw tw{ctx->twf, ctx->twd};
-  cudaEvent_t done[2] = {nullptr, nullptr};
+  cudaEvent_t* done = nullptr;
+  cudaEvent_t ready = nullptr;
   cudaStream_t cs = nullptr;
   if (!dev_out) {
-    CK(cudaStreamCreateWithFlags(&cs, cudaStreamNonBlocking));
-    CK(cudaEventCreateWithFlags(&done[0], cudaEventDisableTiming));
-    CK(cudaEventCreateWithFlags(&done[1], cudaEventDisableTiming));
+    CopyCtx* cc = nullptr;
+    if ((rc = copy_ctx(sp->dev, &cc))) return rc;
+    cs = cc->cs;
+    done = cc->done;
+    ready = cc->ready;
+    // the previous call's copies ended before it returned; order this call's
+    // first chunks after them all the same (the events are reused)
+    CK(cudaStreamWaitEvent(s, done[0], 0));
+    CK(cudaStreamWaitEvent(s, done[1], 0));
   }
   cudaError_t e = cudaSuccess;
   Marks marks;
@@ -695,15 +740,12 @@ extern "C" int ss3d_realize(const ss3d_spectrum* csp, int iseed, int64_t r_first
     if (e == cudaSuccess && zstats) e = launch_reduce_zstats(part, nblk, nb, zs + 2 * (size_t)r0, s);
     mark(&marks, -1, s);
     if (e == cudaSuccess && !dev_out) {
-      cudaEvent_t ready;
-      e = cudaEventCreateWithFlags(&ready, cudaEventDisableTiming);
-      if (e == cudaSuccess) e = cudaEventRecord(ready, s);
+      e = cudaEventRecord(ready, s);
       if (e == cudaSuccess) e = cudaStreamWaitEvent(cs, ready, 0);
       if (e == cudaSuccess)
         e = cudaMemcpyAsync((char*)out + (size_t)r0 * M * oel, stage[slot], (size_t)nb * M * oel,
                             cudaMemcpyDeviceToHost, cs);
       if (e == cudaSuccess) e = cudaEventRecord(done[slot], cs);
-      cudaEventDestroy(ready);
     }
   }
   std::vector<double> hz;
@@ -714,11 +756,6 @@ extern "C" int ss3d_realize(const ss3d_spectrum* csp, int iseed, int64_t r_first
   if (e == cudaSuccess) e = cudaStreamSynchronize(s);
   if (e == cudaSuccess && cs) e = cudaStreamSynchronize(cs);
   if (marks.on) marks_collect(marks);
-  if (cs) {
-    cudaStreamDestroy(cs);
-    cudaEventDestroy(done[0]);
-    cudaEventDestroy(done[1]);
-  }
   if (e != cudaSuccess) return cuda_fail(e, "realize");
   if (zstats) {
     for (int r = 0; r < nreal; r++) {

@@ -44,7 +44,7 @@ __host__ __device__ inline int cond_ld(int ndmax) { return ndmax | 1; }
 // bytes.
 __host__ __device__ inline size_t cond_warp_bytes(int ndmax, int prec) {
   const size_t n = (size_t)ndmax, m = (n + 1) * (size_t)cond_ld(ndmax);
-  const size_t b = prec == 0 ? m * 8 + n * 32 + n * 4 : m * 12 + n * 24 + n * 16 + n * 4;
+  const size_t b = (prec == 0 ? m * 8 + n * 32 + n * 4 : m * 12 + n * 24 + n * 16 + n * 4) + n * 12;
   return (b + 15) & ~(size_t)15;
 }
 
@@ -88,6 +88,40 @@ __device__ __forceinline__ double cov_k(const KModel& m, double dx, double dy, d
     }
   }
   return c;
+}
+
+// Covariance of integer lattice lags.  Data are snapped to nodes (f90:789-792,
+// 826), so every entry of a kriging system is C(di dx, dj dy, dk dz) for an
+// integer lag (di, dj, dk): the difference of two data nodes or of a data node
+// and the node kriged.  Both lie inside the search ellipsoid around the node,
+// so |di| <= 2 e_x / dx (e_x the half-extent of the ellipsoid along x), and so
+// on.  The table holds C over that box for dk >= 0 (C(-h) = C(h)), built once
+// per call; a lag outside it (or no table, when the box is too large) is
+// evaluated directly.
+struct CovTab {
+  const double* v;   // [dk][dj + ty][di + tx], dk in [0, tz]; NULL: no table
+  int tx, ty, tz;
+};
+__device__ __forceinline__ double cov_lat(const CovTab& T, const KModel& m, int di, int dj, int dk, double dx,
+                                          double dy, double dz) {
+  if (dk < 0) {
+    di = -di;
+    dj = -dj;
+    dk = -dk;
+  }
+  if (T.v && dk <= T.tz && abs(dj) <= T.ty && abs(di) <= T.tx)
+    return __ldg(T.v + (di + T.tx) + (size_t)(2 * T.tx + 1) * ((dj + T.ty) + (size_t)(2 * T.ty + 1) * dk));
+  return cov_k(m, (double)di * dx, (double)dj * dy, (double)dk * dz);
+}
+
+__global__ void k_cov_table(KModel m, double dx, double dy, double dz, int tx, int ty, int tz, double* __restrict__ v) {
+  const long long wx = 2 * tx + 1, wy = 2 * ty + 1, tot = wx * wy * (tz + 1);
+  for (long long q = blockIdx.x * (long long)blockDim.x + threadIdx.x; q < tot; q += (long long)gridDim.x * blockDim.x) {
+    const int di = (int)(q % wx) - tx;
+    const int dj = (int)((q / wx) % wy) - ty;
+    const int dk = (int)(q / (wx * wy));
+    v[q] = cov_k(m, (double)di * dx, (double)dj * dy, (double)dk * dz);
+  }
 }
 
 // 1/sqrt(x) for a positive normal x: the hardware approximation (PTX
@@ -273,9 +307,9 @@ __device__ bool warp_cholesky(T* L, T* rinv, int ld, int n, T ridge, const uint8
 // refinement step with the residual b - A w formed in FP64.
 // Dynamic shared memory: the pair table, then one region per warp.
 template <int PREC>
-__global__ void k_cond_krige(CondGeo G, KModel mdl, long long node0, int count, const int* __restrict__ nbr,
-                             const int* __restrict__ nnb, const double* __restrict__ dxs,
-                             const double* __restrict__ dys, const double* __restrict__ dzs,
+__global__ void k_cond_krige(CondGeo G, KModel mdl, CovTab ctab, long long node0, int count,
+                             const int* __restrict__ nbr, const int* __restrict__ nnb, const int* __restrict__ ixs,
+                             const int* __restrict__ iys, const int* __restrict__ izs,
                              const double* __restrict__ dg, const double* __restrict__ simd, double* __restrict__ res,
                              unsigned long long* __restrict__ counters) {
   extern __shared__ __align__(16) unsigned char smc[];
@@ -302,6 +336,7 @@ __global__ void k_cond_krige(CondGeo G, KModel mdl, long long node0, int count, 
   float* tf = wf + ndmax;
   float* rinvf = tf + ndmax;
   int* id = PREC == 0 ? (int*)(rinv + ndmax) : (int*)(rinvf + ndmax);
+  int* lat = id + ndmax;         // lattice indices (0-based) of the neighbours: x, y, z per neighbour
   const long long M = (long long)G.nx * G.ny * G.nz;
   for (int q = blockIdx.x * nwb + wib; q < count; q += gridDim.x * nwb) {
     const long long node = node0 + q;
@@ -322,24 +357,27 @@ __global__ void k_cond_krige(CondGeo G, KModel mdl, long long node0, int count, 
     // a conditioned grid has at most 2^27 nodes: 32-bit index arithmetic
     const uint32_t nu = (uint32_t)node, row = nu / (uint32_t)G.nx;
     const int i = (int)(nu - row * (uint32_t)G.nx), j = (int)(row % (uint32_t)G.ny), k = (int)(row / (uint32_t)G.ny);
-    const double x = G.xmin + (double)i * G.dx, y = G.ymin + (double)j * G.dy, z = G.zmin + (double)k * G.dz;
-    for (int p = lane; p < nn; p += 32) id[p] = nl[p];
+    for (int p = lane; p < nn; p += 32) {
+      const int cp = nl[p];
+      id[p] = cp;
+      lat[3 * p] = __ldg(ixs + cp) - 1;
+      lat[3 * p + 1] = __ldg(iys + cp) - 1;
+      lat[3 * p + 2] = __ldg(izs + cp) - 1;
+    }
     __syncwarp();
     const int ntri = nn * (nn + 1) / 2;
     auto fill_matrix = [&]() {
       for (int e = lane; e < ntri; e += 32) {
         const int p = tri[2 * e], qq = tri[2 * e + 1];
-        const int cp = id[p], cq = id[qq];
-        const double v = cov_k(mdl, dxs[cp] - dxs[cq], dys[cp] - dys[cq], dzs[cp] - dzs[cq]);
+        const double v = cov_lat(ctab, mdl, lat[3 * p] - lat[3 * qq], lat[3 * p + 1] - lat[3 * qq + 1],
+                                 lat[3 * p + 2] - lat[3 * qq + 2], G.dx, G.dy, G.dz);
         A[p * ld + qq] = v;
         A[qq * ld + p] = v;
       }
     };
     fill_matrix();
-    for (int p = lane; p < nn; p += 32) {
-      const int cp = id[p];
-      b[p] = cov_k(mdl, dxs[cp] - x, dys[cp] - y, dzs[cp] - z);
-    }
+    for (int p = lane; p < nn; p += 32)
+      b[p] = cov_lat(ctab, mdl, lat[3 * p] - i, lat[3 * p + 1] - j, lat[3 * p + 2] - k, G.dx, G.dy, G.dz);
     __syncwarp();
     double ridge = 1.0e-10 * G.c0;
     bool ok = false;
@@ -769,6 +807,28 @@ extern "C" int ss3d_condition(double* res, const int n[3], int nreal, const doub
     ++g_launch_count;
     e = cudaGetLastError();
   }
+  // lattice covariance table over the lags two search half-extents wide
+  // (at most the grid), when it stays below 128 MB
+  CovTab ctab{nullptr, 0, 0, 0};
+  double* dctab = nullptr;
+  {
+    auto half = [](double ext, double step, int n) {
+      return (int)std::min<double>(n - 1, ceil(2.0 * ext / step) + 1.0);
+    };
+    const int tx = half(ex, dx, nx), ty = half(ey, dy, ny), tz = half(ez, dz, nz);
+    const double cnt = (2.0 * tx + 1.0) * (2.0 * ty + 1.0) * (tz + 1.0);
+    if (cnt * sizeof(double) <= (double)(128u << 20) && e == cudaSuccess) {
+      const long long ncnt = (long long)cnt;
+      e = bufs.alloc(&dctab, (size_t)ncnt);
+      if (e == cudaSuccess) {
+        k_cov_table<<<(int)std::min<long long>(148 * 16, (ncnt + 255) / 256), 256, 0, stm>>>(kmdl, dx, dy, dz, tx,
+                                                                                           ty, tz, dctab);
+        ++g_launch_count;
+        e = cudaGetLastError();
+      }
+      ctab = CovTab{dctab, tx, ty, tz};
+    }
+  }
   // kriging CTAs: warps per block limited by the shared memory of one warp
   const size_t per = cond_warp_bytes(cp->ndmax, precision == SS3D_FP64 ? 0 : 1);
   const int wpb = (int)std::max<size_t>(1, std::min<size_t>(8, (size_t)(96 * 1024) / per));
@@ -788,12 +848,13 @@ extern "C" int ss3d_condition(double* res, const int n[3], int nreal, const doub
     // one block per wpb nodes (short blocks): work of other streams, e.g. of a
     // serving loop's higher-priority requests, gets SMs as blocks finish
     const int nblk = (int)(((long long)count + wpb - 1) / wpb);
+    const size_t ksm = cond_tri_bytes(cp->ndmax) + per * wpb;
     if (precision == SS3D_FP64)
-      k_cond_krige<0><<<nblk, 32 * wpb, cond_tri_bytes(cp->ndmax) + per * wpb, stm>>>(G, kmdl, node0, count, dnbr, dnnb, ddx, ddy, ddz, ddg,
-                                                          dsimd, dres, dcnt);
+      k_cond_krige<0><<<nblk, 32 * wpb, ksm, stm>>>(G, kmdl, ctab, node0, count, dnbr, dnnb, dix, diy, diz, ddg,
+                                                    dsimd, dres, dcnt);
     else
-      k_cond_krige<1><<<nblk, 32 * wpb, cond_tri_bytes(cp->ndmax) + per * wpb, stm>>>(G, kmdl, node0, count, dnbr, dnnb, ddx, ddy, ddz, ddg,
-                                                          dsimd, dres, dcnt);
+      k_cond_krige<1><<<nblk, 32 * wpb, ksm, stm>>>(G, kmdl, ctab, node0, count, dnbr, dnnb, dix, diy, diz, ddg,
+                                                    dsimd, dres, dcnt);
     ++g_launch_count;
     e = cudaGetLastError();
   }

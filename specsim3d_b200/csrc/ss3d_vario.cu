@@ -9,19 +9,23 @@
 // Since gamma(l s) = gamma(-l s) (the same pairs read in the other order), a
 // direction is normalised so that its leading march component is positive.
 //
-// Kernel layout: a CTA owns a sheared slab of base points
-//     p(t, m) = q0 + t u + m v,   t in [0, 32) lanes,  m in [m0, m0 + T)
-// and stages f on p(t, m) for m in [m0, m0 + T + L mu) in shared memory
-// (s[m][t], coalesced loads along x).  The partner of base (t, m) at lag l is
-// (t, m + l mu).  Two cases:
-//   * general (s has a y or z component): u = e_x, v = s, mu = 1; the slab is
-//     keyed by the residue r of the leading axis and the virtual start q
-//     (points outside the grid are masked);
-//   * pure x (s = (sx, 0, 0)): u = e_y, v = e_x, mu = sx.
-// Each line t meets the grid on one interval of m, so a pair is valid iff its
-// base is valid and m + l mu lies before the end of that interval.  Warp w of
-// the CTA accumulates the lags l = l0 + w, l0 + w + NW, ... in registers; the
-// per-CTA lag sums go to a partial buffer reduced in a fixed order.
+// Kernel layout.  Every direction is walked as lines with a unit march step:
+//   * general (s has a y or z component): a line starts on one of the first
+//     s_a planes of its leading axis a (z, else y) at a virtual start q that
+//     may lie outside the grid, and steps by s; lanes of a CTA take 32
+//     consecutive x starts (coalesced loads along each march step);
+//   * pure x (s = (sx, 0, 0)): a line is row (y, z) restricted to the
+//     residue x = rho (mod sx), rho < min(sx, nx); lanes take 32 rows.
+// Each lane's line meets the grid on one interval of march indices; the lane
+// counts its march from the first point inside (lane-local index), so a pair
+// (base b, partner b + l) is valid iff the partner index is below the lane's
+// line length.  A CTA owns the lane-local bases [m0, m0 + Tb) of its 32 lines
+// and stages their values in shared memory s[row][lane] (pitch 33 doubles).
+// Warp w owns the lags l0 + 16 w + j (j < 16) of the launch and runs register
+// blocks of 8 bases x 16 lags: 8 base values and 23 partner values serve 128
+// pairs, one FP64 subtraction and one FP64 fma per pair.  Lane sums are
+// folded per lag in a fixed order and written as per-CTA partials, reduced by
+// k_vario_reduce in CTA order: results do not depend on scheduling.
 #include <cuda_runtime.h>
 
 #include <algorithm>
@@ -36,25 +40,37 @@
 
 namespace ss3d {
 
-constexpr int VT = 128;      // base march steps per CTA
-constexpr int VNW = 8;       // warps per CTA
-constexpr int VLPT = 16;     // lags per thread per launch
-constexpr int VLCH = VNW * VLPT;  // lags per launch (128)
-constexpr int VPW = 128;     // lags * mu per launch at most: partner window VT + VPW - 1 steps
-constexpr int VP = 33;       // shared-memory pitch (lanes + 1)
+constexpr int VT = 256;            // lane-local bases per CTA at most
+constexpr int VB = 8;              // bases per register block
+constexpr int VL = 16;             // lags per warp
+constexpr int VNW = 8;             // warps per CTA at most
+constexpr int VLCH = VNW * VL;     // lags per launch (128)
+constexpr int VP = 33;             // shared-memory pitch (lanes + 1)
+static_assert(VT % VB == 0, "a CTA's base range is a whole number of register blocks");
 
 struct VarioGeo {
   int nx, ny, nz;
-  int mode;          // 0 general (v = s), 1 pure x (v = e_x, mu = sx)
+  int mode;          // 0 general, 1 pure x
   int sx, sy, sz;    // normalised direction
-  int mu;            // partner offset per lag along the march
   int a;             // general: leading axis 1 = y, 2 = z
-  int sig;           // general: s_a > 0
+  int sig;           // general: s_a > 0; pure x: residues min(sx, nx)
   int qx_lo, nqx;    // general: virtual start range along x (32 per tile); pure x: row tiles
-  int qb_lo, nqb;    // general: virtual start range along the other axis
-  int mmax;          // march length bound
-  int nmb;           // march blocks of VT
+  int qb_lo, nqb;    // general: virtual start range along the other axis; pure x: planes
+  int mmax;          // longest line (march steps inside the grid)
+  int tb;            // lane-local bases per CTA (multiple of VB)
+  int nmb;           // base blocks of tb per line
   int ncta;          // CTAs per realization
+};
+
+// Launch layout of one lag chunk: shared rows [0, na) hold lane-local march
+// m0 .. m0 + na - 1; rows [na, na + nb) (split layout) hold m0 + l0 .. ;
+// the partner of base row b at lag l0 + k sits at row pofs + b + k, and is
+// staged when b + k < prow.
+struct VarioWin {
+  int l0, nl;        // lags l0 .. l0 + nl - 1
+  int na, nb;        // staged rows of the two segments (nb = 0: one segment)
+  int pofs, prow;    // partner row of (b, k = 0) and the partner rows staged
+  int rows;          // rows allocated (na + nb + VB: base blocks may read past)
 };
 
 __host__ __device__ __forceinline__ long long floordiv(long long a, long long b) {  // b > 0
@@ -62,29 +78,32 @@ __host__ __device__ __forceinline__ long long floordiv(long long a, long long b)
 }
 __host__ __device__ __forceinline__ long long ceildiv(long long a, long long b) { return -floordiv(-a, b); }
 
-// Line of lane t of CTA cta: start point (linear index base), step per march
-// index (linear), the valid march interval [vlo, vhi) where the point is
-// inside the grid, and the first base march index m0 of the CTA.
-__device__ __forceinline__ void lane_line(const VarioGeo& G, int cta, int t, int& vlo, int& vhi, long long& base,
+// Line of lane t of CTA cta: linear index of its first point inside the grid
+// (base), linear step, number of points inside (len) and the first lane-local
+// base m0 of the CTA.
+__device__ __forceinline__ void lane_line(const VarioGeo& G, int cta, int t, int& len, long long& base,
                                           long long& step, int& m0) {
-  int mb = cta % G.nmb;
+  const int mb = cta % G.nmb;
   int rest = cta / G.nmb;
-  m0 = mb * VT;
+  m0 = mb * G.tb;
   long long x0, y0, z0, dx, dy, dz;
+  long long hi = G.mmax;
   if (G.mode == 1) {
-    int jt = rest % G.nqx;
-    int k = rest / G.nqx;
-    x0 = 0;
+    const int jt = rest % G.nqx;
+    rest /= G.nqx;
+    const int k = rest % G.nqb;
+    const int rho = rest / G.nqb;
+    x0 = rho;
     y0 = (long long)jt * 32 + t;
     z0 = k;
-    dx = 1;
+    dx = G.sx;
     dy = 0;
     dz = 0;
   } else {
-    int xt = rest % G.nqx;
+    const int xt = rest % G.nqx;
     rest /= G.nqx;
-    int qb = G.qb_lo + rest % G.nqb;
-    int r = rest / G.nqb;
+    const int qb = G.qb_lo + rest % G.nqb;
+    const int r = rest / G.nqb;
     x0 = (long long)G.qx_lo + (long long)xt * 32 + t;
     if (G.a == 2) {
       z0 = r;
@@ -97,7 +116,7 @@ __device__ __forceinline__ void lane_line(const VarioGeo& G, int cta, int t, int
     dy = G.sy;
     dz = G.sz;
   }
-  long long lo = 0, hi = G.mmax;
+  long long lo = 0;
   auto clip = [&](long long c0, long long dc, long long n) {
     if (dc == 0) {
       if (c0 < 0 || c0 >= n) hi = lo;
@@ -114,80 +133,89 @@ __device__ __forceinline__ void lane_line(const VarioGeo& G, int cta, int t, int
   clip(y0, dy, G.ny);
   clip(z0, dz, G.nz);
   if (hi < lo) hi = lo;
-  vlo = (int)lo;
-  vhi = (int)hi;
-  base = x0 + (long long)G.nx * (y0 + (long long)G.ny * z0);
+  len = (int)(hi - lo);
   step = dx + (long long)G.nx * (dy + (long long)G.ny * dz);
+  // first point inside; for an empty line any in-range index (never read)
+  base = len > 0 ? x0 + (long long)G.nx * (y0 + (long long)G.ny * z0) + lo * step : 0;
 }
 
-// Shared memory: base window sb[VT][VP] (march m0 .. m0+VT-1) and partner
-// window sp[VT+VPW-1][VP] (march ps .. , ps = m0 + l0 mu).  For base m and lag
-// l in [l0, l0+nl), the partner index m + l mu - ps lies in
-// [0, VT - 1 + (nl - 1) mu] and nl * mu <= VPW, so every read is inside sp.
-__global__ void __launch_bounds__(32 * VNW) k_vario(VarioGeo G, const double* __restrict__ f, long long fstride,
-                                                    int l0, int nl, double* __restrict__ part) {
+__device__ __forceinline__ double vload(const double* __restrict__ fr, long long base, long long step, int m,
+                                        int len) {
+  return m < len ? __ldg(fr + base + (long long)m * step) : 0.0;
+}
+
+__global__ void __launch_bounds__(32 * VNW, 3) k_vario(VarioGeo G, VarioWin W, const double* __restrict__ f,
+                                                    long long fstride, double* __restrict__ part) {
   extern __shared__ __align__(16) double smv[];
-  double* sb = smv;
-  double* spw = smv + VT * VP;
   const int r = blockIdx.y;
   const int cta = blockIdx.x;
   const int t = threadIdx.x & 31, w = threadIdx.x >> 5;
+  const int nw = blockDim.x >> 5;
   const double* fr = f + (long long)r * fstride;
-  const int pspan = VT + (nl - 1) * G.mu;
-  int vlo, vhi, m0;
+  int len, m0;
   long long base, step;
-  lane_line(G, cta, t, vlo, vhi, base, step, m0);
-  const int ps = m0 + l0 * G.mu;
+  lane_line(G, cta, t, len, base, step, m0);
+  // ---- staging: segment A march m0 + q -> row q; segment B march m0 + l0 + q -> row na + q;
+  // the VB rows past them are zero (read by the last base block, never used)
+  const int nrow = W.na + W.nb;
   if (G.mode == 0) {
-    // lanes t are consecutive x: coalesced along each march step
-    for (int q = w; q < VT; q += VNW) {
-      const int m = m0 + q;
-      sb[q * VP + t] = (m >= vlo && m < vhi) ? __ldg(fr + base + (long long)m * step) : 0.0;
-    }
-    for (int q = w; q < pspan; q += VNW) {
-      const int m = ps + q;
-      spw[q * VP + t] = (m >= vlo && m < vhi) ? __ldg(fr + base + (long long)m * step) : 0.0;
+    for (int q = w; q < W.rows; q += nw) {
+      double v = 0.0;
+      if (q < W.na)
+        v = vload(fr, base, step, m0 + q, len);
+      else if (q < nrow)
+        v = vload(fr, base, step, m0 + W.l0 + (q - W.na), len);
+      smv[q * VP + t] = v;
     }
   } else {
-    // pure x: line t is row t of the tile; lanes run along x for coalescing
-    for (int row = w; row < 32; row += VNW) {
-      int rvlo, rvhi, rm0;
+    for (int row = w; row < 32; row += nw) {
+      int rlen, rm0;
       long long rbase, rstep;
-      lane_line(G, cta, row, rvlo, rvhi, rbase, rstep, rm0);
-      for (int q = t; q < VT; q += 32) {
-        const int m = m0 + q;
-        sb[q * VP + row] = (m >= rvlo && m < rvhi) ? __ldg(fr + rbase + m) : 0.0;
-      }
-      for (int q = t; q < pspan; q += 32) {
-        const int m = ps + q;
-        spw[q * VP + row] = (m >= rvlo && m < rvhi) ? __ldg(fr + rbase + m) : 0.0;
+      lane_line(G, cta, row, rlen, rbase, rstep, rm0);
+      for (int q = t; q < W.rows; q += 32) {
+        double v = 0.0;
+        if (q < W.na)
+          v = vload(fr, rbase, rstep, m0 + q, rlen);
+        else if (q < nrow)
+          v = vload(fr, rbase, rstep, m0 + W.l0 + (q - W.na), rlen);
+        smv[q * VP + row] = v;
       }
     }
   }
   __syncthreads();
-  double acc[VLPT];
+  // ---- pairs: bases b in [0, tb), lags l0 + lw + j; partner row pofs + b + lw + j,
+  // valid while b + lw + j < plim (inside the line and inside the staged rows)
+  const int lw = w * VL;
+  const int plim = min(len - m0 - W.l0, W.prow);
+  const int bmax = min(G.tb, __reduce_max_sync(0xffffffffu, plim) - lw);
+  double acc[VL];
 #pragma unroll
-  for (int q = 0; q < VLPT; ++q) acc[q] = 0.0;
-  const int mb0 = max(m0, vlo), mb1 = min(m0 + VT, vhi);
-  for (int m = mb0; m < mb1; ++m) {
-    const double b = sb[(m - m0) * VP + t];
+  for (int j = 0; j < VL; ++j) acc[j] = 0.0;
+  const double* sl = smv + t;
+  for (int b0 = 0; b0 < bmax; b0 += VB) {
+    double bv[VB];
 #pragma unroll
-    for (int q = 0; q < VLPT; ++q) {
-      const int li = w + q * VNW;
-      const int mp = m + (l0 + li) * G.mu;
-      if (li < nl && mp < vhi) {
-        const double d = spw[(mp - ps) * VP + t] - b;
-        acc[q] = fma(d, d, acc[q]);
+    for (int i = 0; i < VB; ++i) bv[i] = sl[(b0 + i) * VP];
+    const int q0 = b0 + lw;
+    const double* pp = sl + (W.pofs + q0) * VP;
+#pragma unroll
+    for (int p = 0; p < VB + VL - 1; ++p) {
+      if (q0 + p < plim) {
+        const double pv = pp[p * VP];
+#pragma unroll
+        for (int i = (p - VL + 1 > 0 ? p - VL + 1 : 0); i <= (p < VB - 1 ? p : VB - 1); ++i) {
+          const double d = pv - bv[i];
+          acc[p - i] = fma(d, d, acc[p - i]);
+        }
       }
     }
   }
 #pragma unroll
-  for (int q = 0; q < VLPT; ++q) {
-    double v = acc[q];
+  for (int j = 0; j < VL; ++j) {
+    double v = acc[j];
 #pragma unroll
     for (int off = 16; off > 0; off >>= 1) v += __shfl_down_sync(0xffffffffu, v, off);
-    const int li = w + q * VNW;
-    if (t == 0 && li < nl) part[((long long)r * G.ncta + cta) * VLCH + li] = v;
+    if (t == 0 && lw + j < W.nl) part[((long long)r * G.ncta + cta) * VLCH + lw + j] = v;
   }
 }
 
@@ -283,21 +311,18 @@ extern "C" int ss3d_vario(const double* res, const int n[3], int nreal, int ndir
     G.sx = a;
     G.sy = b;
     G.sz = c;
+    long long ncta = 0;
     if (a == 0 && b == 0 && c == 0) {
       G.mode = 1;   // zero lag vector: every difference is 0, gamma stays 0
-      G.mu = 1;
-      G.ncta = 0;
     } else if (b == 0 && c == 0) {
       G.mode = 1;
-      G.mu = std::max(1, a);
-      G.mmax = nx;
-      G.nqx = (ny + 31) / 32;   // row tiles
+      G.sig = std::min(a, nx);                // residues rho < min(sx, nx)
+      G.mmax = (nx + a - 1) / a;
+      G.nqx = (ny + 31) / 32;                 // row tiles
       G.nqb = nz;
-      G.nmb = (nx + VT - 1) / VT;
-      G.ncta = G.nmb * G.nqx * nz;
+      ncta = (long long)G.nqx * nz * G.sig;
     } else {
       G.mode = 0;
-      G.mu = 1;
       G.a = c != 0 ? 2 : 1;
       G.sig = c != 0 ? c : b;
       const int na = G.a == 2 ? nz : ny;
@@ -311,14 +336,18 @@ extern "C" int ss3d_vario(const double* res, const int n[3], int nreal, int ndir
       G.nqx = (int)((qx_hi - qx_lo + 1 + 31) / 32);
       G.qb_lo = (int)qb_lo;
       G.nqb = (int)(qb_hi - qb_lo + 1);
-      G.nmb = (G.mmax + VT - 1) / VT;
-      long long ncta = (long long)G.nmb * G.nqx * G.nqb * G.sig;
-      if (ncta > 0x7fffffffLL) {
-        e = cudaErrorInvalidValue;
-        break;
-      }
-      G.ncta = (int)ncta;
+      ncta = (long long)G.nqx * G.nqb * G.sig;
     }
+    if (ncta > 0) {
+      G.tb = std::min(VT, (G.mmax + VB - 1) / VB * VB);
+      G.nmb = (G.mmax + G.tb - 1) / G.tb;
+      ncta *= G.nmb;
+    }
+    if (ncta > 0x7fffffffLL) {
+      e = cudaErrorInvalidValue;
+      break;
+    }
+    G.ncta = (int)ncta;
     geos[d] = G;
     part_elems = std::max(part_elems, (size_t)G.ncta * VLCH);
   }
@@ -331,23 +360,40 @@ extern "C" int ss3d_vario(const double* res, const int n[3], int nreal, int ndir
   for (int d = 0; d < ndir && e == cudaSuccess; d++) {
     const VarioGeo& G = geos[d];
     if (nlag[d] == 0 || G.ncta == 0) continue;
-    // lag chunks: at most VLCH lags with nl * mu <= VPW (partner window bound)
-    const int chunk = std::max(1, std::min(VLCH, VPW / std::max(1, G.mu)));
-    for (int l0 = 1; l0 <= nlag[d] && e == cudaSuccess; l0 += chunk) {
-      const int nl = std::min(chunk, nlag[d] - l0 + 1);
-      const size_t smem = sizeof(double) * VP * (size_t)(VT + VT + (nl - 1) * G.mu);
+    for (int l0 = 1; l0 <= nlag[d] && e == cudaSuccess; l0 += VLCH) {
+      VarioWin W{};
+      W.l0 = l0;
+      W.nl = std::min(VLCH, nlag[d] - l0 + 1);
+      const int nw = (W.nl + VL - 1) / VL;
+      // partners of base b < tb at lag offsets k < nw VL lie at lane-local
+      // march m0 + l0 + b + k; march steps past the longest line are never read
+      const int span = std::min(G.tb + nw * VL - 1, std::max(0, G.mmax - l0));
+      const int one = std::min(G.mmax, l0 + span);   // rows of one segment from m0
+      if (one <= G.tb + span) {
+        W.na = one;
+        W.nb = 0;
+        W.pofs = l0;
+        W.prow = std::max(0, one - l0);
+      } else {
+        W.na = G.tb;
+        W.nb = span;
+        W.pofs = G.tb;
+        W.prow = span;
+      }
+      W.rows = W.na + W.nb + VB;
+      const size_t smem = sizeof(double) * VP * (size_t)W.rows;
       e = func_smem(reinterpret_cast<const void*>(k_vario), smem);
       if (e != cudaSuccess) break;
       std::vector<long long> npc(VLCH, 0);
-      for (int li = 0; li < nl; li++) npc[li] = np_all[(l0 + li - 1) + (size_t)nlagmax * d];
+      for (int li = 0; li < W.nl; li++) npc[li] = np_all[(l0 + li - 1) + (size_t)nlagmax * d];
       e = cudaMemcpyAsync(npdev, npc.data(), sizeof(long long) * VLCH, cudaMemcpyHostToDevice, st);
       for (int r0 = 0; r0 < nreal && e == cudaSuccess; r0 += rgroup) {
         const int nr = std::min(rgroup, nreal - r0);
-        k_vario<<<dim3(G.ncta, nr), 32 * VNW, smem, st>>>(G, fdev + (size_t)r0 * M, (long long)M, l0, nl, part);
+        k_vario<<<dim3(G.ncta, nr), 32 * nw, smem, st>>>(G, W, fdev + (size_t)r0 * M, (long long)M, part);
         ++g_launch_count;
         e = cudaGetLastError();
         if (e != cudaSuccess) break;
-        k_vario_reduce<<<dim3(nl, nr), 256, 0, st>>>(part, G.ncta, l0, nl, d, ndir, nlagmax, npdev, gdev, r0);
+        k_vario_reduce<<<dim3(W.nl, nr), 256, 0, st>>>(part, G.ncta, l0, W.nl, d, ndir, nlagmax, npdev, gdev, r0);
         ++g_launch_count;
         e = cudaGetLastError();
       }

@@ -33,14 +33,20 @@ def cfg2(gpu):
 
 
 def test_cfg2_spectrum(cfg2):
+    """Amplitudes within 1e-12 of the largest; the diagnostic sums within
+    1e-7: the oracle, like the reference (f90:1280-1288), adds the 2^27 values
+    of S one after the other in FP64, which drifts by up to about
+    2^27 * 2^-53 = 1.5e-8 relative, while the GPU sums in a fixed tree order.
+    Parseval, sum S = C(0), holds for the GPU sums to 1e-9."""
     gpu, sp, amp, st = cfg2
     assert sp.np == (512, 512, 512)
     ref = recipes.half_of_full(amp, 512)
     got = sp.amp()
     assert np.max(np.abs(got - ref)) <= 1e-12 * np.max(ref)
     assert sp.stats["c0"] == st["c0"]
-    assert abs(sp.stats["spos"] - st["spos"]) <= 1e-12 * st["spos"]
-    assert abs(sp.stats["sneg"] - st["sneg"]) <= 1e-12 * st["spos"]
+    assert abs(sp.stats["spos"] - st["spos"]) <= 1e-7 * st["spos"]
+    assert abs(sp.stats["sneg"] - st["sneg"]) <= 1e-7 * st["spos"]
+    assert abs(sp.stats["spos"] + sp.stats["sneg"] - st["c0"]) <= 1e-9 * st["c0"]
 
 
 @pytest.mark.parametrize("r", [0, 7])
