@@ -258,48 +258,70 @@ def _serving_cond(model, ndata, seed):
     return dict(params=params, rows=np.column_stack([xyz, val]), xmin=(0.0, 0.0, 0.0))
 
 
-def bench_serving(ss, rates=(200.0, 1000.0), count=300, slots=8, budget=64 << 30, premap=24 << 30):
-    """Serving form on a Poisson request stream (seed 2024) over a pool of 64
-    models (seed 2025): grids log-uniform 32..256 per axis, nreal 1..16, 20 %
-    conditional with 200..2000 data, precision form throughout (FP32 synthesis
-    and transforms; the conditional requests' fields are float64 and their
-    kriging solves are FP32 with one FP64 residual refinement).  Open loop: a feeder submits each request at its
-    arrival time.  Latency = completion - arrival.  Beside it the plain path,
-    one request at a time with no spectra cache (spectrum, realizations and
-    conditioning per request): its service times are measured, and its latency
-    at each rate is the FIFO single-server recursion on those times."""
+SERVING_RATES = (50.0, 100.0, 200.0, 500.0, 1000.0, 2000.0)
+
+
+def _pcts(lat_ms):
+    if len(lat_ms) == 0:
+        return {"n": 0}
+    a = np.asarray(lat_ms)
+    return {"n": int(a.size), "p50_ms": round(float(np.percentile(a, 50)), 3),
+            "p99_ms": round(float(np.percentile(a, 99)), 3)}
+
+
+def bench_serving(ss, rates=SERVING_RATES, count=4000, slots=8, budget=64 << 30, premap=24 << 30,
+                  arena_bytes=40 << 30):
+    """Serving form on the stated configuration: a Poisson request stream of
+    `count` requests (seed 2024) at each rate over a pool of 64 models (seed
+    2025): grids log-uniform 32..256 per axis, nreal 1..16, 20 % conditional
+    with 200..2000 data, precision form throughout (FP32 synthesis and
+    transforms; conditional fields are float64 and their kriging solves FP32
+    with one FP64 residual refinement).  Open loop: a feeder submits each
+    request at its arrival time; latency = completion - arrival, reported for
+    all requests and per class (unconditional / conditional).  Beside it the
+    plain path, one request at a time with no spectra cache: its service times
+    are measured, and its latency at each rate is the FIFO single-server
+    recursion on those times.
+
+    Outputs: the 4,000 requests' fields would take about 200 GB, so each
+    request writes into a slice of one preallocated device arena taken in
+    arrival order as a ring (`arena_bytes`).  Two requests share bytes only when
+    about a thousand requests lie between them in the queue, while the
+    admission order keeps running requests within slots + max_bypass queue
+    positions of each other; the bench does not read the fields."""
     import threading
     import torch
     from specsim3d_b200 import workloads
     pool = workloads.model_pool()
     out = {"workload": f"{count} requests per rate, Poisson arrivals (seed 2024), pool of 64 models (seed 2025), "
                        "grids log-uniform 32..256 per axis, nreal U{1..16}, 20 % conditional (200..2000 points); "
-                       "unmeasured closed-loop and open-loop passes first",
-           "slots": slots, "hbm_budget_gb": budget / 2 ** 30, "premap_gb": premap / 2 ** 30, "rates": {}}
-
-    def alloc(q):
+                       "unmeasured closed-loop and open-loop passes first; outputs in a ring arena",
+           "slots": slots, "hbm_budget_gb": budget / 2 ** 30, "premap_gb": premap / 2 ** 30,
+           "arena_gb": arena_bytes / 2 ** 30, "rates": {}}
+    base_reqs = workloads.request_stream(1.0, count=count)
+    arena = torch.empty(arena_bytes, dtype=torch.uint8, device="cuda")
+    outs, off = [], 0
+    for q in base_reqs:
         m = pool[q["model"]]
         nx, ny, nz = m["n"]
-        return torch.empty((q["nreal"], nz, ny, nx), dtype=torch.float64 if q["ndata"] else torch.float32,
-                           device="cuda")
-
-    def cond_of(q, k):
-        return _serving_cond(pool[q["model"]], q["ndata"], 5000 + k) if q["ndata"] else None
-
-    def prec_of(q):
-        return ss.FP32        # precision form; conditional fields are float64 arrays, kriging FP32 + FP64 refinement
-
-    base_reqs = workloads.request_stream(1.0, count=count)
-    conds = [cond_of(q, k) for k, q in enumerate(base_reqs)]
+        dt = torch.float64 if q["ndata"] else torch.float32
+        nb = q["nreal"] * nx * ny * nz * (8 if q["ndata"] else 4)
+        if off + nb > arena_bytes:
+            off = 0
+        outs.append(arena[off:off + nb].view(dt).view(q["nreal"], nz, ny, nx))
+        off = (off + nb + 255) // 256 * 256
+    conds = [_serving_cond(pool[q["model"]], q["ndata"], 5000 + k) if q["ndata"] else None
+             for k, q in enumerate(base_reqs)]
     cells_of = [q["nreal"] * int(np.prod(pool[q["model"]]["n"])) for q in base_reqs]
-    # warm-up (not measured): one closed-loop pass over the requests maps the
-    # device memory the slots and spectra will use and allocates the output
-    # buffers; every measured rate then starts from an empty spectra cache on a
-    # new server
+    is_cond = np.array([q["ndata"] > 0 for q in base_reqs])
+    prec = ss.FP32
+    # warm-up (not measured): a closed-loop pass over the first requests maps
+    # the device memory the slots and spectra use; every measured rate then
+    # starts from an empty spectra cache on a new server
     srv = ss.Server(slots=slots, hbm_budget=budget, premap_bytes=premap)
-    outs = [alloc(q) for q in base_reqs]
-    ts = [srv.submit(pool[q["model"]], q["iseed"], q["nreal"], 1, prec_of(q), out=o, cond=conds[k])
-          for k, (q, o) in enumerate(zip(base_reqs, outs))]
+    nw = min(count, 1000)
+    ts = [srv.submit(pool[q["model"]], q["iseed"], q["nreal"], 1, prec, out=outs[k], cond=conds[k])
+          for k, q in enumerate(base_reqs[:nw])]
     for t in ts:
         srv.wait(t)
     srv.close()
@@ -316,7 +338,7 @@ def bench_serving(ss, rates=(200.0, 1000.0), count=300, slots=8, budget=64 << 30
                 dt = t_arr - srv.clock()
                 if dt > 0:
                     time.sleep(dt)
-                tickets[k] = srv.submit(pool[q["model"]], q["iseed"], q["nreal"], 1, prec_of(q), out=outs[k],
+                tickets[k] = srv.submit(pool[q["model"]], q["iseed"], q["nreal"], 1, prec, out=outs[k],
                                         t_arrival=t_arr, cond=conds[k])
 
         th = threading.Thread(target=feeder)
@@ -331,23 +353,21 @@ def bench_serving(ss, rates=(200.0, 1000.0), count=300, slots=8, budget=64 << 30
         srv.close()
         return res, st, t_start
 
-    # and one unmeasured open-loop pass at the highest rate: the device pages
-    # of the peak footprint of an open-loop run get mapped before any timing
+    # one unmeasured open-loop pass at the highest rate maps the pages of an
+    # open-loop run's peak footprint before any timing
     open_loop(max(rates))
-    # the output buffers of the warm-up serve every measured pass (request k
-    # has the same grid at every rate): a device allocation inside the timed
-    # loop would synchronise the device under the slots
     torch.cuda.synchronize()
     for rate in rates:
         res, st, t_start = open_loop(rate)
-        ok = [r for r in res if r["status"] == 0]
-        lat = np.array([r["t_done"] - r["t_arrival"] for r in ok]) * 1e3
-        span = max(r["t_done"] for r in ok) - t_start
+        ok = np.array([r["status"] == 0 for r in res])
+        lat = np.array([r["t_done"] - r["t_arrival"] for r in res]) * 1e3
+        span = max(r["t_done"] for r in res) - t_start
         cells = sum(c for c, r in zip(cells_of, res) if r["status"] == 0)
         out["rates"][str(int(rate))] = {
-            "p50_ms": round(float(np.percentile(lat, 50)), 3), "p99_ms": round(float(np.percentile(lat, 99)), 3),
-            "mcells_s": round(cells / span / 1e6, 1), "completed": len(ok), "failed": count - len(ok),
-            "cache_hits": st["cache_hits"], "cache_misses": st["cache_misses"], "peak_running": st["peak_running"],
+            **_pcts(lat[ok]), "mcells_s": round(cells / span / 1e6, 1), "completed": int(ok.sum()),
+            "failed": int((~ok).sum()), "unconditional": _pcts(lat[ok & ~is_cond]),
+            "conditional": _pcts(lat[ok & is_cond]), "cache_hits": st["cache_hits"],
+            "cache_misses": st["cache_misses"], "peak_running": st["peak_running"],
             "peak_gb": round(st["peak_bytes"] / 2 ** 30, 2)}
     # plain path: one request at a time, no cache
     svc = []
@@ -357,16 +377,17 @@ def bench_serving(ss, rates=(200.0, 1000.0), count=300, slots=8, budget=64 << 30
         t0 = time.perf_counter()
         o = outs[k]
         sp = ss.Spectrum(m["structs"], m["nugget"], m["d"], m["n"], m["ipad"])
-        sp.realize(q["iseed"], q["nreal"], 1, prec_of(q), out=o)
+        sp.realize(q["iseed"], q["nreal"], 1, prec, out=o)
         if conds[k] is not None:
             c = conds[k]
-            ss.condition(o, c["xmin"], m["d"], m["structs"], m["nugget"], c["params"], c["rows"], prec_of(q))
+            ss.condition(o, c["xmin"], m["d"], m["structs"], m["nugget"], c["params"], c["rows"], prec)
         sp.close()
         torch.cuda.synchronize()
         svc.append(time.perf_counter() - t0)
+    svc = np.array(svc)
     tot_cells = sum(cells_of)
-    plain = {"mcells_s": round(tot_cells / sum(svc) / 1e6, 1), "mean_service_ms": round(1e3 * float(np.mean(svc)), 3),
-             "rates": {}}
+    plain = {"mcells_s": round(tot_cells / svc.sum() / 1e6, 1), "mean_service_ms": round(1e3 * float(svc.mean()), 3),
+             "service_share_conditional": round(float(svc[is_cond].sum() / svc.sum()), 3), "rates": {}}
     for rate in rates:
         reqs = workloads.request_stream(rate, count=count)
         done, lat = 0.0, []
@@ -374,13 +395,14 @@ def bench_serving(ss, rates=(200.0, 1000.0), count=300, slots=8, budget=64 << 30
             done = max(done, q["t_arrival"]) + sv
             lat.append(done - q["t_arrival"])
         lat = np.array(lat) * 1e3
-        plain["rates"][str(int(rate))] = {"p50_ms": round(float(np.percentile(lat, 50)), 3),
-                                         "p99_ms": round(float(np.percentile(lat, 99)), 3)}
+        plain["rates"][str(int(rate))] = {**_pcts(lat), "unconditional": _pcts(lat[~is_cond]),
+                                         "conditional": _pcts(lat[is_cond])}
     out["one_at_a_time"] = plain
+    del outs, arena
     return out
 
 
-def bench_conditional(ss, stream):
+def bench_conditional(ss, stream, cpu=True):
     """Conditional configuration: 128x128x64, exponential sill 1 nugget 0.05
     ranges 40/20/8 azimuth 60; truth = realization of seed 4242 (igauss 0); 2,000
     data at uniform-random locations (seed 99) with values exp(0.5 z) of the
@@ -426,11 +448,28 @@ def bench_conditional(ss, stream):
            "neighbours_total": st["nsum"], "regularised_systems": st["nfail"],
            "fp32_vs_fp64": {"max_abs_over_sd": float(d.amax().item()) / sd,
                             "rms_over_sd": float(d.pow_(2).mean().sqrt().item()) / sd, "target": 1e-5}}
+    if cpu:
+        # the same conditioning through the oracle (C restatement of the Fortran,
+        # OpenMP) on the host cores, on the same unconditioned fields
+        ora = oracle_lib()
+        host = sp.realize(4243, 16, 0, ss.FP64)
+        op = dict(ixc=1, iyc=2, izc=3, ivc=4, iwc=0, tmin=-1e21, tmax=1e21, itrans=1, skmean=0.0, zlo=0.0,
+                  zhi=params["zmax"], ltail=1, ltpar=0.0, utail=1, utpar=0.0, rmax=40.0, rmed=20.0, rvert=8.0,
+                  sa1=60.0, sa2=0.0, sa3=0.0, ndmax=24)
+        t0 = time.perf_counter()
+        ost, _ = ora.condition(host, (0.0, 0.0, 0.0), (1.0, 1.0, 1.0), structs, 0.05, op, rows)
+        tc = time.perf_counter() - t0
+        cores = int(os.environ.get("OMP_NUM_THREADS", os.cpu_count() or 1))
+        out["cpu_baseline"] = {"ms": round(tc * 1e3, 1), "mcells_s": round(M * 16 / tc / 1e6, 1), "cores": cores,
+                               "kind": "port", "neighbours_total": ost["nsum"],
+                               "sample": "one conditioning call of the same workload (C restatement of the Fortran, "
+                                         f"OpenMP {cores} threads)",
+                               "gpu_fp64_speedup": round(tc / times["fp64"], 1)}
     sp.close()
     return out
 
 
-def bench_vario(ss, sp, nreal, seed, igauss):
+def bench_vario(ss, sp, nreal, seed, igauss, cpu=True):
     """--vario on the precision configuration: directions (1,0,0), (0,1,0),
     (0,0,1), lags 1..100, FP64 sums over all node pairs of the FP64
     realizations; exact pair counts."""
@@ -453,10 +492,58 @@ def bench_vario(ss, sp, nreal, seed, igauss):
     for di, (sx, sy, sz, nl) in enumerate(dirs):
         model = np.array([c0 - ss.covariance(WL["structs"], WL["nugget"], l * sx, l * sy, l * sz) for l in range(1, nl + 1)])
         rms.append(float(np.sqrt(np.mean((gam[:, di, :nl].mean(axis=0) - model) ** 2)) / c0))
-    return {"workload": "256^3, 8 FP64 realizations, directions x, y, z, lags 1..100", "ms": round(t * 1e3, 3),
-            "pairs": pairs, "gpairs_s": round(pairs / t / 1e9, 2), "fp64_gflop_s": round(3 * pairs / t / 1e9, 1),
-            "pair_count_check": int(npairs[0, 0]) == (n[0] - 1) * n[1] * n[2],
-            "sample_vs_model_rms_over_sill": [round(x, 4) for x in rms]}
+    out = {"workload": "256^3, 8 FP64 realizations, directions x, y, z, lags 1..100", "ms": round(t * 1e3, 3),
+           "pairs": pairs, "gpairs_s": round(pairs / t / 1e9, 2), "fp64_gflop_s": round(3 * pairs / t / 1e9, 1),
+           "pair_count_check": int(npairs[0, 0]) == (n[0] - 1) * n[1] * n[2],
+           "sample_vs_model_rms_over_sill": [round(x, 4) for x in rms]}
+    if cpu:
+        # the oracle's all-pairs loops (f90:405-431, OpenMP over directions and
+        # lags) on one of the realizations, on the host cores
+        ora = oracle_lib()
+        h = f[:1].cpu().numpy()
+        t0 = time.perf_counter()
+        ora.vario(h, dirs)
+        tc = time.perf_counter() - t0
+        cores = int(os.environ.get("OMP_NUM_THREADS", os.cpu_count() or 1))
+        out["cpu_baseline"] = {"ms_per_realization": round(tc * 1e3, 1), "gpairs_s": round(pairs / nreal / tc / 1e9, 3),
+                               "cores": cores, "kind": "port",
+                               "sample": f"1 realization of the same workload (C restatement, OpenMP {cores} threads)",
+                               "gpu_speedup": round(tc * nreal / t, 1)}
+    return out
+
+
+def bench_cfg1(ss, stream, k=200, cpu=True):
+    """Plain method, small: 64x64x16, spherical 20/10/5 N45E, ipad 1, igauss 0,
+    seed 69069, FP64 throughout; one realization per call into device memory
+    (spectrum built once), and the oracle's spectrum + realization on the host."""
+    import torch
+    n = (64, 64, 16)
+    st = [(1, 1.0, 20.0, 10.0, 5.0, 45.0, 0.0, 0.0)]
+    torch.cuda.synchronize()
+    t0 = time.perf_counter()
+    sp = ss.Spectrum(st, 0.0, (1.0, 1.0, 1.0), n, 1)
+    t_spec = time.perf_counter() - t0
+    o = torch.empty((1, n[2], n[1], n[0]), dtype=torch.float64, device="cuda")
+    ms = _ev_ms(stream, lambda: sp.realize(69069, 1, 0, ss.FP64, out=o), k, 10)
+    M = n[0] * n[1] * n[2]
+    out = {"workload": "64x64x16 spherical 20/10/5 az 45, ipad 1 (periodic 128x128x32), igauss 0, seed 69069, FP64",
+           "ms_per_realization": round(ms, 4), "mcells_s": round(M / (ms * 1e-3) / 1e6, 1),
+           "spectrum_ms_wall": round(t_spec * 1e3, 3)}
+    if cpu:
+        ora = oracle_lib()
+        np3, _ = ora.grid(st, (1.0, 1.0, 1.0), n, 1)
+        t0 = time.perf_counter()
+        amp, _ = ora.spectrum(st, 0.0, (1.0, 1.0, 1.0), np3)
+        t1 = time.perf_counter()
+        reps = 5
+        for _ in range(reps):
+            ora.realize(amp, np3, n, 69069, 1, 0)
+        t2 = time.perf_counter()
+        cores = int(os.environ.get("OMP_NUM_THREADS", os.cpu_count() or 1))
+        out["cpu_baseline"] = {"ms_per_realization": round((t2 - t1) / reps * 1e3, 2),
+                               "spectrum_ms": round((t1 - t0) * 1e3, 2), "cores": cores, "kind": "port"}
+    sp.close()
+    return out
 
 
 def run_ours(args):
@@ -649,8 +736,10 @@ def run_ours(args):
     if world == 1 and not args.no_serving:
         line["serving"] = bench_serving(ss)
     if world == 1 and not args.no_batch:
-        line["conditional"] = bench_conditional(ss, stream)
-        line["vario"] = bench_vario(ss, sp, nreal, WL["seed"], WL["igauss"])
+        cpu = not args.no_cpu_baseline
+        line["conditional"] = bench_conditional(ss, stream, cpu=cpu)
+        line["vario"] = bench_vario(ss, sp, nreal, WL["seed"], WL["igauss"], cpu=cpu)
+        line["cfg1"] = bench_cfg1(ss, stream, cpu=cpu)
     if rank == 0 and world == 1 and not args.no_cpu_baseline:
         try:
             sec, t_spec, cores, _ = cpu_reference_sample(1, 0)

@@ -6,7 +6,7 @@ from seeded runs of the Fortran program:
     full double precision (make_figures.py measure_scaling recipe:
     spherical 20/10/5 N45E, ipad 1, seed 99, n^3 grid, nreal 2 (1 at 256));
   * docs/figures/tables/figS1_yao_rms.csv, fig04_models_rms.csv,
-    fig07_legacy_vs_padded.csv  statistics at 4-5 digits;
+    fig05_cases.csv, fig07_legacy_vs_padded.csv  statistics at 4-5 digits;
   * docs/figures/tables/fig12_conditional_validation.csv,
     fig13_conditional_nscore.csv  statistics of seeded conditional runs
     (make_figures.py cond_case / fig12_cond_validation / fig13_cond_nscore).
@@ -46,6 +46,10 @@ def main():
     for row in csv.DictReader(open(os.path.join(tab, "fig12_conditional_validation.csv"))):
         if row["code"] == "SPECSIM3D":
             pins["fig12"] = {k: (row[k] if k == "code" else float(row[k])) for k in row}
+    pins["fig05"] = [dict(case=row["case"], model=row["model"], n_lags=int(row["n_lags"]), rms=float(row["rms"]),
+                          mc_noise=float(row["mc_noise"]), rms_over_noise=float(row["rms_over_noise"]),
+                          bias=float(row["bias"]))
+                     for row in csv.DictReader(open(os.path.join(tab, "fig05_cases.csv")))]
     pins["fig13"] = {row["quantity"]: float(row["value"])
                      for row in csv.DictReader(open(os.path.join(tab, "fig13_conditional_nscore.csv")))}
     pins["cases"] = {
@@ -57,6 +61,10 @@ def main():
         "fig04": "as figS1 for models 1,2,3 (ranges 20/10/5 az 45); rms over lags with h <= range of the direction",
         "fig07": "gaussian 20/10/5 az 45 nreal 40 seed 31791191, vario (1,1,0,57), mean gamma for h > 25 (ipad 0/1); "
                  "spherical nreal 300 seed 777: sd over realizations of the sample variance and mean (ipad 0/1)",
+        "fig05": "64x64x16, ipad 1, seed 2024, nreal 20; 6 anisotropy cases x 3 models + nested sph/exp with nugget "
+                 "0.1; --vario with 1,500 one-lag directions drawn by default_rng(12345).integers(-30..30, -30..30, "
+                 "-12..12) (zero vectors dropped); gamma_model/mean/sd as printed (es14.6); lags with 0.05 < "
+                 "gamma_model/sill < 0.97, first 300; rms, noise = rms of sd/sqrt(20), ratio, bias",
         "fig12": "64x64x16, exponential 20/10/5 az 45, nugget 0, ipad 1; truth = realization 1 of seed 2024 (.bin, "
                  "float32); 150 distinct nodes drawn by default_rng(7).choice(65536, 150, replace=False) in "
                  "(x, y, z) C order, data = truth there written with %.8g; conditioning cpar: columns 1 2 3 4 0, "

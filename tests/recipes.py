@@ -177,3 +177,63 @@ def conditional_tables(realize, condition, which=("fig12", "fig13")):
         condition(res, cond_params(itrans=1, zlim=(0.0, zhi)), cond_rows(ijk, val))
         out["fig13"] = fig13_table(truth_ln, val, as_bin(res), ijk)
     return out
+
+
+# ---------------------------------------------------------------- anisotropy cases
+# Restatement of docs/make_figures.py fig05_cases (459-495): 6 anisotropy cases x
+# 3 models plus a nested model with nugget on a 64x64x16 grid, 20 realizations of
+# seed 2024 each; the mean experimental semivariogram at up to 300 arbitrary
+# integer lag vectors (one-lag directions of the --vario file, drawn from a
+# fresh default_rng(12345)) against the model; the CSV values are the
+# reference's es14.6 (vario_report f90:433-530).
+FIG05_CASES = [
+    ("A iso 15/15/15", 0.0, [(1.0, 15, 15, 15, 0, 0, 0)]),
+    ("B 2:1 20/10/10", 0.0, [(1.0, 20, 10, 10, 30, 0, 0)]),
+    ("C 4:1 20/5/5", 0.0, [(1.0, 20, 5, 5, 60, 0, 0)]),
+    ("D layered 10/10/2", 0.0, [(1.0, 10, 10, 2, 0, 0, 0)]),
+    ("E extreme 40/4/2", 0.0, [(1.0, 40, 4, 2, 135, 0, 0)]),
+    ("F rotated 20/8/4 (az30 dip20 plg15)", 0.0, [(1.0, 20, 8, 4, 30, 20, 15)]),
+]
+FIG05_NESTED = ("G nested + nugget 0.1 (sph + exp)", 0.1, [(1, 0.5, 20, 10, 5, 45, 0, 0), (2, 0.4, 8, 8, 3, 0, 0, 0)])
+FIG05_MODELS = (("spherical", 1), ("exponential", 2), ("gaussian", 3))
+
+
+def fig05_lags():
+    rng = np.random.default_rng(12345)
+    cand = np.column_stack([rng.integers(-30, 31, 1500), rng.integers(-30, 31, 1500), rng.integers(-12, 13, 1500)])
+    return cand[np.any(cand != 0, axis=1)]
+
+
+def fig05_jobs():
+    jobs = []
+    for cname, nug, st in FIG05_CASES:
+        for mname, it in FIG05_MODELS:
+            jobs.append((cname, mname, nug, [(it,) + tuple(float(v) for v in s) for s in st]))
+    jobs.append((FIG05_NESTED[0], "nested", FIG05_NESTED[1], [tuple(float(v) for v in s) for s in FIG05_NESTED[2]]))
+    return jobs
+
+
+def es14_6(v):
+    return float("%.6e" % v)
+
+
+def fig05_row(gam, lags, nugget, structs, covariance):
+    """One row of fig05_cases.csv from gam (nreal, ndir) at the one-lag
+    directions `lags` (np > 0 for all of them on this grid); covariance(structs,
+    nugget, hx, hy, hz) is the model covariance of f90:153-178."""
+    nreal = gam.shape[0]
+    c0 = nugget + sum(s[1] for s in structs)
+    gm = np.array([es14_6(sum(gam[r, d] for r in range(nreal)) / nreal) for d in range(gam.shape[1])])
+    gsd = []
+    for d in range(gam.shape[1]):
+        mean = sum(gam[r, d] for r in range(nreal)) / nreal
+        gsd.append(es14_6(np.sqrt(sum((gam[r, d] - mean) ** 2 for r in range(nreal)) / (nreal - 1))))
+    gsd = np.array(gsd)
+    gt = np.array([es14_6(c0 - covariance(structs, nugget, float(a), float(b), float(c))) for a, b, c in lags])
+    se = gsd / np.sqrt(nreal)
+    keep = (gt > 0.05 * c0) & (gt < 0.97 * c0)
+    idx = np.flatnonzero(keep)[:300]
+    rms = float(np.sqrt(np.mean((gm[idx] - gt[idx]) ** 2)))
+    noise = float(np.sqrt(np.mean(se[idx] ** 2)))
+    return dict(n_lags=len(idx), rms=round(rms, 4), mc_noise=round(noise, 4), rms_over_noise=round(rms / noise, 2),
+                bias=round(float(np.mean(gm[idx] - gt[idx])), 4))

@@ -158,3 +158,25 @@ def test_conditional_tables_fig12_fig13():
     want12 = {k: v for k, v in PINS["fig12"].items() if k not in ("code", "nreal", "seconds_per_realization")}
     assert got["fig12"] == want12
     assert got["fig13"] == PINS["fig13"]
+
+
+def test_fig05_anisotropy_cases():
+    """fig05_cases.csv, all 19 rows to every printed digit: 6 anisotropy cases x
+    3 models plus the nested model with nugget, 20 realizations each, the mean
+    experimental semivariogram at up to 300 arbitrary lag vectors against the
+    model (the reference's seeded recipe, restated in tests/recipes.py)."""
+    lags = recipes.fig05_lags()
+    dirs = [(int(a), int(b), int(c), 1) for a, b, c in lags]
+
+    def cov(structs, nug, hx, hy, hz):
+        return ora.lib().ora_covariance(ora.structs(structs), len(structs), nug, hx, hy, hz)
+
+    want = {(p["case"], p["model"]): {k: p[k] for k in ("n_lags", "rms", "mc_noise", "rms_over_noise", "bias")}
+            for p in PINS["fig05"]}
+    n = (64, 64, 16)
+    for cname, mname, nug, st in recipes.fig05_jobs():
+        np3, _ = ora.grid(st, (1.0, 1.0, 1.0), n, 1)
+        amp, _ = ora.spectrum(st, nug, (1.0, 1.0, 1.0), np3)
+        res, _ = ora.realize(amp, np3, n, 2024, 20, 0)
+        gam = ora.vario(res, dirs)[:, :, 0]
+        assert recipes.fig05_row(gam, lags, nug, st, cov) == want[(cname, mname)], (cname, mname)
