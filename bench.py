@@ -49,8 +49,11 @@ def parse():
     ap.add_argument("--no-cpu-baseline", action="store_true")
     ap.add_argument("--no-batch", action="store_true", help="skip the mixed-grid batched workload")
     ap.add_argument("--no-serving", action="store_true", help="skip the serving workload")
-    ap.add_argument("--profile-case", action="store_true",
-                    help="profiling case: the same grid, 1 realization, three FP32 calls, no timing")
+    ap.add_argument("--profile-case", nargs="?", const="realize", default=None,
+                    choices=["realize", "cond", "vario", "spectrum"],
+                    help="profiling case, no timing: realize (the bench grid, 1 realization, three FP32 calls), "
+                         "cond (the conditional workload, one FP64 and one FP32 conditioning call), vario (one FP64 "
+                         "256^3 realization, directions x, y, z, lags 1..100), spectrum (one 512^3 spectrum build)")
     return ap.parse_args()
 
 
@@ -758,13 +761,50 @@ def run_ours(args):
     return 0
 
 
-def run_profile_case():
-    """Small case for ncu: the bench grid with one realization per call (about
-    1.5 GB on the device), tile variants autotuned as in the bench, then three
-    FP32 calls into a device buffer inside the NVTX range "profile"."""
+def run_profile_case(kind="realize"):
+    """Small cases for ncu.  realize: the bench grid with one realization per
+    call (about 1.5 GB on the device), tile variants autotuned as in the bench,
+    then three FP32 calls into a device buffer inside the NVTX range "profile".
+    cond: the conditional workload (128x128x64, 2,000 data, 16 realizations,
+    about 0.2 GB), one FP64 then one FP32 conditioning call.  vario: one FP64
+    realization of the bench grid (134 MB) and its variograms along x, y, z,
+    lags 1..100.  spectrum: one spectrum build of the bench model (512^3
+    periodic grid, about 3 GB of temporaries)."""
     import torch
     import specsim3d_b200 as ss
     n = WL["n"]
+    if kind == "cond":
+        nc = (128, 128, 64)
+        structs = [(2, 1.0, 40.0, 20.0, 8.0, 60.0, 0.0, 0.0)]
+        sp = ss.Spectrum(structs, 0.05, (1.0, 1.0, 1.0), nc, 1)
+        truth = sp.realize(4242, 1, 0, ss.FP64)[0]
+        rng = np.random.default_rng(99)
+        xyz = np.stack([rng.uniform(0, nc[a] - 1, 2000) for a in range(3)], axis=1)
+        ix = np.rint(xyz).astype(int)
+        val = np.exp(0.5 * truth[ix[:, 2], ix[:, 1], ix[:, 0]])
+        params = dict(ixc=1, iyc=2, izc=3, ivc=4, iwc=0, tmin=-1e21, tmax=1e21, itrans=1, skmean=0.0, zmin=0.0,
+                      zmax=2.0 * float(val.max()), ltail=1, ltpar=0.0, utail=1, utpar=0.0, radius=(40.0, 20.0, 8.0),
+                      angles=(60.0, 0.0, 0.0), ndmax=24)
+        f = torch.empty((16, nc[2], nc[1], nc[0]), dtype=torch.float64, device="cuda")
+        for prec in (ss.FP64, ss.FP32):
+            sp.realize(4243, 16, 0, ss.FP64, out=f)
+            ss.condition(f, (0.0, 0.0, 0.0), (1.0, 1.0, 1.0), structs, 0.05, params, np.column_stack([xyz, val]), prec)
+        torch.cuda.synchronize()
+        sp.close()
+        return 0
+    if kind == "spectrum":
+        sp = ss.Spectrum(WL["structs"], WL["nugget"], WL["d"], n, WL["ipad"])
+        torch.cuda.synchronize()
+        sp.close()
+        return 0
+    if kind == "vario":
+        sp = ss.Spectrum(WL["structs"], WL["nugget"], WL["d"], n, WL["ipad"])
+        f = torch.empty((1, n[2], n[1], n[0]), dtype=torch.float64, device="cuda")
+        sp.realize(WL["seed"], 1, WL["igauss"], ss.FP64, out=f)
+        ss.vario(f, [(1, 0, 0, 100), (0, 1, 0, 100), (0, 0, 1, 100)])
+        torch.cuda.synchronize()
+        sp.close()
+        return 0
     sp = ss.Spectrum(WL["structs"], WL["nugget"], WL["d"], n, WL["ipad"])
     ss.autotune(sp, WL["igauss"], ss.FP32, 1)
     out = torch.empty((1, n[2], n[1], n[0]), dtype=torch.float32, device="cuda")
@@ -781,7 +821,7 @@ def run_profile_case():
 def main():
     args = parse()
     if args.profile_case:
-        return run_profile_case()
+        return run_profile_case(args.profile_case)
     if args.impl == "reference":
         return run_reference(args)
     return run_ours(args)

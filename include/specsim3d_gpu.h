@@ -131,6 +131,13 @@ int ss3d_row_state(const int np[3], int igauss, int iseed, int64_t r, int j, int
 int ss3d_debug_states(const ss3d_spectrum *sp, int iseed, int64_t r, int igauss, uint32_t *states);
 int ss3d_debug_coefficients(const ss3d_spectrum *sp, int iseed, int64_t r, int igauss, int precision, double *coef);
 
+/* Unscaled 3D FFT of a full complex grid a(nx,ny,nz) in place, FP64, x fastest,
+ * interleaved (re, im) doubles, host or device memory: isign -1 forward
+ * (e^{-2 pi i k n/N}), +1 inverse.  Replaces fft3d, f90:254-304 (exported for
+ * unit tests; the simulation path itself uses Hermitian half-spectrum passes).
+ * Every axis a power of two up to 2048, at most 2^27 nodes. */
+int ss3d_fft3d(double *a, int nx, int ny, int nz, int isign);
+
 /* Realizations like ss3d_realize, but without allocating device memory.  No
  * counterpart in the reference (the Fortran program allocates its own arrays).
  * For callers that cannot call cudaMalloc when they need realizations: an

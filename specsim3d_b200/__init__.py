@@ -302,6 +302,24 @@ def vario(res, dirs):
     return gam, npairs
 
 
+def fft3d(a, isign):
+    """Unscaled 3D FFT in place (fft3d, f90:254-304) of a complex128 array of
+    shape (nz, ny, nx) (numpy, or a torch CUDA tensor); isign -1 forward, +1
+    inverse.  Every axis a power of two."""
+    nz, ny, nx = a.shape
+    if isinstance(a, np.ndarray):
+        if a.dtype != np.complex128 or not a.flags.c_contiguous:
+            raise ValueError("fft3d needs a C-contiguous complex128 array")
+        ptr = ctypes.c_void_p(a.ctypes.data)
+    else:
+        import torch
+        if a.dtype != torch.complex128 or not a.is_contiguous():
+            raise ValueError("fft3d needs a contiguous complex128 tensor")
+        ptr = ctypes.c_void_p(a.data_ptr())
+    L.check(L.lib().ss3d_fft3d(ptr, int(nx), int(ny), int(nz), int(isign)))
+    return a
+
+
 def condition(res, xmin, d, structs, nugget, params, rows, precision=FP64):
     """Conditioning by kriging of the residual, in place on res (f90:700-1081).
 

@@ -22,7 +22,7 @@ EXPORTS = (
     "ss3d_setrot", "ss3d_covariance", "ss3d_grid_size",
     "ss3d_spectrum_create", "ss3d_spectrum_free", "ss3d_spectrum_info", "ss3d_spectrum_bytes", "ss3d_spectrum_amp",
     "ss3d_realize", "ss3d_debug_states", "ss3d_debug_coefficients", "ss3d_row_state",
-    "ss3d_vario", "ss3d_condition",
+    "ss3d_vario", "ss3d_condition", "ss3d_fft3d",
     "ss3d_set_stream", "ss3d_last_error", "ss3d_version", "ss3d_profile", "ss3d_profile_read", "ss3d_autotune", "ss3d_set_variant",
     "ss3d_realize_workspace_bytes", "ss3d_release_workspace", "ss3d_trim_pool",
     "ss3d_batch_create", "ss3d_batch_run", "ss3d_batch_autotune", "ss3d_batch_info", "ss3d_batch_time",
@@ -132,6 +132,7 @@ def lib():
         "ss3d_vario": (I, [P, pI, I, I, pI, pI, pI, pI, P, P]),
         "ss3d_condition": (I, [P, pI, I, pD, pD, ctypes.POINTER(Struct), I, D, ctypes.POINTER(CondParams), P, I, I,
                                I, ctypes.POINTER(CondStats), P, P, P, P, P, P, P]),
+        "ss3d_fft3d": (I, [P, I, I, I, I]),
         "ss3d_set_stream": (I, [P]),
         "ss3d_last_error": (ctypes.c_char_p, []),
         "ss3d_version": (ctypes.c_char_p, []),

@@ -719,6 +719,7 @@ extern "C" int ss3d_realize(const ss3d_spectrum* csp, int iseed, int64_t r_first
   cudaError_t e = cudaSuccess;
   Marks marks;
   marks.on = g_prof;
+  const unsigned long long pipes0 = g_pipe_launches.load();
   int ib = 0;
   for (int r0 = 0; r0 < nreal && e == cudaSuccess; r0 += bt, ++ib) {
     int nb = std::min(bt, nreal - r0);
@@ -757,6 +758,8 @@ extern "C" int ss3d_realize(const ss3d_spectrum* csp, int iseed, int64_t r_first
   if (e == cudaSuccess && cs) e = cudaStreamSynchronize(cs);
   if (marks.on) marks_collect(marks);
   if (e != cudaSuccess) return cuda_fail(e, "realize");
+  if (g_pipe_launches.load() != pipes0 && pipe_error_take(s))
+    return fail(SS3D_ECUDA, "realize: a bulk-copy wait of the middle pass timed out");
   if (zstats) {
     for (int r = 0; r < nreal; r++) {
       double mean = hz[2 * r] / (double)M;
@@ -765,6 +768,41 @@ extern "C" int ss3d_realize(const ss3d_spectrum* csp, int iseed, int64_t r_first
       zstats[3 * r + 2] = 0.0;
     }
   }
+  return SS3D_OK;
+}
+
+// ---------------------------------------------------------------- full-grid transform (test export)
+extern "C" int ss3d_fft3d(double* a, int nx, int ny, int nz, int isign) {
+  if (!a) return fail(SS3D_EINVAL, "a is NULL");
+  if (isign != -1 && isign != 1) return fail(SS3D_EINVAL, "isign must be -1 or +1");
+  auto pow2 = [](int v) { return v >= 1 && (v & (v - 1)) == 0; };
+  if (!pow2(nx) || !pow2(ny) || !pow2(nz)) return fail(SS3D_EINVAL, "grid sizes must be powers of two");
+  if (ilog2i(nx) > MAX_LOGN_D || ilog2i(ny) > MAX_LOGN_D || ilog2i(nz) > MAX_LOGN_D)
+    return fail(SS3D_ETOOLARGE, "axis longer than the supported FP64 transform length (%d)", 1 << MAX_LOGN_D);
+  if ((double)nx * ny * nz > 134217728.0) return fail(SS3D_ETOOLARGE, "grid above 2^27 nodes");
+  int dev = 0;
+  CK(cudaGetDevice(&dev));
+  DevCtx* ctx;
+  int rc;
+  if ((rc = get_ctx(&ctx))) return rc;
+  const size_t n = (size_t)nx * ny * nz;
+  bool dev_a = false;
+  if ((rc = check_ptr(a, dev, 16, "a", &dev_a))) return rc;
+  cudaStream_t s = g_stream;
+  double2* d = reinterpret_cast<double2*>(a);
+  if (!dev_a) {
+    CK(cudaMallocAsync((void**)&d, sizeof(double2) * n, s));
+    cudaError_t e = cudaMemcpyAsync(d, a, sizeof(double2) * n, cudaMemcpyHostToDevice, s);
+    if (e != cudaSuccess) {
+      cudaFreeAsync(d, s);
+      return cuda_fail(e, "fft3d");
+    }
+  }
+  cudaError_t e = launch_fft3d(d, nx, ny, nz, isign, Tw{ctx->twf, ctx->twd}, s);
+  if (e == cudaSuccess && !dev_a) e = cudaMemcpyAsync(a, d, sizeof(double2) * n, cudaMemcpyDeviceToHost, s);
+  if (!dev_a) cudaFreeAsync(d, s);
+  if (e == cudaSuccess) e = cudaStreamSynchronize(s);
+  if (e != cudaSuccess) return cuda_fail(e, "fft3d");
   return SS3D_OK;
 }
 
@@ -939,9 +977,10 @@ extern "C" int ss3d_autotune(const ss3d_spectrum* sp, int igauss, int precision,
   int bestv[3] = {0, 0, 0};
   int rc = SS3D_OK;
   // variants per kind: 0-3 everywhere, FP32 column passes also 4-7 (two
-  // lines per thread), the row pass also 4 (rows held in warps); a kind with
+  // lines per thread), the FP32 middle pass also 8-9 (tiles staged by bulk
+  // tensor copies), the row pass also 4 (rows held in warps); a kind with
   // fewer variants runs its variant v mod 4 meanwhile
-  const int nvk[3] = {precision == SS3D_FP32 ? 8 : 4, precision == SS3D_FP32 ? 8 : 4, 5};
+  const int nvk[3] = {precision == SS3D_FP32 ? 10 : 4, precision == SS3D_FP32 ? 8 : 4, 5};
   const int nv = std::max(nvk[0], nvk[2]);
   auto vk = [&](int k, int v) { return v < nvk[k] ? v : v % 4; };
   for (int v = 0; v < nv && rc == SS3D_OK; v++) {
@@ -972,8 +1011,9 @@ extern "C" int ss3d_autotune(const ss3d_spectrum* sp, int igauss, int precision,
 }
 
 extern "C" int ss3d_set_variant(int kind, int precision, int logn, int variant) {
-  // 4-7: FP32 two-line column tiles; 4 of the row pass: rows held in warps
-  const int vmax = kind == 2 ? 4 : (precision == SS3D_FP32 ? 7 : 3);
+  // 4-7: FP32 two-line column tiles; 8, 9: FP32 middle pass staged by bulk
+  // tensor copies (one and two lines per thread); 4 of the row pass: rows held in warps
+  const int vmax = kind == 2 ? 4 : (precision == SS3D_FP32 ? (kind == 0 ? 9 : 7) : 3);
   if (kind < 0 || kind > 2 || (precision != SS3D_FP64 && precision != SS3D_FP32) || logn < 0 || logn > 15 ||
       variant < 0 || variant > vmax)
     return fail(SS3D_EINVAL, "invalid variant selection");

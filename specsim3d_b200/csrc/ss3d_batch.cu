@@ -200,6 +200,7 @@ struct ss3d_batch {
   size_t smem[3] = {0, 0, 0};
   cudaGraph_t graph = nullptr;
   cudaGraphExec_t exec = nullptr;
+  bool pipes = false;        // the graph holds kernels with bounded bulk-copy waits
   Tw tw{};
   const uint32_t* ptab = nullptr;
   std::vector<uint32_t> s0;
@@ -375,7 +376,9 @@ int capture(ss3d_batch* b) {
   if (e != cudaSuccess) return set_error(SS3D_ECUDA, cudaGetErrorString(e));
   e = cudaStreamBeginCapture(cs, cudaStreamCaptureModeRelaxed);
   if (e == cudaSuccess) {
+    const unsigned long long pipes0 = g_pipe_launches.load();
     cudaError_t e2 = enqueue(b, cs);
+    b->pipes = g_pipe_launches.load() != pipes0;
     e = cudaStreamEndCapture(cs, &b->graph);
     if (e2 != cudaSuccess) e = e2;
   }
@@ -573,6 +576,8 @@ extern "C" int ss3d_batch_run(ss3d_batch* b) {
   g_launch_count += (unsigned long long)b->kernels;
   if (e == cudaSuccess) e = cudaStreamSynchronize(st);
   if (e != cudaSuccess) return cuda_err(e, "batch run");
+  if (b->pipes && pipe_error_take(st))
+    return set_error(SS3D_ECUDA, "batch run: a bulk-copy wait of the middle pass timed out");
   return SS3D_OK;
 }
 
@@ -661,8 +666,9 @@ extern "C" int ss3d_batch_autotune(ss3d_batch* b) {
   for (int k : {1, 0, 2}) {
     int bestv = 0;
     float bestk = 1e30f;
-    // column passes 4-7: two-line tiles; row pass 4: rows held in warps
-    for (int v = 0; v < (k == 2 ? 5 : 8) && e == cudaSuccess; v++) {
+    // column passes 4-7: two-line tiles; middle pass 8-9: tiles staged by
+    // bulk tensor copies; row pass 4: rows held in warps
+    for (int v = 0; v < (k == 2 ? 5 : (k == 0 ? 10 : 8)) && e == cudaSuccess; v++) {
       for (int L = 0; L < 16; L++)
         if (used[k][L]) b->var[k][L] = v;
       e = time_run(b, st, ms, true);

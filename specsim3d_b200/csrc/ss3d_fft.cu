@@ -26,6 +26,7 @@
 #include "ss3d_bodies.cuh"
 #include "ss3d_engine.cuh"
 #include "ss3d_internal.h"
+#include "ss3d_tma.cuh"
 
 namespace ss3d {
 
@@ -88,6 +89,130 @@ __global__ void __launch_bounds__(AxisCfg<R, LOGN, V>::NTH, (col_min_blocks<R, L
     col_body_pair<LOGN, CF::TX, CF::TPC, SIGN>(a, g, in, out, tw, blockIdx.x, smraw);
   else
     col_body<R, LOGN, CF::TX, CF::TPC, SIGN>(a, g, in, out, tw, blockIdx.x, smraw);
+}
+
+// ---------------------------------------------------------------- middle pass fed by bulk tensor copies
+// Variants 8 (one line per thread) and 9 (two lines per thread as a cpair) of
+// the FP32 middle (y) pass.  A persistent CTA per SM walks the tiles of the
+// pass (LPT consecutive lines x N positions, 64 KB for N >= 128) in the item
+// order of col_body.  Tiles are staged by cp.async.bulk.tensor copies into two
+// shared-memory stages: while tile q is transformed from stage b, the copy of
+// the CTA's next tile lands in stage b ^ 1.  The first radix pass reads its
+// inputs from the stage, which then serves as the exchange buffer of the
+// later passes; the last pass stores the pruned outputs to global memory as
+// col_body does.  The butterflies are those of col_body / col_body_pair, so
+// the results are the same bits.
+__device__ int g_pipe_err;   // set when a copy wait of a pipelined kernel timed out
+
+template <int LOGN, int P> struct TmaCfg;
+template <int LOGN> struct TmaCfg<LOGN, 0> {
+  using CF = ColCfg<float, LOGN, 0>;
+  using C = float2;
+  static constexpr int N = CF::N, TX = CF::TX, TPC = CF::TPC, NTH = CF::NTH, LPT = CF::TX;
+};
+template <int LOGN> struct TmaCfg<LOGN, 1> {
+  using CF = PairCfg<LOGN, 0>;
+  using C = cpair;
+  static constexpr int N = CF::N, TX = CF::TX, TPC = CF::TPC, NTH = CF::NTH, LPT = 2 * CF::TX;
+};
+template <int LOGN, int P> struct TmaLayout : TmaCfg<LOGN, P> {
+  using B = TmaCfg<LOGN, P>;
+  static constexpr int ROWS = B::N < 256 ? B::N : 256;   // rows per copy (a box dimension is at most 256)
+  static constexpr int NBOX = B::N / ROWS;
+  static constexpr int STAGE = B::N * B::LPT * 8;        // bytes of one staged tile (= its exchange buffer)
+  static constexpr int TW_OFF = 2 * STAGE;
+  static constexpr int BAR_OFF = TW_OFF + B::N * (int)sizeof(typename B::C);
+  static constexpr size_t SMEM = BAR_OFF + 16 + 128;   // + room to align the stages on 128 bytes
+  static_assert(B::LPT * 8 % 16 == 0 && B::LPT <= 256, "box rows of whole 16-byte units, at most 256 elements");
+  static_assert(STAGE % 128 == 0, "stages on 128-byte boundaries");
+};
+
+template <int LOGN, int P>
+__global__ void __launch_bounds__(TmaCfg<LOGN, P>::NTH, 1)
+    k_col_tma(AxisArgs a, Geo g, float2* out, Tw tw, const __grid_constant__ CUtensorMap map, int ntiles) {
+  using L = TmaLayout<LOGN, P>;
+  using C = typename L::C;
+  constexpr int N = L::N, TX = L::TX, TPC = L::TPC, NTH = L::NTH, LPT = L::LPT;
+  constexpr int NR0 = N / Sched<LOGN>::radix(0);
+  extern __shared__ __align__(16) unsigned char smdyn[];
+  // bulk copies land on 128-byte boundaries: round the dynamic base up
+  unsigned char* smraw = smdyn + ((128u - (smem_addr(smdyn) & 127u)) & 127u);
+  C* stw = reinterpret_cast<C*>(smraw + L::TW_OFF);
+  uint64_t* bar = reinterpret_cast<uint64_t*>(smraw + L::BAR_OFF);
+  const int tid = threadIdx.x;
+  if (tid == 0) {
+    mbar_init(&bar[0], 1);
+    mbar_init(&bar[1], 1);
+    mbar_init_fence();
+  }
+  if constexpr (P == 1) {
+    load_tw_pair<N, NTH>(reinterpret_cast<cpair*>(stw), tw);
+  } else {
+    for (int q = tid; q < N; q += NTH) stw[q] = tw.f[N - 1 + q];
+  }
+  __syncthreads();
+  // tile q: realization r, group grp, first line line0 (the item order of col_body)
+  auto decode = [&](int q, int& r, int& grp, int& line0) {
+    r = q % a.nreal;
+    const int tt = q / a.nreal;
+    grp = tt / a.tpg;
+    line0 = (tt % a.tpg) * LPT;
+  };
+  auto issue = [&](int q, int b) {   // one thread: arm stage b's barrier and start the copies
+    int r, grp, line0;
+    decode(q, r, grp, line0);
+    unsigned char* dst = smraw + b * L::STAGE;
+    mbar_arrive_expect_tx(&bar[b], (uint32_t)L::STAGE);
+#pragma unroll
+    for (int k = 0; k < L::NBOX; ++k)
+      tma_load_3d(dst + k * L::ROWS * LPT * 8, &map, &bar[b], line0, k * L::ROWS, r * a.ngroups + grp);
+  };
+  int q = blockIdx.x;
+  if (tid == 0 && q < ntiles) issue(q, 0);
+  const int t = tid % TX;
+  const int S = (int)a.S;
+  const int nout = a.nout;
+  for (int it = 0; q < ntiles; q += gridDim.x, ++it) {
+    const int b = it & 1;
+    const uint32_t parity = (uint32_t)((it >> 1) & 1);
+    const bool ok = mbar_wait_bounded(&bar[b], parity);
+    if (__syncthreads_or(!ok)) {
+      // a copy did not arrive in time: report it, give it a bounded time to
+      // land in this CTA's shared memory, and stop
+      if (tid == 0) atomicExch(&g_pipe_err, 1);
+      mbar_wait_bounded(&bar[b], parity);
+      return;
+    }
+    if (tid == 0 && q + (int)gridDim.x < ntiles) issue(q + (int)gridDim.x, b ^ 1);
+    int r, grp, line0;
+    decode(q, r, grp, line0);
+    C* s = reinterpret_cast<C*>(smraw + b * L::STAGE);
+    if constexpr (P == 0) {
+      const bool valid = line_valid(g, line0 + t, a.lines);
+      float2* dst = out + ((long long)grp * a.gstride + line0 + t + (long long)r * a.rstride);
+      const float2* src = reinterpret_cast<const float2*>(s) + t;
+      fft_tile<LOGN, TX, TPC, +1, TX, true, false>(
+          s, stw, [&](int jb, int rr) { return src[(jb + rr * NR0) * TX]; },
+          [&](int pos, float2 v) {
+            if (valid && pos < nout) dst[pos * S] = v;
+          });
+    } else {
+      const int line = line0 + 2 * t;
+      const bool valid = line_valid(g, line, a.lines);
+      float4* dst = reinterpret_cast<float4*>(out + ((long long)grp * a.gstride + line + (long long)r * a.rstride));
+      const float4* src = reinterpret_cast<const float4*>(s) + t;
+      const int S2 = S / 2;
+      fft_tile<LOGN, TX, TPC, +1, TX, true, false>(
+          s, stw, [&](int jb, int rr) { return pair_of(src[(jb + rr * NR0) * TX]); },
+          [&](int pos, cpair v) {
+            if (valid && pos < nout) dst[pos * S2] = quad_of(v);
+          });
+    }
+    // the stage is refilled by a copy two tiles later: order this tile's
+    // shared-memory accesses before it
+    fence_proxy_async_smem();
+    __syncthreads();
+  }
 }
 
 // first inverse pass with the coefficient synthesis fused into the loader
@@ -293,6 +418,34 @@ __global__ void __launch_bounds__(NT) k_spec_rows(Model m, double dx, double dy,
   }
 }
 
+// c2c transform of nrows contiguous rows of length 2^LOGN in place, unscaled
+// (the x pass of the full-grid transform ss3d_fft3d): TX rows staged in
+// shared memory, the shared-memory Stockham engine, rows written back
+template <int LOGN, int SIGN>
+__global__ void __launch_bounds__(NT) k_rows_c2c(long long nrows, double2* __restrict__ a, Tw tw) {
+  using C = double2;
+  constexpr int N = 1 << LOGN;
+  constexpr int TX = RowTX<double, LOGN>::TX;
+  constexpr int PITCH = TX + 1;
+  extern __shared__ __align__(16) unsigned char smraw[];
+  C* s = reinterpret_cast<C*>(smraw);
+  C* stw = s + N * PITCH;
+  const long long row0 = (long long)blockIdx.x * TX;
+  load_tw(stw, tw.d, N, N);
+  for (int q = threadIdx.x; q < N * TX; q += NT) {
+    const int t = q / N, p = q % N;
+    const long long row = row0 + t;
+    s[p * PITCH + t] = row < nrows ? a[row * N + p] : cmk<C>(0.0, 0.0);
+  }
+  __syncthreads();
+  smem_fft<LOGN, TX, PITCH, NT, SIGN, 1>(s, stw);
+  for (int q = threadIdx.x; q < N * TX; q += NT) {
+    const int t = q / N, p = q % N;
+    const long long row = row0 + t;
+    if (row < nrows) a[row * N + p] = s[p * PITCH + t];
+  }
+}
+
 // npx == 1: X[0] = c(0, j, k)
 __global__ void k_spec_rows_n1(Model m, double dx, double dy, double dz, Geo g, double2* __restrict__ out) {
   const int nrows = g.npy * g.npz;
@@ -453,6 +606,89 @@ static cudaError_t run_axis_c2c_v(const AxisArgs& a, const Geo& g, const cpx_t<R
   }
 }
 
+// ---- host side of the pipelined middle pass
+std::atomic<unsigned long long> g_pipe_launches{0};
+
+namespace {
+using EncodeTiledFn = CUresult (*)(CUtensorMap*, CUtensorMapDataType, cuuint32_t, void*, const cuuint64_t*,
+                                   const cuuint64_t*, const cuuint32_t*, const cuuint32_t*, CUtensorMapInterleave,
+                                   CUtensorMapSwizzle, CUtensorMapL2promotion, CUtensorMapFloatOOBfill);
+EncodeTiledFn encode_tiled() {
+  static EncodeTiledFn fn = [] {
+    void* p = nullptr;
+    cudaDriverEntryPointQueryResult q;
+    if (cudaGetDriverEntryPoint("cuTensorMapEncodeTiled", &p, cudaEnableDefault, &q) != cudaSuccess ||
+        q != cudaDriverEntryPointSuccess)
+      p = nullptr;
+    cudaGetLastError();
+    return reinterpret_cast<EncodeTiledFn>(p);
+  }();
+  return fn;
+}
+}  // namespace
+
+// whether the pipelined pass can take this pass: the middle (y) pass in place
+// over groups of N rows of pitch S, realizations back to back, 16-byte rows
+static bool tma_pass_ok(const AxisArgs& a, int n, const void* in, const void* out) {
+  return a.axis == 1 && in == out && a.gstride == (long long)n * a.S &&
+         (a.nreal == 1 || a.rstride == (long long)a.ngroups * a.gstride) && (a.S * 8) % 16 == 0 &&
+         ((uintptr_t)out % 16) == 0 && (long long)a.ngroups * a.nreal < (1LL << 31) && encode_tiled() != nullptr;
+}
+
+template <int L, int P>
+static cudaError_t run_axis_c2c_tma(const AxisArgs& a, const Geo& g, float2* out, Tw tw, cudaStream_t st) {
+  using LY = TmaLayout<L, P>;
+  CUtensorMap map;
+  const cuuint64_t dims[3] = {(cuuint64_t)a.S, (cuuint64_t)LY::N, (cuuint64_t)a.ngroups * (cuuint64_t)a.nreal};
+  const cuuint64_t strides[2] = {(cuuint64_t)a.S * 8, (cuuint64_t)a.gstride * 8};
+  const cuuint32_t box[3] = {(cuuint32_t)LY::LPT, (cuuint32_t)LY::ROWS, 1};
+  const cuuint32_t estr[3] = {1, 1, 1};
+  // complex FP32 values move as 8-byte elements; columns past the row pitch read as zeros
+  if (encode_tiled()(&map, CU_TENSOR_MAP_DATA_TYPE_FLOAT64, 3, out, dims, strides, box, estr,
+                     CU_TENSOR_MAP_INTERLEAVE_NONE, CU_TENSOR_MAP_SWIZZLE_NONE, CU_TENSOR_MAP_L2_PROMOTION_L2_256B,
+                     CU_TENSOR_MAP_FLOAT_OOB_FILL_NONE) != CUDA_SUCCESS)
+    return cudaErrorInvalidValue;
+  auto kern = k_col_tma<L, P>;
+  cudaError_t e = func_smem(reinterpret_cast<const void*>(kern), LY::SMEM);
+  if (e != cudaSuccess) return e;
+  static int occ[2][16] = {};   // resident CTAs per SM, per variant and length (same on every B200)
+  int& o = occ[P][L];
+  if (o == 0) {
+    e = cudaOccupancyMaxActiveBlocksPerMultiprocessor(&o, kern, LY::NTH, LY::SMEM);
+    if (e != cudaSuccess) return e;
+    o = std::max(o, 1);
+  }
+  int dev = 0, nsm = 148;
+  cudaGetDevice(&dev);
+  cudaDeviceGetAttribute(&nsm, cudaDevAttrMultiProcessorCount, dev);
+  AxisArgs b = a;
+  b.tpg = (a.lines + LY::LPT - 1) / LY::LPT;
+  const long long ntiles = (long long)b.tpg * a.ngroups * a.nreal;
+  if (ntiles <= 0) return cudaSuccess;
+  if (ntiles >= (1LL << 31)) return cudaErrorInvalidValue;
+  const int grid = (int)std::min<long long>(ntiles, (long long)nsm * o);
+  kern<<<grid, LY::NTH, LY::SMEM, st>>>(b, g, out, tw, map, (int)ntiles);
+  ++g_launch_count;
+  ++g_pipe_launches;
+  return cudaGetLastError();
+}
+
+// Reads and clears the flag a timed-out copy wait leaves behind; true if set.
+bool pipe_error_take(cudaStream_t st) {
+  int v = 0;
+  if (cudaMemcpyFromSymbolAsync(&v, g_pipe_err, sizeof v, 0, cudaMemcpyDeviceToHost, st) != cudaSuccess ||
+      cudaStreamSynchronize(st) != cudaSuccess) {
+    cudaGetLastError();
+    return true;
+  }
+  if (v) {
+    const int zero = 0;
+    cudaMemcpyToSymbolAsync(g_pipe_err, &zero, sizeof zero, 0, cudaMemcpyHostToDevice, st);
+    cudaStreamSynchronize(st);
+  }
+  return v != 0;
+}
+
 template <typename R, int L, int V>
 static cudaError_t run_axis_gen_v(const AxisArgs& a, const Geo& g, const R* amp, const uint32_t* rs,
                                   const uint32_t* apow, cpx_t<R>* out, Tw tw, cudaStream_t st) {
@@ -529,6 +765,17 @@ static cudaError_t run_axis_c2c(const AxisArgs& a, const Geo& g, const cpx_t<R>*
         case 6: return run_axis_c2c_v<R, L, SIGN, 6>(a, g, in, out, tw, st);
         case 7: return run_axis_c2c_v<R, L, SIGN, 7>(a, g, in, out, tw, st);
         default: break;
+      }
+      // 8, 9: tiles staged by bulk tensor copies (inverse middle pass only;
+      // other passes run the same tile shape with direct loads)
+      const int v = g_variant[0][1][L];
+      if (SIGN > 0 && (v == 8 || v == 9)) {
+        if (tma_pass_ok(a, 1 << L, in, out)) {
+          if (v == 8) return run_axis_c2c_tma<L, 0>(a, g, reinterpret_cast<float2*>(out), tw, st);
+          return run_axis_c2c_tma<L, 1>(a, g, reinterpret_cast<float2*>(out), tw, st);
+        }
+        if (v == 8) return run_axis_c2c_v<R, L, SIGN, 0>(a, g, in, out, tw, st);
+        return run_axis_c2c_v<R, L, SIGN, 4>(a, g, in, out, tw, st);
       }
     }
   }
@@ -657,6 +904,81 @@ cudaError_t launch_spectrum(const Model& m, const double d[3], const Geo& g, dou
   k_reduce_spec<<<1, RS_NT, 0, st>>>(part, nb, result);
   ++g_launch_count;
   return cudaGetLastError();
+}
+
+template <int L, int SIGN>
+static cudaError_t run_rows_c2c(long long nrows, double2* a, Tw tw, cudaStream_t st) {
+  if constexpr (L == 0) {
+    return cudaSuccess;   // length-1 rows: identity
+  } else {
+    constexpr int TX = RowTX<double, L>::TX;
+    constexpr int N = 1 << L;
+    const size_t smem = (size_t)(N * (TX + 1) + N) * sizeof(double2);
+    cudaError_t e = set_smem(k_rows_c2c<L, SIGN>, smem);
+    if (e != cudaSuccess) return e;
+    const long long nblk = (nrows + TX - 1) / TX;
+    if (nblk > 0x7fffffffLL) return cudaErrorInvalidValue;
+    k_rows_c2c<L, SIGN><<<(unsigned)nblk, NT, smem, st>>>(nrows, a, tw);
+    ++g_launch_count;
+    return cudaGetLastError();
+  }
+}
+
+// Unscaled 3D c2c transform of a full complex grid a[nz][ny][nx] in place
+// (fft3d, f90:254-304): isign -1 forward (e^{-i}), +1 inverse; every axis a
+// power of two up to 2^MAX_LOGN_D.
+cudaError_t launch_fft3d(double2* a, int nx, int ny, int nz, int isign, Tw tw, cudaStream_t st) {
+  const int Lx = ilog2(nx), Ly = ilog2(ny), Lz = ilog2(nz);
+  if ((1 << Lx) != nx || (1 << Ly) != ny || (1 << Lz) != nz) return cudaErrorInvalidValue;
+  Geo g{};
+  g.npx = g.nx = nx;
+  g.npy = g.ny = ny;
+  g.npz = g.nz = nz;
+  g.H = g.HP = nx;   // full rows: every line of a plane is valid
+  cudaError_t e = cudaErrorInvalidValue;
+  const long long rows = (long long)ny * nz;
+  if (isign < 0) {
+    SS3D_LOGN_SWITCH(Lx, MAX_LOGN_D, e = (run_rows_c2c<L, -1>(rows, a, tw, st)));
+  } else {
+    SS3D_LOGN_SWITCH(Lx, MAX_LOGN_D, e = (run_rows_c2c<L, +1>(rows, a, tw, st)));
+  }
+  if (e != cudaSuccess) return e;
+  if (ny > 1) {
+    AxisArgs b{};
+    b.S = nx;
+    b.nout = ny;
+    b.lines = nx;
+    b.ngroups = nz;
+    b.gstride = (long long)nx * ny;
+    b.rstride = 0;
+    b.nreal = 1;
+    b.axis = 1;
+    e = cudaErrorInvalidValue;
+    if (isign < 0) {
+      SS3D_LOGN_SWITCH(Ly, MAX_LOGN_D, e = (run_axis_c2c<double, L, -1>(b, g, a, a, tw, st)));
+    } else {
+      SS3D_LOGN_SWITCH(Ly, MAX_LOGN_D, e = (run_axis_c2c<double, L, +1>(b, g, a, a, tw, st)));
+    }
+    if (e != cudaSuccess) return e;
+  }
+  if (nz > 1) {
+    AxisArgs c{};
+    c.S = (long long)nx * ny;
+    c.nout = nz;
+    c.lines = nx * ny;
+    c.ngroups = 1;
+    c.gstride = 0;
+    c.rstride = 0;
+    c.nreal = 1;
+    c.axis = 2;
+    e = cudaErrorInvalidValue;
+    if (isign < 0) {
+      SS3D_LOGN_SWITCH(Lz, MAX_LOGN_D, e = (run_axis_c2c<double, L, -1>(c, g, a, a, tw, st)));
+    } else {
+      SS3D_LOGN_SWITCH(Lz, MAX_LOGN_D, e = (run_axis_c2c<double, L, +1>(c, g, a, a, tw, st)));
+    }
+  }
+  return e;
 }
 
 cudaError_t launch_rowstates(const Geo& g, uint32_t s0, long long r_first, int nreal, const uint32_t* ptab,

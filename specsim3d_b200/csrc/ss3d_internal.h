@@ -74,6 +74,11 @@ void mark(Marks* m, int stage, cudaStream_t st);   // records an event opening `
 // streams can make the call wait for them, so repeated calls return at once.
 cudaError_t func_smem(const void* kernel, size_t bytes);
 extern std::atomic<unsigned long long> g_launch_count;   // kernels launched by the library (all threads)
+// launches of kernels that stage tiles with bulk copies and bounded waits;
+// after work that contains one, pipe_error_take reads (and clears) the flag a
+// timed-out wait leaves, synchronising the stream
+extern std::atomic<unsigned long long> g_pipe_launches;
+bool pipe_error_take(cudaStream_t st);
 
 // ---- launchers (ss3d_fft.cu); all return cudaError_t of the last launch
 cudaError_t launch_spectrum(const Model& m, const double d[3], const Geo& g, double2* work, double* amp64,
@@ -91,6 +96,7 @@ cudaError_t launch_realize(const Geo& g, const R* amp, const uint32_t* rowstates
 template <typename R>
 cudaError_t launch_gen(const Geo& g, const R* amp, const uint32_t* rowstates, const uint32_t* apow,
                        cpx_t<R>* work, long long wstride, int nreal, cudaStream_t st);
+cudaError_t launch_fft3d(double2* a, int nx, int ny, int nz, int isign, Tw tw, cudaStream_t st);
 cudaError_t launch_reduce_zstats(const double* part, int nblk_per_r, int nreal, double* zsum, cudaStream_t st);
 int realize_part_blocks(const Geo& g, bool dbl);
 

@@ -177,6 +177,7 @@ extern "C" int ss3d_realize_noalloc(const ss3d_spectrum* sp, int iseed, int64_t 
   const uint32_t s0 = (uint32_t)(a % 2147483646LL + 1);
   const size_t M = (size_t)g.nx * g.ny * g.nz;
   cudaStream_t st = current_stream();
+  const unsigned long long pipes0 = g_pipe_launches.load();
   for (int r = 0; r < nreal && e == cudaSuccess; ++r) {
     e = launch_rowstates(g, s0, r_first + r, 1, ptab, rs, r == 0 ? apow : nullptr, st);
     void* dst = (char*)out + (size_t)r * M * oel;
@@ -194,5 +195,7 @@ extern "C" int ss3d_realize_noalloc(const ss3d_spectrum* sp, int iseed, int64_t 
     cudaGetLastError();
     return fail(SS3D_ECUDA, std::string("realize_noalloc: ") + cudaGetErrorString(e));
   }
+  if (g_pipe_launches.load() != pipes0 && pipe_error_take(st))
+    return fail(SS3D_ECUDA, "realize_noalloc: a bulk-copy wait of the middle pass timed out");
   return SS3D_OK;
 }

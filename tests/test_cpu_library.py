@@ -121,8 +121,9 @@ def test_gpu_calls_without_gpu_report_cuda_error():
 
 def test_variant_selection_ranges():
     """ss3d_set_variant (host only): 0-3 for every pass; 4-7 for the FP32 column
-    passes (two lines per thread); 4 for the row pass in both precisions (rows
-    held in warps); anything else is refused."""
+    passes (two lines per thread); 8-9 for the FP32 middle pass (tiles staged
+    by bulk tensor copies); 4 for the row pass in both precisions (rows held in
+    warps); anything else is refused."""
     from specsim3d_b200 import _lib
     import specsim3d_b200 as ss
     L = _lib.lib()
@@ -137,8 +138,12 @@ def test_variant_selection_ranges():
             assert L.ss3d_set_variant(3, prec, 8, 0) != 0
         for kind in (0, 1):
             assert L.ss3d_set_variant(kind, ss.FP32, 8, 7) == 0
-            assert L.ss3d_set_variant(kind, ss.FP32, 8, 8) != 0
             assert L.ss3d_set_variant(kind, ss.FP64, 8, 4) != 0
+        # middle pass only: 8, 9 stage their tiles with bulk tensor copies (FP32)
+        assert L.ss3d_set_variant(0, ss.FP32, 8, 9) == 0
+        assert L.ss3d_set_variant(0, ss.FP32, 8, 10) != 0
+        assert L.ss3d_set_variant(1, ss.FP32, 8, 8) != 0
+        assert L.ss3d_set_variant(0, ss.FP64, 8, 8) != 0
     finally:
         for prec in (ss.FP32, ss.FP64):
             for kind in (0, 1, 2):

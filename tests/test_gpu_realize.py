@@ -161,7 +161,7 @@ def test_tile_variants_give_identical_results(gpu):
         for kind, logn in ((0, 7), (1, 5), (2, 6)):
             L.ss3d_set_variant(kind, prec, logn, 0)
     chosen = gpu.autotune(sp, 1, gpu.FP32, 2)
-    assert chosen["row_pass"] in {0, 1, 2, 3, 4} and set(chosen.values()) <= set(range(8))
+    assert chosen["row_pass"] in {0, 1, 2, 3, 4} and set(chosen.values()) <= set(range(10))
     assert np.array_equal(sp.realize(77, 2, 1, gpu.FP32), sp.realize(77, 2, 1, gpu.FP32))
 
 
@@ -195,8 +195,9 @@ def test_two_line_variants_identical(gpu, n, ipad, igauss):
                 assert L.ss3d_set_variant(kind, gpu.FP32, lg, v) == 0
             got = sp.realize(4321, 3, igauss, gpu.FP32, dtype=np.float32)
             assert np.array_equal(got, ref), (v, float(np.max(np.abs(got - ref))))
-        # mixed: synthesis on two lines, middle pass on one, and the reverse
-        for vs, vm in ((4, 0), (0, 6), (5, 1), (7, 5)):
+        # mixed: synthesis on two lines, middle pass on one, and the reverse;
+        # middle pass 8 and 9: tiles staged by bulk tensor copies
+        for vs, vm in ((4, 0), (0, 6), (5, 1), (7, 5), (0, 8), (6, 9), (4, 8)):
             for kind, lg in kinds:
                 L.ss3d_set_variant(kind, gpu.FP32, lg, vs if kind == 1 else vm)
             assert np.array_equal(sp.realize(4321, 3, igauss, gpu.FP32, dtype=np.float32), ref)
@@ -204,7 +205,8 @@ def test_two_line_variants_identical(gpu, n, ipad, igauss):
         for kind, lg in kinds:
             L.ss3d_set_variant(kind, gpu.FP32, lg, 0)
     assert L.ss3d_set_variant(2, gpu.FP32, 6, 5) != 0      # the row pass has no two-line tiles
-    assert L.ss3d_set_variant(0, gpu.FP32, 6, 8) != 0
+    assert L.ss3d_set_variant(1, gpu.FP32, 6, 8) != 0      # bulk-copy tiles: middle pass only
+    assert L.ss3d_set_variant(0, gpu.FP32, 6, 10) != 0
 
 
 @pytest.mark.parametrize("prec", ["FP32", "FP64"])
@@ -288,3 +290,34 @@ def test_misaligned_device_output_is_refused(gpu):
     got = sp.realize(7, 1, 0, gpu.FP32, out=host[1:].reshape(1, n[2], n[1], n[0]))
     assert np.array_equal(got, sp.realize(7, 1, 0, gpu.FP32, dtype=np.float32))
     sp.close()
+
+
+@pytest.mark.parametrize("n", [(64, 64, 16), (256, 256, 8), (40, 36, 20), (30, 20, 9), (128, 100, 3)])
+def test_bulk_copy_middle_pass_identical(gpu, n):
+    """Middle pass variants 8 and 9 (tiles staged in shared memory by bulk
+    tensor copies, two-stage pipeline in a persistent CTA) give the bits of the
+    direct-load tiles, through ss3d_realize (several realizations per launch),
+    and the batched form (graph capture) on the same grid."""
+    import torch
+    from specsim3d_b200 import _lib
+    L = _lib.lib()
+    sts = [(3, 1.0, 14.0, 9.0, 5.0, 35.0, 10.0, 5.0)]
+    sp = gpu.Spectrum(sts, 0.1, (1.0, 1.0, 1.0), n, 1)
+    if sp.np[2] == 1 or sp.np[1] == 1:
+        pytest.skip("no middle pass on this grid")
+    lg = int(sp.np[1]).bit_length() - 1
+    if not 5 <= lg <= 10:
+        pytest.skip("middle-pass length outside the tuned range")
+    ref = sp.realize(2468, 3, 1, gpu.FP32, dtype=np.float32)
+    try:
+        for v in (8, 9):
+            assert L.ss3d_set_variant(0, gpu.FP32, lg, v) == 0
+            got = sp.realize(2468, 3, 1, gpu.FP32, dtype=np.float32)
+            assert np.array_equal(got, ref), (v, float(np.max(np.abs(got - ref))))
+            out = torch.empty((3, n[2], n[1], n[0]), dtype=torch.float32, device="cuda")
+            b = gpu.Batch([(sp, 2468, 1, 0, 3, out)])
+            b.run()
+            b.close()
+            assert np.array_equal(out.cpu().numpy(), ref)
+    finally:
+        L.ss3d_set_variant(0, gpu.FP32, lg, 0)
