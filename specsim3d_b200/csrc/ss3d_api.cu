@@ -464,7 +464,7 @@ extern "C" int ss3d_spectrum_create(const ss3d_struct* st, int nst, double nugge
   cudaStream_t s = g_stream;
   double2* work = nullptr;
   SpecPartial* part = nullptr;
-  const int npart = 148 * 8;
+  const int npart = spectrum_parts(g) - 1;
   // temporaries come from the stream-ordered pool: no device-wide synchronisation
   // when they are freed, so that other threads' streams keep running
   cudaError_t e = cudaMallocAsync((void**)&work, sizeof(double2) * nh, s);

@@ -23,6 +23,7 @@
 #include <cstdio>
 #include <cstring>
 #include <string>
+#include <type_traits>
 #include <vector>
 
 #include "../../include/specsim3d_gpu.h"
@@ -114,6 +115,24 @@ __device__ __forceinline__ double cov_lat(const CovTab& T, const KModel& m, int 
   return cov_k(m, (double)di * dx, (double)dj * dy, (double)dk * dz);
 }
 
+// the same lookup with the out-of-table case as a call on a model in global
+// memory (keeps the kernels that unroll their fills small)
+__device__ __noinline__ double cov_lag_direct(const KModel* __restrict__ m, int di, int dj, int dk, double dx,
+                                              double dy, double dz) {
+  return cov_k(*m, (double)di * dx, (double)dj * dy, (double)dk * dz);
+}
+__device__ __forceinline__ double cov_lat_g(const CovTab& T, const KModel* __restrict__ m, int di, int dj, int dk,
+                                            double dx, double dy, double dz) {
+  if (dk < 0) {
+    di = -di;
+    dj = -dj;
+    dk = -dk;
+  }
+  if (T.v && dk <= T.tz && abs(dj) <= T.ty && abs(di) <= T.tx)
+    return __ldg(T.v + (di + T.tx) + (size_t)(2 * T.tx + 1) * ((dj + T.ty) + (size_t)(2 * T.ty + 1) * dk));
+  return cov_lag_direct(m, di, dj, dk, dx, dy, dz);
+}
+
 __global__ void k_cov_table(KModel m, double dx, double dy, double dz, int tx, int ty, int tz, double* __restrict__ v) {
   const long long wx = 2 * tx + 1, wy = 2 * ty + 1, tot = wx * wy * (tz + 1);
   for (long long q = blockIdx.x * (long long)blockDim.x + threadIdx.x; q < tot; q += (long long)gridDim.x * blockDim.x) {
@@ -143,7 +162,10 @@ __device__ __forceinline__ float rsqrt_nr(float x) {
 }
 
 // neighbour search of nodes [node0, node0 + count): writes nn and the
-// neighbour ids (0-based data index) and flags the exact data nodes
+// neighbour ids (0-based data index) and flags the exact data nodes.  CAP >=
+// ndmax bounds the per-thread candidate list (local memory): a list of 100
+// entries for ndmax 24 spilled about 400 bytes per node to DRAM.
+template <int CAP>
 __global__ void k_cond_search(CondGeo G, long long node0, int count, const double* __restrict__ dxs,
                               const double* __restrict__ dys, const double* __restrict__ dzs,
                               const int* __restrict__ sbstart, const int* __restrict__ sbidx,
@@ -161,8 +183,8 @@ __global__ void k_cond_search(CondGeo G, long long node0, int count, const doubl
   const int bx = clampi((int)__ddiv_rn(__dadd_rn(__dsub_rn(x, G.xmin), __dmul_rn(0.5, G.dx)), G.bsx) + 1, 1, G.nsbx);
   const int by = clampi((int)__ddiv_rn(__dadd_rn(__dsub_rn(y, G.ymin), __dmul_rn(0.5, G.dy)), G.bsy) + 1, 1, G.nsby);
   const int bz = clampi((int)__ddiv_rn(__dadd_rn(__dsub_rn(z, G.zmin), __dmul_rn(0.5, G.dz)), G.bsz) + 1, 1, G.nsbz);
-  double cd[100];
-  int cid[100];
+  double cd[CAP];
+  int cid[CAP];
   int nn = 0;
   const int ndmax = G.ndmax;
   for (int kb = max(1, bz - G.mbz); kb <= min(G.nsbz, bz + G.mbz); ++kb)
@@ -431,6 +453,206 @@ __global__ void k_cond_krige(CondGeo G, KModel mdl, CovTab ctab, long long node0
     for (int l = lane; l < G.nreal; l += 32) {
       double sks = 0.0;
       for (int p = 0; p < nn; ++p) sks += w[p] * simd[id[p] + (long long)G.nd * l];
+      res[node + M * l] = zk + res[node + M * l] - sks;
+    }
+    __syncwarp();
+  }
+  __syncthreads();
+  if (threadIdx.x < 4 && bcount[threadIdx.x]) atomicAdd(&counters[threadIdx.x], bcount[threadIdx.x]);
+}
+
+// ---------------------------------------------------------------- kriging, rows in registers
+// The same kriging for ndmax <= 32, with the system of a node held by one warp
+// in registers: lane r owns row r of the covariance matrix (NDT >= ndmax
+// doubles, or floats in the FP32 form).  Column step c of the right-looking
+// Cholesky: the pivot comes from lane c by a shuffle, each lane scales its
+// element of column c by the pivot's reciprocal square root, the scaled
+// column goes to a shared-memory vector (two alternating buffers, one warp
+// barrier per column) and every lane updates its row with it from registers.
+// The forward substitution L y = b runs in the same loop; the back
+// substitution L^T w = y reads the transpose of L from shared memory.  Lanes
+// and columns past the node's neighbour count hold values that no valid
+// entry ever reads.  FP32 form: FP32 factor and solves, the FP64 matrix kept
+// in shared memory for the residual of one refinement step.  Same ridge rule,
+// neighbour order and counters as k_cond_krige.
+template <int PREC, int NDT> struct KregLayout {
+  using T = typename std::conditional<PREC == 0, double, float>::type;
+  static constexpr int PITCH = NDT + 1;
+  static constexpr int LAT = 0;                                            // int4 per neighbour
+  static constexpr int W = LAT + 16 * NDT;                                 // double w
+  static constexpr int COL = W + 8 * NDT;                                  // 2 x 32 T
+  static constexpr int LS = COL + 2 * 32 * (int)sizeof(T);                 // NDT x PITCH T (transpose of L)
+  static constexpr int AS = (LS + NDT * PITCH * (int)sizeof(T) + 15) & ~15; // NDT x PITCH double (FP32 form)
+  static constexpr int BYTES = ((PREC == 0 ? AS : AS + NDT * PITCH * 8) + 15) & ~15;
+};
+
+template <int PREC, int NDT>
+__global__ void __launch_bounds__(256, 2) k_cond_krige_reg(CondGeo G, const KModel* __restrict__ mdl, CovTab ctab,
+                                                        long long node0,
+                                                        int count, const int* __restrict__ nbr,
+                                                        const int* __restrict__ nnb, const int* __restrict__ ixs,
+                                                        const int* __restrict__ iys, const int* __restrict__ izs,
+                                                        const double* __restrict__ dg,
+                                                        const double* __restrict__ simd, double* __restrict__ res,
+                                                        unsigned long long* __restrict__ counters) {
+  using Ly = KregLayout<PREC, NDT>;
+  using T = typename Ly::T;
+  constexpr int PITCH = Ly::PITCH;
+  extern __shared__ __align__(16) unsigned char smk[];
+  __shared__ unsigned long long bcount[4];
+  const int lane = threadIdx.x & 31, wib = threadIdx.x >> 5;
+  const int nwb = blockDim.x >> 5;
+  if (threadIdx.x < 4) bcount[threadIdx.x] = 0;
+  __syncthreads();
+  unsigned char* mine = smk + (size_t)Ly::BYTES * wib;
+  int4* lat = reinterpret_cast<int4*>(mine + Ly::LAT);
+  double* wsm = reinterpret_cast<double*>(mine + Ly::W);
+  T* colb = reinterpret_cast<T*>(mine + Ly::COL);
+  T* Ls = reinterpret_cast<T*>(mine + Ly::LS);
+  double* As = reinterpret_cast<double*>(mine + Ly::AS);   // FP32 form only
+  const long long M = (long long)G.nx * G.ny * G.nz;
+  for (int q = blockIdx.x * nwb + wib; q < count; q += gridDim.x * nwb) {
+    const long long node = node0 + q;
+    const int code = nnb[q];
+    const int nn = code & 0xffff, exact = code >> 16;
+    if (lane == 0) atomicAdd_block(&bcount[0], (unsigned long long)nn);
+    if (nn == 0) {
+      if (lane == 0) atomicAdd_block(&bcount[2], 1ull);
+      continue;
+    }
+    const int* nl = nbr + (long long)q * G.ndmax;
+    if (exact) {
+      const double v = dg[nl[0]];
+      for (int l = lane; l < G.nreal; l += 32) res[node + M * l] = v;
+      if (lane == 0) atomicAdd_block(&bcount[3], 1ull);
+      continue;
+    }
+    // a conditioned grid has at most 2^27 nodes: 32-bit index arithmetic
+    const uint32_t nu = (uint32_t)node, row = nu / (uint32_t)G.nx;
+    const int i = (int)(nu - row * (uint32_t)G.nx), j = (int)(row % (uint32_t)G.ny), k = (int)(row / (uint32_t)G.ny);
+    const bool act = lane < nn;
+    int4 me = make_int4(0, 0, 0, 0);
+    if (act) {
+      const int cp = nl[lane];
+      me = make_int4(__ldg(ixs + cp) - 1, __ldg(iys + cp) - 1, __ldg(izs + cp) - 1, cp);
+      lat[lane] = me;
+    }
+    __syncwarp();
+    const double b = act ? cov_lat_g(ctab, mdl, me.x - i, me.y - j, me.z - k, G.dx, G.dy, G.dz) : 0.0;
+    // row `lane` of A in shared memory (FP64 in As for the FP32 form, else in Ls)
+    if (lane < NDT) {
+      for (int c = 0; c < NDT; ++c) {
+        double v = 0.0;
+        if (c < nn && act) {
+          const int4 o = lat[c];
+          v = cov_lat_g(ctab, mdl, me.x - o.x, me.y - o.y, me.z - o.z, G.dx, G.dy, G.dz);
+        }
+        if constexpr (PREC == 1)
+          As[lane * PITCH + c] = v;
+        else
+          Ls[lane * PITCH + c] = v;
+      }
+    }
+    double ridge = 1.0e-10 * G.c0;
+    T a[NDT];
+    T myinv = T(0), yv = T(0);
+    bool good = false;
+    int tries;
+    for (tries = 1; tries <= 3; ++tries) {
+      // row `lane` of A + ridge I into registers (identity rows for lanes past nn)
+#pragma unroll
+      for (int c = 0; c < NDT; ++c) {
+        double v = 0.0;
+        if (lane < NDT) v = PREC == 1 ? As[lane * PITCH + c] : (double)Ls[lane * PITCH + c];
+        if (c == lane) v = act ? v + ridge : 1.0;
+        a[c] = (T)v;
+      }
+      T bcur = (T)b;
+      good = true;
+#pragma unroll
+      for (int c = 0; c < NDT; ++c) {
+        if (c < nn) {
+          const T piv = __shfl_sync(0xffffffffu, a[c], c);
+          if (!(piv > T(0))) {   // the same value in every lane: a uniform exit
+            good = false;
+            break;
+          }
+          const T inv = rsqrt_nr(piv);
+          const T lrc = a[c] * inv;
+          a[c] = lrc;
+          if (lane == c) myinv = inv;
+          T* cb = colb + (c & 1) * 32;
+          cb[lane] = lrc;
+          __syncwarp();
+          const T yc = __shfl_sync(0xffffffffu, bcur * inv, c);
+          if (lane == c) yv = yc;
+          bcur = fma(-lrc, yc, bcur);
+#pragma unroll
+          for (int kk = c + 1; kk < NDT; ++kk) a[kk] = fma(-lrc, cb[kk], a[kk]);
+        }
+      }
+      if (good) break;
+      ridge = ridge * 1.0e3;
+      __syncwarp();
+    }
+    if (!good) {
+      if (lane == 0) atomicAdd_block(&bcount[1], 1ull);
+      continue;
+    }
+    if (tries > 1 && lane == 0) atomicAdd_block(&bcount[1], 1ull);
+    // back substitution L^T w = y with the transpose of L in shared memory
+    if (lane < NDT) {
+#pragma unroll
+      for (int c = 0; c < NDT; ++c) Ls[lane * PITCH + c] = a[c];
+    }
+    __syncwarp();
+    T acc = yv, w = T(0);
+#pragma unroll
+    for (int r = NDT - 1; r >= 0; --r) {
+      if (r < nn) {
+        const T wr = __shfl_sync(0xffffffffu, acc * myinv, r);
+        if (lane == r) w = wr;
+        if (lane < r) acc = fma(-Ls[r * PITCH + lane], wr, acc);
+      }
+    }
+    if (act) wsm[lane] = (double)w;
+    __syncwarp();
+    if constexpr (PREC == 1) {
+      // one refinement: residual b - (A + ridge I) w in FP64, then
+      // L L^T d = residual in FP32 and w += d
+      double rres = 0.0;
+      if (act) {
+        rres = b - ridge * wsm[lane];
+        for (int c = 0; c < nn; ++c) rres -= As[lane * PITCH + c] * wsm[c];
+      }
+      T dcur = (T)rres, dy = T(0);
+#pragma unroll
+      for (int c = 0; c < NDT; ++c) {
+        if (c < nn) {
+          const T yc = __shfl_sync(0xffffffffu, dcur * myinv, c);
+          if (lane == c) dy = yc;
+          dcur = fma(-a[c], yc, dcur);
+        }
+      }
+      T acc2 = dy, d = T(0);
+#pragma unroll
+      for (int r = NDT - 1; r >= 0; --r) {
+        if (r < nn) {
+          const T wr = __shfl_sync(0xffffffffu, acc2 * myinv, r);
+          if (lane == r) d = wr;
+          if (lane < r) acc2 = fma(-Ls[r * PITCH + lane], wr, acc2);
+        }
+      }
+      __syncwarp();
+      if (act) wsm[lane] += (double)d;
+      __syncwarp();
+    }
+    double zk = act ? wsm[lane] * dg[me.w] : 0.0;   // sum of w dg: a butterfly over the lanes
+#pragma unroll
+    for (int off = 16; off > 0; off >>= 1) zk += __shfl_xor_sync(0xffffffffu, zk, off);
+    for (int l = lane; l < G.nreal; l += 32) {
+      double sks = 0.0;
+      for (int p = 0; p < nn; ++p) sks += wsm[p] * simd[lat[p].w + (long long)G.nd * l];
       res[node + M * l] = zk + res[node + M * l] - sks;
     }
     __syncwarp();
@@ -829,34 +1051,63 @@ extern "C" int ss3d_condition(double* res, const int n[3], int nreal, const doub
       ctab = CovTab{dctab, tx, ty, tz};
     }
   }
-  // kriging CTAs: warps per block limited by the shared memory of one warp
-  const size_t per = cond_warp_bytes(cp->ndmax, precision == SS3D_FP64 ? 0 : 1);
-  const int wpb = (int)std::max<size_t>(1, std::min<size_t>(8, (size_t)(96 * 1024) / per));
-  if (e == cudaSuccess) {
-    if (precision == SS3D_FP64)
-      e = func_smem(reinterpret_cast<const void*>(k_cond_krige<0>), cond_tri_bytes(cp->ndmax) + per * wpb);
-    else
-      e = func_smem(reinterpret_cast<const void*>(k_cond_krige<1>), cond_tri_bytes(cp->ndmax) + per * wpb);
+  // kriging kernel: rows in registers for ndmax <= 32 (compile-time classes
+  // of 8, 16, 24, 32), else the shared-memory warp Cholesky; CTAs of at most
+  // 8 warps, limited by the shared memory of one warp
+  const bool fp32 = precision == SS3D_FP32;
+  const int ndt = cp->ndmax <= 8 ? 8 : cp->ndmax <= 16 ? 16 : cp->ndmax <= 24 ? 24 : cp->ndmax <= 32 ? 32 : 0;
+  const void* kfn = nullptr;
+  size_t per = 0, kfix = 0;
+  switch (ndt * 2 + (fp32 ? 1 : 0)) {
+    case 16: kfn = (const void*)k_cond_krige_reg<0, 8>; per = KregLayout<0, 8>::BYTES; break;
+    case 17: kfn = (const void*)k_cond_krige_reg<1, 8>; per = KregLayout<1, 8>::BYTES; break;
+    case 32: kfn = (const void*)k_cond_krige_reg<0, 16>; per = KregLayout<0, 16>::BYTES; break;
+    case 33: kfn = (const void*)k_cond_krige_reg<1, 16>; per = KregLayout<1, 16>::BYTES; break;
+    case 48: kfn = (const void*)k_cond_krige_reg<0, 24>; per = KregLayout<0, 24>::BYTES; break;
+    case 49: kfn = (const void*)k_cond_krige_reg<1, 24>; per = KregLayout<1, 24>::BYTES; break;
+    case 64: kfn = (const void*)k_cond_krige_reg<0, 32>; per = KregLayout<0, 32>::BYTES; break;
+    case 65: kfn = (const void*)k_cond_krige_reg<1, 32>; per = KregLayout<1, 32>::BYTES; break;
+    default:
+      kfn = fp32 ? (const void*)k_cond_krige<1> : (const void*)k_cond_krige<0>;
+      per = cond_warp_bytes(cp->ndmax, fp32 ? 1 : 0);
+      kfix = cond_tri_bytes(cp->ndmax);
   }
+  const int wpb = (int)std::max<size_t>(1, std::min<size_t>(8, (size_t)(96 * 1024) / per));
+  if (e == cudaSuccess) e = func_smem(kfn, kfix + per * wpb);
+  KModel* dmdl = nullptr;   // the register kernels read the model from global memory
+  if (e == cudaSuccess) e = bufs.alloc(&dmdl, 1);
+  if (e == cudaSuccess) e = cudaMemcpyAsync(dmdl, &kmdl, sizeof kmdl, cudaMemcpyHostToDevice, stm);
   for (long long node0 = 0; node0 < M && e == cudaSuccess; node0 += chunk) {
     const int count = (int)std::min<long long>(chunk, M - node0);
-    k_cond_search<<<(count + 127) / 128, 128, 0, stm>>>(G, node0, count, ddx, ddy, ddz, dsbs, dsbi, dix, diy, diz,
-                                                       dnbr, dnnb);
+    const unsigned sblk = (unsigned)((count + 127) / 128);
+    if (cp->ndmax <= 8)
+      k_cond_search<8><<<sblk, 128, 0, stm>>>(G, node0, count, ddx, ddy, ddz, dsbs, dsbi, dix, diy, diz, dnbr, dnnb);
+    else if (cp->ndmax <= 16)
+      k_cond_search<16><<<sblk, 128, 0, stm>>>(G, node0, count, ddx, ddy, ddz, dsbs, dsbi, dix, diy, diz, dnbr, dnnb);
+    else if (cp->ndmax <= 24)
+      k_cond_search<24><<<sblk, 128, 0, stm>>>(G, node0, count, ddx, ddy, ddz, dsbs, dsbi, dix, diy, diz, dnbr, dnnb);
+    else if (cp->ndmax <= 32)
+      k_cond_search<32><<<sblk, 128, 0, stm>>>(G, node0, count, ddx, ddy, ddz, dsbs, dsbi, dix, diy, diz, dnbr, dnnb);
+    else if (cp->ndmax <= 64)
+      k_cond_search<64><<<sblk, 128, 0, stm>>>(G, node0, count, ddx, ddy, ddz, dsbs, dsbi, dix, diy, diz, dnbr, dnnb);
+    else
+      k_cond_search<100><<<sblk, 128, 0, stm>>>(G, node0, count, ddx, ddy, ddz, dsbs, dsbi, dix, diy, diz, dnbr,
+                                               dnnb);
     ++g_launch_count;
     e = cudaGetLastError();
     if (e != cudaSuccess) break;
     // one block per wpb nodes (short blocks): work of other streams, e.g. of a
     // serving loop's higher-priority requests, gets SMs as blocks finish
     const int nblk = (int)(((long long)count + wpb - 1) / wpb);
-    const size_t ksm = cond_tri_bytes(cp->ndmax) + per * wpb;
-    if (precision == SS3D_FP64)
-      k_cond_krige<0><<<nblk, 32 * wpb, ksm, stm>>>(G, kmdl, ctab, node0, count, dnbr, dnnb, dix, diy, diz, ddg,
-                                                    dsimd, dres, dcnt);
-    else
-      k_cond_krige<1><<<nblk, 32 * wpb, ksm, stm>>>(G, kmdl, ctab, node0, count, dnbr, dnnb, dix, diy, diz, ddg,
-                                                    dsimd, dres, dcnt);
+    const size_t ksm = kfix + per * wpb;
+    void* kargs_reg[] = {&G, &dmdl, &ctab, &node0, (void*)&count, &dnbr, &dnnb, &dix, &diy, &diz, &ddg, &dsimd,
+                         &dres, &dcnt};
+    void* kargs_old[] = {&G, &kmdl, &ctab, &node0, (void*)&count, &dnbr, &dnnb, &dix, &diy, &diz, &ddg, &dsimd,
+                         &dres, &dcnt};
+    void** kargs = ndt ? kargs_reg : kargs_old;
+    e = cudaLaunchKernel(kfn, dim3((unsigned)nblk), dim3(32 * wpb), kargs, ksm, stm);
     ++g_launch_count;
-    e = cudaGetLastError();
+    if (e == cudaSuccess) e = cudaGetLastError();
   }
   const long long tot = M * nreal;
   if (e == cudaSuccess && cp->itrans == 1) {

@@ -512,6 +512,86 @@ __global__ void k_spec_amp(Geo g, const double2* __restrict__ X, double* __restr
   }
 }
 
+// Last forward pass (z) of the spectrum with the amplitude step fused into its
+// stores (f90:1273-1292): S = X / N, amp = sqrt(max(Re S, 0)) in FP64 and its
+// FP32 copy, written straight from the registers of the transform instead of
+// storing X and reading it back; the padding columns get amplitude 0.  Per
+// block diagnostics (max |Im S|, max |Re S|, sums of the positive and negative
+// parts of S over the full spectrum, indices 0 < i < npx/2 counting for
+// themselves and their mirror) go to part[blockIdx.x] for k_reduce_spec.
+template <int LOGN>
+__global__ void __launch_bounds__(ColCfg<double, LOGN, 0>::NTH)
+    k_col_amp(AxisArgs a, Geo g, const double2* __restrict__ in, double* __restrict__ amp64, float* __restrict__ amp32,
+              Tw tw, SpecPartial* __restrict__ part) {
+  using C = double2;
+  using CF = ColCfg<double, LOGN, 0>;
+  constexpr int N = 1 << LOGN, TX = CF::TX, TPC = CF::TPC, NTH = CF::NTH;
+  constexpr int NR0 = N / Sched<LOGN>::radix(0);
+  extern __shared__ __align__(16) unsigned char smraw[];
+  C* s = reinterpret_cast<C*>(smraw);
+  C* stw = s + N * TX;
+  const int line0 = blockIdx.x * TX;
+  const int t = threadIdx.x % TX;
+  const int line = line0 + t;
+  const bool inside = line < a.lines;
+  const int i = inside ? line % g.HP : 0;
+  const bool valid = inside && i < g.H;
+  const C* src = in + (valid ? line : 0);
+  const int S = (int)a.S;
+  const double rn = (double)g.npx * (double)g.npy * (double)g.npz;
+  const double wgt = (i == 0 || 2 * i == g.npx) ? 1.0 : 2.0;
+  double mi = 0.0, mr = 0.0, sp = 0.0, sn = 0.0;
+  for (int q = threadIdx.x; q < N; q += NTH) stw[q] = tw.d[N - 1 + q];
+  __syncthreads();
+  fft_tile<LOGN, TX, TPC, -1>(
+      s, stw, [&](int jb, int r) { return src[(jb + r * NR0) * S]; },
+      [&](int pos, C v) {
+        if (valid) {
+          const double re = v.x / rn, im = v.y / rn;
+          mi = fmax(mi, fabs(im));
+          mr = fmax(mr, fabs(re));
+          double am = 0.0;
+          if (re < 0.0) {
+            sn += wgt * re;
+          } else {
+            sp += wgt * re;
+            am = sqrt(re);
+          }
+          amp64[(long long)pos * S + line] = am;
+          amp32[(long long)pos * S + line] = (float)am;
+        } else if (inside) {
+          amp64[(long long)pos * S + line] = 0.0;
+          amp32[(long long)pos * S + line] = 0.0f;
+        }
+      });
+  __shared__ double red[4][NTH / 32];
+#pragma unroll
+  for (int off = 16; off > 0; off >>= 1) {
+    mi = fmax(mi, __shfl_down_sync(0xffffffffu, mi, off));
+    mr = fmax(mr, __shfl_down_sync(0xffffffffu, mr, off));
+    sp += __shfl_down_sync(0xffffffffu, sp, off);
+    sn += __shfl_down_sync(0xffffffffu, sn, off);
+  }
+  if ((threadIdx.x & 31) == 0) {
+    const int w = threadIdx.x >> 5;
+    red[0][w] = mi;
+    red[1][w] = mr;
+    red[2][w] = sp;
+    red[3][w] = sn;
+  }
+  __syncthreads();
+  if (threadIdx.x == 0) {
+    SpecPartial p{0, 0, 0, 0};
+    for (int w = 0; w < NTH / 32; ++w) {
+      p.maximag = fmax(p.maximag, red[0][w]);
+      p.maxreal = fmax(p.maxreal, red[1][w]);
+      p.spos += red[2][w];
+      p.sneg += red[3][w];
+    }
+    part[blockIdx.x] = p;
+  }
+}
+
 // Sum of the per-block partials in a fixed order, independent of scheduling:
 // one block of RS_NT threads; thread t combines partials t, t + RS_NT, ... in
 // index order, then each warp folds its lanes by halving distances, and warp 0
@@ -821,6 +901,37 @@ static cudaError_t run_rows_c2r(const Geo& g, const cpx_t<R>* in, long long rstr
 }
 
 template <int L>
+static cudaError_t run_col_amp(const AxisArgs& a, const Geo& g, const double2* in, double* amp64, float* amp32, Tw tw,
+                               SpecPartial* part, int npart_max, int* nb, cudaStream_t st) {
+  if constexpr (L == 0) {
+    return cudaErrorInvalidValue;
+  } else {
+    using CF = ColCfg<double, L, 0>;
+    const size_t smem = (size_t)(CF::N * CF::TX + CF::N) * sizeof(double2);
+    cudaError_t e = set_smem(k_col_amp<L>, smem);
+    if (e != cudaSuccess) return e;
+    const int blocks = (a.lines + CF::TX - 1) / CF::TX;
+    if (blocks > npart_max) return cudaErrorInvalidValue;
+    *nb = blocks;
+    k_col_amp<L><<<blocks, CF::NTH, smem, st>>>(a, g, in, amp64, amp32, tw, part);
+    ++g_launch_count;
+    return cudaGetLastError();
+  }
+}
+
+// partial-sum entries the spectrum build needs for grid g (one per block of
+// the amplitude step), plus one for the result
+int spectrum_parts(const Geo& g) {
+  if (g.npz > 1) {
+    const int L = ilog2(g.npz);
+    const int tx = std::min(64, std::max(2, 4096 >> L));   // ColCfg<double, L, 0>::TX
+    const long long lines = (long long)g.npy * g.HP;
+    return (int)std::max<long long>(148 * 8, (lines + tx - 1) / tx) + 1;
+  }
+  return 148 * 8 + 1;
+}
+
+template <int L>
 static cudaError_t run_spec_rows(const Model& m, const double d[3], const Geo& g, double2* out, Tw tw,
                                  cudaStream_t st) {
   constexpr int TX = RowTX<double, L>::TX;
@@ -881,26 +992,26 @@ cudaError_t launch_spectrum(const Model& m, const double d[3], const Geo& g, dou
     SS3D_LOGN_SWITCH(L, MAX_LOGN_D, e = (run_axis_c2c<double, L, -1>(a, g, work, work, tw, st)));
     if (e != cudaSuccess) return e;
   }
+  int nb = 0;
   if (g.npz > 1) {
+    // z pass with the amplitude step in its stores
     AxisArgs a{};
     a.S = (long long)g.npy * g.HP;
     a.nout = g.npz;
     a.lines = g.npy * g.HP;
     a.ngroups = 1;
-    a.gstride = 0;
-    a.rstride = 0;
-    a.nreal = 1;
     a.axis = 2;
     int L = ilog2(g.npz);
     e = cudaErrorInvalidValue;
-    SS3D_LOGN_SWITCH(L, MAX_LOGN_D, e = (run_axis_c2c<double, L, -1>(a, g, work, work, tw, st)));
+    SS3D_LOGN_SWITCH(L, MAX_LOGN_D, e = (run_col_amp<L>(a, g, work, amp64, amp32, tw, part, npart_max, &nb, st)));
     if (e != cudaSuccess) return e;
+  } else {
+    long long tot = (long long)g.npz * g.npy * g.HP;
+    nb = (int)std::min<long long>(npart_max, (tot + NT - 1) / NT);
+    k_spec_amp<<<nb, NT, 0, st>>>(g, work, amp64, amp32, part);
+    ++g_launch_count;
+    if ((e = cudaGetLastError()) != cudaSuccess) return e;
   }
-  long long tot = (long long)g.npz * g.npy * g.HP;
-  int nb = (int)std::min<long long>(npart_max, (tot + NT - 1) / NT);
-  k_spec_amp<<<nb, NT, 0, st>>>(g, work, amp64, amp32, part);
-  ++g_launch_count;
-  if ((e = cudaGetLastError()) != cudaSuccess) return e;
   k_reduce_spec<<<1, RS_NT, 0, st>>>(part, nb, result);
   ++g_launch_count;
   return cudaGetLastError();

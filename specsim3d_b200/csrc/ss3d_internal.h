@@ -84,6 +84,7 @@ bool pipe_error_take(cudaStream_t st);
 cudaError_t launch_spectrum(const Model& m, const double d[3], const Geo& g, double2* work, double* amp64,
                             float* amp32, SpecPartial* part, int npart_max, SpecPartial* result, Tw tw,
                             cudaStream_t st);
+int spectrum_parts(const Geo& g);   // partial-sum entries of a spectrum build (npart_max + 1)
 cudaError_t launch_rowstates(const Geo& g, uint32_t s0, long long r_first, int nreal, const uint32_t* ptab,
                              uint32_t* rowstates, uint32_t* apow, cudaStream_t st);
 // out_kind: 0 float output, 1 double output; first_done (may be NULL) is
