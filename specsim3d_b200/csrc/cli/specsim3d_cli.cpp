@@ -23,6 +23,7 @@
 #include <fstream>
 #include <sstream>
 #include <string>
+#include <thread>
 #include <vector>
 
 #include "../../../include/specsim3d_gpu.h"
@@ -271,13 +272,15 @@ void write_vtk_bin(const std::string& fname, const float* a, const int n[3], con
   fclose(fp);
 }
 
-// VTK XML ImageData, raw appended little-endian float32, UInt64 headers (f90:307-359)
-void write_vti(const std::string& fname, const double* res, const int n[3], int nreal, const double x0[3],
-               const double d[3]) {
+// VTK XML ImageData, raw appended little-endian float32, UInt64 headers
+// (f90:307-359), written in three parts so that realizations can be appended
+// as they arrive: the header (it depends on the sizes only), one block per
+// realization, the footer
+FILE* vti_open(const std::string& fname, const int n[3], int nreal, const double x0[3], const double d[3]) {
   const uint16_t probe = 1;
   if (*(const unsigned char*)&probe != 1) stop_text("write_vti: big-endian machines are not supported");
   FILE* fp = fopen(fname.c_str(), "wb");
-  if (!fp) return;
+  if (!fp) return nullptr;
   const long long nbytes = 4LL * n[0] * n[1] * n[2];
   char ext[128];
   snprintf(ext, sizeof ext, "0 %d 0 %d 0 %d", n[0] - 1, n[1] - 1, n[2] - 1);
@@ -292,16 +295,29 @@ void write_vti(const std::string& fname, const double* res, const int n[3], int 
             (nbytes + 8) * (long long)(r - 1));
   fprintf(fp, "      </PointData>\n      <CellData/>\n    </Piece>\n  </ImageData>\n");
   fprintf(fp, "  <AppendedData encoding=\"raw\">\n   _");
+  return fp;
+}
+void vti_block(FILE* fp, const float* a, size_t m) {
+  const uint64_t nb = 4ull * m;
+  fwrite(&nb, 8, 1, fp);
+  fwrite(a, sizeof(float), m, fp);
+}
+void vti_close(FILE* fp) {
+  fprintf(fp, "\n  </AppendedData>\n</VTKFile>\n");
+  fclose(fp);
+}
+
+void write_vti(const std::string& fname, const double* res, const int n[3], int nreal, const double x0[3],
+               const double d[3]) {
+  FILE* fp = vti_open(fname, n, nreal, x0, d);
+  if (!fp) return;
   const size_t m = (size_t)n[0] * n[1] * n[2];
   std::vector<float> sp(m);
   for (int r = 0; r < nreal; r++) {
     for (size_t q = 0; q < m; q++) sp[q] = (float)res[q + m * r];
-    const uint64_t nb = (uint64_t)nbytes;
-    fwrite(&nb, 8, 1, fp);
-    fwrite(sp.data(), sizeof(float), m, fp);
+    vti_block(fp, sp.data(), m);
   }
-  fprintf(fp, "\n  </AppendedData>\n</VTKFile>\n");
-  fclose(fp);
+  vti_close(fp);
 }
 
 // ---------------------------------------------------------------- variogram report (f90:434-529)
@@ -633,13 +649,52 @@ int main(int argc, char** argv) {
   const double tsp = now();
   printf(" time covariance+spectrum: %s s\n", F(tsp - t0, 8, 2).c_str());
   const size_t m = (size_t)n[0] * n[1] * n[2];
+  auto stats_line = [&](int r, const double* z) {
+    printf(" realization%s  mean=%s  variance=%s  max|Im|=%s\n", I(r + 1, 3).c_str(), F(z[0], 9, 4).c_str(),
+           F(z[1], 9, 4).c_str(), ES(z[2], 9, 2).c_str());
+  };
+  if (!docond && !dovario && !outgs && !outvtk1a) {
+    // Streaming: only float32 files are written (.bin, .vti, binary VTK), and
+    // none needs all realizations at once.  Chunks of about 64 MB are
+    // realized straight to float32 (the same rounding as the conversion of
+    // the FP64 values below) and written by a second thread while the next
+    // chunk is computed, instead of holding every realization in memory.
+    const int chunk = (int)std::max<size_t>(1, std::min<size_t>((size_t)std::max(nreal, 1), ((size_t)64 << 20) / (4 * m)));
+    std::vector<float> buf[2] = {std::vector<float>(m * chunk), std::vector<float>(m * chunk)};
+    std::vector<double> zs(3 * (size_t)chunk);
+    FILE* fb = binout ? fopen((outbase + ".bin").c_str(), "wb") : nullptr;
+    FILE* fv = outvti ? vti_open(outbase + ".vti", n, nreal, xmin, d) : nullptr;
+    std::thread writer;
+    for (int r0 = 0, c = 0; r0 < nreal; r0 += chunk, ++c) {
+      const int nb = std::min(chunk, nreal - r0);
+      std::vector<float>& out = buf[c & 1];
+      check(ss3d_realize(sp, iseed, r0, nb, igauss, precision, out.data(), SS3D_OUT_F32, zs.data()), "ss3d_realize");
+      for (int r = 0; r < nb; r++) stats_line(r0 + r, &zs[3 * (size_t)r]);
+      if (writer.joinable()) writer.join();
+      writer = std::thread([&, r0, nb, c] {
+        const float* a = buf[c & 1].data();
+        if (fb) fwrite(a, sizeof(float), m * nb, fb);
+        for (int r = 0; r < nb; r++) {
+          if (fv) vti_block(fv, a + m * r, m);
+          if (vtkall || (outvtk1b && r0 + r == 0))
+            write_vtk_bin(outbase + "_" + std::to_string(r0 + r + 1) + ".vtk", a + m * r, n, xmin, d,
+                          "SPECSIM3D realization");
+        }
+      });
+    }
+    if (writer.joinable()) writer.join();
+    if (fb) fclose(fb);
+    if (fv) vti_close(fv);
+    ss3d_spectrum_free(sp);
+    printf(" time realizations         : %s s\n", F(now() - tsp, 8, 2).c_str());
+    printf(" elapsed time: %s s\n", F(now() - t0, 8, 2).c_str());
+    return 0;
+  }
   std::vector<double> res(m * std::max(nreal, 1));
   std::vector<double> zs(3 * (size_t)std::max(nreal, 1));
   check(ss3d_realize(sp, iseed, 0, nreal, igauss, precision, res.data(), SS3D_OUT_F64, zs.data()), "ss3d_realize");
   ss3d_spectrum_free(sp);
-  for (int r = 0; r < nreal; r++)
-    printf(" realization%s  mean=%s  variance=%s  max|Im|=%s\n", I(r + 1, 3).c_str(), F(zs[3 * r], 9, 4).c_str(),
-           F(zs[3 * r + 1], 9, 4).c_str(), ES(zs[3 * r + 2], 9, 2).c_str());
+  for (int r = 0; r < nreal; r++) stats_line(r, &zs[3 * (size_t)r]);
   if (docond) condition(res.data(), n, nreal, xmin, d, st, nugget, condfile, outbase, legacy ? nullptr : &pf, precision);
   const double tsm = now();
   printf(" time realizations         : %s s\n", F(tsm - tsp, 8, 2).c_str());
