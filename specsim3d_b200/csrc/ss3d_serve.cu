@@ -184,15 +184,19 @@ Req* admit_locked(ss3d_server* s, int w, std::vector<ss3d_spectrum*>& freed, boo
     }
     // conditional requests fill the GPU with their search and kriging
     // kernels: at most max_cond of them run at once, the other slots keep
-    // serving unconditional requests beside them
-    if (r->cond && s->cond_running >= s->cfg.max_cond) {
-      if (i == 0 && r->bypassed >= s->cfg.max_bypass) return nullptr;
-      continue;
-    }
+    // serving unconditional requests beside them.  A head that waits only for
+    // a conditional slot is not passed in the sense of max_bypass: requests
+    // that take no such slot cannot delay it, so they are admitted past it
+    // without limit (counting them stopped all admission, for as long as a
+    // kriging call of the largest grids runs, once max_bypass was reached)
+    if (r->cond && s->cond_running >= s->cfg.max_cond) continue;
     evict_locked(s, r->key, freed, [&] { return s->charged + s->cache_bytes + need <= s->budget(); });
     if (s->charged + s->cache_bytes + need <= s->budget()) {
       s->queue.erase(s->queue.begin() + (long)i);
-      if (i > 0) s->queue.front()->bypassed++;
+      if (i > 0) {
+        Req* h = s->queue.front();
+        if (!(h->cond && s->cond_running >= s->cfg.max_cond)) h->bypassed++;
+      }
       s->retained[w] += grow;
       r->held = r->tmp_bytes + (have ? 0 : r->build_bytes);
       s->charged += grow + r->held;

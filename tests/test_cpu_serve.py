@@ -5,7 +5,9 @@ the memory accounting are the production code paths).
 Checks: the device bytes charged never exceed the budget; slots run requests
 at the same time; repeated models hit the cache; a request that can never fit
 fails with SS3D_ENOMEM instead of blocking the queue; a large request waiting
-at the head is passed at most max_bypass times.
+at the head is passed at most max_bypass times; a conditional request that
+waits at the head only for a conditional slot does not hold back the
+unconditional requests behind it.
 """
 import numpy as np
 import pytest
@@ -110,3 +112,26 @@ def test_idle_slots_give_back_work_space():
     srv.close()
     assert all(r["status"] == 0 for r in res), [r["message"] for r in res if r["status"]]
     assert st["peak_bytes"] <= st["budget_bytes"]
+
+
+def test_head_waiting_for_a_conditional_slot_does_not_block():
+    """max_cond 1: while one long conditional request runs, a second one waits
+    at the head of the queue for the conditional slot.  The unconditional
+    requests behind it take no such slot and must all be admitted while the
+    first one runs, not only max_bypass of them."""
+    big = dict(structs=[(2, 1.0, 30.0, 30.0, 30.0, 0.0, 0.0, 0.0)], nugget=0.0, d=(1, 1, 1), n=(128, 128, 64), ipad=1)
+    small = dict(structs=[(1, 1.0, 5.0, 5.0, 5.0, 0.0, 0.0, 0.0)], nugget=0.0, d=(1, 1, 1), n=(16, 16, 16), ipad=1)
+    params = dict(ixc=1, iyc=2, izc=3, ivc=4, iwc=0, tmin=-1e21, tmax=1e21, itrans=0, skmean=0.0, zmin=0.0, zmax=1.0,
+                  ltail=1, ltpar=0.0, utail=1, utpar=0.0, radius=(10.0, 10.0, 10.0), angles=(0.0, 0.0, 0.0), ndmax=8)
+    cond = dict(params=params, rows=np.array([[1.0, 2.0, 3.0, 0.5], [5.0, 6.0, 7.0, -0.5]]), xmin=(0.0, 0.0, 0.0))
+    srv = _server(slots=4, hbm_budget=4 * GB, max_bypass=2, max_cond=1, dry_run_ns_per_cell=2.0)
+    t_a = srv.submit(big, 1, 16, cond=cond)
+    t_b = srv.submit(big, 2, 16, cond=cond)
+    ts = [srv.submit(small, 10 + k, 1) for k in range(12)]
+    rs = [srv.wait(t) for t in ts]
+    r_a = srv.wait(t_a)
+    r_b = srv.wait(t_b)
+    srv.close()
+    assert r_a["status"] == 0 and r_b["status"] == 0 and all(r["status"] == 0 for r in rs)
+    assert r_b["t_admit"] >= r_a["t_done"]                       # one conditional slot
+    assert all(r["t_done"] <= r_a["t_done"] for r in rs), [round(r["t_admit"] - r_a["t_admit"], 4) for r in rs]
