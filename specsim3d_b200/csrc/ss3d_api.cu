@@ -974,13 +974,16 @@ extern "C" int ss3d_autotune(const ss3d_spectrum* sp, int igauss, int precision,
   CK(cudaMalloc(&out, sizeof(float) * M * nreal));
   const bool prof_was = g_prof;
   double best[3] = {1e30, 1e30, 1e30};
+  double fused_ms = 1e30;   // row variant 5: middle and row passes in one kernel
   int bestv[3] = {0, 0, 0};
   int rc = SS3D_OK;
   // variants per kind: 0-3 everywhere, FP32 column passes also 4-7 (two
   // lines per thread), the FP32 middle pass also 8-9 (tiles staged by bulk
-  // tensor copies), the row pass also 4 (rows held in warps); a kind with
-  // fewer variants runs its variant v mod 4 meanwhile
-  const int nvk[3] = {precision == SS3D_FP32 ? 10 : 4, precision == SS3D_FP32 ? 8 : 4, 5};
+  // tensor copies), the row pass also 4 (rows held in warps) and, in FP32, 5
+  // (middle and row passes fused over a cluster) and 6 (two rows per lane on
+  // packed FP32); a kind with fewer variants runs its variant v mod 4 meanwhile
+  const int nvk[3] = {precision == SS3D_FP32 ? 10 : 4, precision == SS3D_FP32 ? 8 : 4,
+                      precision == SS3D_FP32 ? 7 : 5};
   const int nv = std::max(nvk[0], nvk[2]);
   auto vk = [&](int k, int v) { return v < nvk[k] ? v : v % 4; };
   for (int v = 0; v < nv && rc == SS3D_OK; v++) {
@@ -995,12 +998,24 @@ extern "C" int ss3d_autotune(const ss3d_spectrum* sp, int igauss, int precision,
     g_prof = prof_was;
     if (rc) break;
     const double ms[3] = {g_prof_ms[2], g_prof_ms[1], g_prof_ms[3]};   // stage 2 middle, 1 synthesis, 3 rows
+    // row variant 5 runs the middle pass inside the row stage: it competes
+    // with the best middle + row pair below, not with either pass alone
+    const bool joint = L[2] >= 0 && vk(2, v) == 5;
+    if (joint && L[0] >= 0 && g_prof_ms[2] == 0.0) {
+      fused_ms = std::min(fused_ms, ms[2]);
+      if (L[1] >= 0 && ms[1] < best[1]) {
+        best[1] = ms[1];
+        bestv[1] = vk(1, v);
+      }
+      continue;
+    }
     for (int k = 0; k < 3; k++)
-      if (L[k] >= 0 && ms[k] < best[k]) {
+      if (L[k] >= 0 && ms[k] < best[k] && !(k == 2 && vk(2, v) == 5)) {
         best[k] = ms[k];
         bestv[k] = vk(k, v);
       }
   }
+  if (fused_ms < best[0] + best[2]) bestv[2] = 5;
   for (int k = 0; k < 3; k++)
     if (L[k] >= 0) g_variant[k][p][L[k]] = bestv[k];
   for (int q = 0; q < SS3D_NSTAGE; q++) g_prof_ms[q] = 0;
@@ -1012,8 +1027,10 @@ extern "C" int ss3d_autotune(const ss3d_spectrum* sp, int igauss, int precision,
 
 extern "C" int ss3d_set_variant(int kind, int precision, int logn, int variant) {
   // 4-7: FP32 two-line column tiles; 8, 9: FP32 middle pass staged by bulk
-  // tensor copies (one and two lines per thread); 4 of the row pass: rows held in warps
-  const int vmax = kind == 2 ? 4 : (precision == SS3D_FP32 ? (kind == 0 ? 9 : 7) : 3);
+  // tensor copies (one and two lines per thread); 4 of the row pass: rows held
+  // in warps; 5 of the FP32 row pass: middle and row passes fused over a
+  // cluster; 6 of the FP32 row pass: two rows per lane on packed FP32
+  const int vmax = kind == 2 ? (precision == SS3D_FP32 ? 6 : 4) : (precision == SS3D_FP32 ? (kind == 0 ? 9 : 7) : 3);
   if (kind < 0 || kind > 2 || (precision != SS3D_FP64 && precision != SS3D_FP32) || logn < 0 || logn > 15 ||
       variant < 0 || variant > vmax)
     return fail(SS3D_EINVAL, "invalid variant selection");

@@ -667,8 +667,9 @@ extern "C" int ss3d_batch_autotune(ss3d_batch* b) {
     int bestv = 0;
     float bestk = 1e30f;
     // column passes 4-7: two-line tiles; middle pass 8-9: tiles staged by
-    // bulk tensor copies; row pass 4: rows held in warps
-    for (int v = 0; v < (k == 2 ? 5 : (k == 0 ? 10 : 8)) && e == cudaSuccess; v++) {
+    // bulk tensor copies; row pass 4: rows held in warps, 5: middle and row
+    // passes fused over a cluster, 6: two rows per lane on packed FP32
+    for (int v = 0; v < (k == 2 ? 7 : (k == 0 ? 10 : 8)) && e == cudaSuccess; v++) {
       for (int L = 0; L < 16; L++)
         if (used[k][L]) b->var[k][L] = v;
       e = time_run(b, st, ms, true);

@@ -678,4 +678,136 @@ __device__ __forceinline__ void rows_warp_body(const Geo& g, const cpx_t<R>* __r
   }
 }
 
+// ---------------------------------------------------------------- x pass, two rows per lane on packed FP32
+// Row variant 6 (FP32, lengths 8..256): rows_warp_body with the rows taken in
+// pairs (A = 2 p, B = 2 p + 1), each lane holding one cpair per position (the
+// real parts of A and B in one register pair, the imaginary parts in the
+// other).  The packing and every butterfly and twiddle product is then one
+// packed FP32 instruction for both rows, and the shuffles' lane arithmetic,
+// the exchange addresses and the crop tests are shared by the two.  Lane by
+// lane the operations are those of rows_warp_body (ksub on pairs is
+// fma(b, -1, a), the exact IEEE difference), so the values are the same bits.
+// The exchange layout of the row-warp tiles keeps its minimum number of
+// shared-memory wavefronts with 16-byte elements.
+template <int LOGN> struct RowPairCfg {
+  static constexpr int N = 1 << LOGN;
+  static constexpr int ET = 8;                  // pairs of elements per lane
+  static constexpr int TPC = N / ET;            // lanes per row pair
+  static constexpr int RPW = TPC >= 32 ? 1 : 32 / TPC;
+  static constexpr int NW = 8;                  // warps per block
+  static constexpr int NTH = 32 * NW;
+  static constexpr int ROWS = 2 * NW * RPW;     // rows per block
+  static constexpr int SLICE = N * RPW;         // exchange elements per warp
+  static constexpr bool ok = LOGN >= 3 && LOGN <= 8;
+  static constexpr size_t smem = (size_t)(2 * N + NW * SLICE) * sizeof(cpair);
+};
+
+__device__ __forceinline__ cpair pair_rows(float2 a, float2 b) {
+  return cpair{make_float2(a.x, b.x), make_float2(a.y, b.y)};
+}
+
+template <typename O, int LOGN>
+__device__ __forceinline__ void rows_pair_body(const Geo& g, const float2* __restrict__ in, long long rstride,
+                                               O* __restrict__ out, long long ostride, int nreal, int nblk_per_r,
+                                               double* __restrict__ part, const Tw& tw, int item,
+                                               unsigned char* smraw) {
+  using C = cpair;
+  using W = RowPairCfg<LOGN>;
+  constexpr int N = W::N, ET = W::ET, TPC = W::TPC, RPW = W::RPW;
+  static_assert(W::ok && TPC * RPW == 32, "row pairs of whole warps");
+  C* stw = reinterpret_cast<C*>(smraw);   // N entries e^{-2 pi i m/(2N)}, broadcast to both rows
+  C* stwN = stw + N;                      // N entries e^{-2 pi i m/N}
+  const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
+  C* sx = stwN + N + warp * W::SLICE;
+  const int r = item % nreal;
+  const int blk = item / nreal;
+  for (int q = threadIdx.x; q < N; q += W::NTH) {
+    const float2 a = tw.f[2 * N - 1 + q], b = tw.f[N - 1 + q];
+    stw[q] = cpair{make_float2(a.x, a.x), make_float2(a.y, a.y)};
+    stwN[q] = cpair{make_float2(b.x, b.x), make_float2(b.y, b.y)};
+  }
+  const int t = lane % RPW, c = lane / RPW;
+  const int nrows = g.ny * g.nz;
+  const int rowA = ((blk * W::NW + warp) * RPW + t) * 2, rowB = rowA + 1;
+  const bool okA = rowA < nrows, okB = rowB < nrows;
+  const int jA = okA ? rowA % g.ny : 0, kA = okA ? rowA / g.ny : 0;
+  const int jB = okB ? rowB % g.ny : 0, kB = okB ? rowB / g.ny : 0;
+  const float2* src = in + (long long)r * rstride;
+  const float2* rpA = src + ((long long)kA * g.npy + jA) * g.HP;
+  const float2* rpB = src + ((long long)kB * g.npy + jB) * g.HP;
+  C x[ET];
+#pragma unroll
+  for (int i = 0; i < ET; ++i) x[i] = pair_rows(rpA[c + TPC * i], rpB[c + TPC * i]);
+  const C xN = pair_rows(rpA[N], rpB[N]);
+  __syncthreads();
+  // the packing of rows_warp_body on both rows at once
+  const int mirror = ((TPC - c) % TPC) * RPW + t;
+  C z[ET];
+#pragma unroll
+  for (int i = 0; i < ET; ++i) {
+    C b;
+    b.x.x = __shfl_sync(0xffffffffu, x[ET - 1 - i].x.x, mirror);
+    b.x.y = __shfl_sync(0xffffffffu, x[ET - 1 - i].x.y, mirror);
+    b.y.x = __shfl_sync(0xffffffffu, x[ET - 1 - i].y.x, mirror);
+    b.y.y = __shfl_sync(0xffffffffu, x[ET - 1 - i].y.y, mirror);
+    if (c == 0) b = i == 0 ? xN : x[(ET - i) % ET];
+    C a = x[i];
+    const int q = c + TPC * i;
+    if (q == 0) {
+      a.y = make_float2(0.f, 0.f);
+      b.y = make_float2(0.f, 0.f);
+    }
+    C w = stw[q];
+    w.y = kneg(w.y);
+    const C bc = cmk<C>(b.x, kneg(b.y));
+    z[i] = cadd(cadd(a, bc), cmul_si<+1>(cmul(w, csub(a, bc))));
+  }
+  constexpr int R0 = Sched<LOGN>::radix(0), NBT = ET / R0;
+  C v[ET];
+#pragma unroll
+  for (int m = 0; m < NBT; ++m)
+#pragma unroll
+    for (int rr = 0; rr < R0; ++rr) v[m * R0 + rr] = z[m + rr * NBT];
+  double s1 = 0.0, s2 = 0.0;
+  const bool stats = part != nullptr;
+  O* orA = out + (long long)r * ostride + (long long)(okA ? rowA : 0) * g.nx;
+  O* orB = out + (long long)r * ostride + (long long)(okB ? rowB : 0) * g.nx;
+  const int nxh = (g.nx + 1) / 2;
+  const bool even = (g.nx & 1) == 0;
+  auto put = [&](O* orow, float re, float im, int pos) {
+    const bool second = even || 2 * pos + 1 < g.nx;
+    if (even) {
+      if constexpr (sizeof(O) == 4) {
+        reinterpret_cast<float2*>(orow)[pos] = make_float2(re, im);
+      } else {
+        reinterpret_cast<double2*>(orow)[pos] = make_double2((double)re, (double)im);
+      }
+    } else {
+      orow[2 * pos] = (O)re;
+      if (second) orow[2 * pos + 1] = (O)im;
+    }
+    if (stats) {
+      s1 += (double)re;
+      s2 += (double)re * (double)re;
+      if (second) {
+        s1 += (double)im;
+        s2 += (double)im * (double)im;
+      }
+    }
+  };
+  fft_tile_regs<LOGN, RPW, TPC, +1, RPW, false, false, -1>(sx, stwN, v, t, c, [&](int pos, C zz) {
+    if (pos < nxh) {
+      if (okA) put(orA, zz.x.x, zz.y.x, pos);
+      if (okB) put(orB, zz.x.y, zz.y.y, pos);
+    }
+  });
+  if (part) {
+    block_sum2<W::NTH>(s1, s2);
+    if (threadIdx.x == 0) {
+      part[2 * ((long long)r * nblk_per_r + blk)] = s1;
+      part[2 * ((long long)r * nblk_per_r + blk) + 1] = s2;
+    }
+  }
+}
+
 }  // namespace ss3d

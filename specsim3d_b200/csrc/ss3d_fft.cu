@@ -18,6 +18,7 @@
 // warp covers whole 32-byte sectors) and runs the radix-8/4/2 Stockham engine
 // of ss3d_device.cuh on it.  Only the positions that survive the final crop are
 // written back (z pass: k < nz; y pass: j < ny; x pass: i < nx).
+#include <cooperative_groups.h>
 #include <cuda_runtime.h>
 
 #include <algorithm>
@@ -215,6 +216,135 @@ __global__ void __launch_bounds__(TmaCfg<LOGN, P>::NTH, 1)
   }
 }
 
+// ---------------------------------------------------------------- middle and row passes fused over a cluster
+// Row pass variant 5 (FP32, float output, no statistics): the middle (y)
+// inverse pass and the C2R row (x) pass of one plane k of one realization in
+// one thread-block cluster of CL CTAs, so that the y pass output never goes
+// to HBM.  Phase 1: CTA c of the cluster transforms the column tiles
+// c, c + CL, ... of the plane along y (TXY columns x NY positions, the tile
+// staged from HBM through registers as col_body does) and stores each output
+// row j < ny straight into the shared-memory row tile of the CTA that owns
+// row j (rows c' TXR .. c' TXR + TXR - 1 belong to CTA c'), through
+// distributed shared memory.  A cluster barrier.  Phase 2: each CTA packs,
+// transforms and crops its TXR rows exactly as rows_body does after its
+// staging, and stores them.  Every column and row sees the butterflies of
+// col_body and rows_body, so the results are the same bits.
+template <int LY, int LX> struct YXCfg {
+  static constexpr int NY = 1 << LY, NX = 1 << LX;
+  static constexpr int NTH = 512;
+  static constexpr int ETY = 8;                       // phase 1: elements per thread
+  static constexpr int TPCY = NY / ETY;
+  static constexpr int TXY = NTH / TPCY;              // columns per y tile
+  using RC = RowCfg<float, LX, 0>;                    // phase 2: the row tile of rows_body
+  static constexpr int TXR = RC::TX, TPCR = RC::TPC, PR = TXR + 1;
+  static constexpr bool ok = LY >= 6 && LY <= 9 && LX >= 7 && LX <= 9 && RC::NTH0 == NTH && TXY >= 1 &&
+                             TXY <= 64 && TXY * TPCY == NTH;
+  static constexpr int ROWBUF = (NX + 1) * PR;        // float2: this CTA's rows, [position][row]
+  static constexpr int YP = NY + 4;                   // column pitch of a finished y tile
+  static constexpr int YTILE = TXY * YP;              // float2: exchange buffer, then the finished tile
+  static constexpr size_t SMEM = (size_t)(ROWBUF + YTILE + NY + 3 * NX) * sizeof(float2);
+};
+
+template <int LY, int LX, int CL>
+__global__ void __cluster_dims__(CL, 1, 1) __launch_bounds__(512, 2)
+    k_yx_fused(Geo g, const float2* __restrict__ work, long long wstride, float* __restrict__ out, Tw tw) {
+  namespace cg = cooperative_groups;
+  using Y = YXCfg<LY, LX>;
+  using C = float2;
+  constexpr int NY = Y::NY, NX = Y::NX, TXY = Y::TXY, TPCY = Y::TPCY, TXR = Y::TXR, TPCR = Y::TPCR, PR = Y::PR;
+  constexpr int NTH = Y::NTH;
+  constexpr int NR0 = NY / Sched<LY>::radix(0);
+  extern __shared__ __align__(16) unsigned char smraw[];
+  C* rowbuf = reinterpret_cast<C*>(smraw);
+  C* ytile = rowbuf + Y::ROWBUF;
+  C* stwy = ytile + Y::YTILE;   // NY entries e^{-2 pi i m/NY}
+  C* stw = stwy + NY;           // 2 NX entries e^{-2 pi i m/(2 NX)}
+  C* stwN = stw + 2 * NX;       // NX entries e^{-2 pi i m/NX}
+  cg::cluster_group cl = cg::this_cluster();
+  const int rank = (int)cl.block_rank();
+  const int plane = blockIdx.x / CL;   // r nz + k
+  const int r = plane / g.nz, k = plane - (plane / g.nz) * g.nz;
+  const int tid = threadIdx.x;
+  for (int q = tid; q < NY; q += NTH) stwy[q] = tw.f[NY - 1 + q];
+  for (int q = tid; q < 2 * NX; q += NTH) stw[q] = tw.f[2 * NX - 1 + q];
+  for (int q = tid; q < NX; q += NTH) stwN[q] = tw.f[NX - 1 + q];
+  // every CTA of the cluster has started (its shared memory exists) before any
+  // CTA writes into it
+  cl.sync();
+  // ---- phase 1: y transforms of this CTA's column tiles, rows j < ny to their owners
+  const C* pin = work + (long long)r * wstride + (long long)k * g.npy * g.HP;
+  const int H = g.H;
+  const int ntiles = (H + TXY - 1) / TXY;
+  const int t = tid % TXY;
+  const int S = g.HP;
+  const int ny = g.ny;
+  constexpr int YP = Y::YP;
+  for (int u = rank; u < ntiles; u += CL) {
+    const int i = u * TXY + t;
+    const bool valid = i < H;
+    const C* src = pin + (valid ? i : 0);
+    // the finished tile goes to shared memory column by column (pitch NY + 4:
+    // the 8 columns x 4 consecutive positions of a warp's store hit every bank
+    // pair twice) ...
+    fft_tile<LY, TXY, TPCY, +1, TXY, false, true>(
+        ytile, stwy, [&](int jb, int rr) { return src[(jb + rr * NR0) * S]; },
+        [&](int pos, C v) { ytile[t * YP + pos] = v; });
+    __syncthreads();
+    // ... and from there to the owners of its rows, a warp storing consecutive
+    // positions of one column (contiguous in the owner's row tile)
+    const int ncol = min(TXY, H - u * TXY);
+    for (int q = tid; q < ncol * ny; q += NTH) {
+      const int cc = q / ny, pos = q - cc * ny;
+      const int owner = pos / TXR;
+      C* rb = cl.map_shared_rank(rowbuf, owner);
+      rb[(u * TXY + cc) * PR + (pos - owner * TXR)] = ytile[cc * YP + pos];
+    }
+    __syncthreads();   // the next tile reuses the buffer
+  }
+  cl.sync();           // every row tile of the cluster is complete
+  // ---- phase 2: C2R of rows j = rank TXR + tt (the steps of rows_body after its staging)
+  for (int q = tid; q < (NX / 2 + 1) * TXR; q += NTH) {
+    const int tt = q % TXR, kk = q / TXR;
+    const int kc = NX - kk;
+    C a = rowbuf[kk * PR + tt], b = rowbuf[kc * PR + tt];
+    if (kk == 0) {
+      a.y = 0.f;
+      b.y = 0.f;
+    }
+    C w = stw[kk];
+    w.y = -w.y;
+    const C bc = cmk<C>(b.x, -b.y);
+    const C zk = cadd(cadd(a, bc), cmul_si<+1>(cmul(w, csub(a, bc))));
+    if (kk != 0 && kc != kk) {
+      C w2 = stw[kc];
+      w2.y = -w2.y;
+      const C ac = cmk<C>(a.x, -a.y);
+      rowbuf[kc * PR + tt] = cadd(cadd(b, ac), cmul_si<+1>(cmul(w2, csub(b, ac))));
+    }
+    rowbuf[kk * PR + tt] = zk;
+  }
+  __syncthreads();
+  fft_rows_inv<float, LX, TXR, TPCR>(rowbuf, stwN);
+  float* dst = out + (long long)r * ((long long)g.nx * g.ny * g.nz) + (long long)k * g.ny * g.nx;
+  const int nxh = (g.nx + 1) / 2;
+  const bool even = (g.nx & 1) == 0;
+  const int lane = tid & 31, warp = tid >> 5;
+  for (int tt = warp; tt < TXR; tt += NTH / 32) {
+    const int j = rank * TXR + tt;
+    if (j >= ny) break;
+    float* rp = dst + (long long)j * g.nx;
+    for (int m = lane; m < nxh; m += 32) {
+      const C z = rowbuf[m * PR + tt];
+      if (even) {
+        reinterpret_cast<float2*>(rp)[m] = make_float2(z.x, z.y);
+      } else {
+        rp[2 * m] = z.x;
+        if (2 * m + 1 < g.nx) rp[2 * m + 1] = z.y;
+      }
+    }
+  }
+}
+
 // first inverse pass with the coefficient synthesis fused into the loader
 // (GAUSS: igauss of the realizations, 0 phases, 1 Gaussian coefficients)
 template <typename R, int LOGN, int V, int GAUSS>
@@ -310,6 +440,15 @@ __global__ void __launch_bounds__(RowWarpCfg<R, LOGN>::NTH)
                 int nreal, int nblk_per_r, double* __restrict__ part, Tw tw) {
   extern __shared__ __align__(16) unsigned char smraw[];
   rows_warp_body<R, O, LOGN>(g, in, rstride, out, ostride, nreal, nblk_per_r, part, tw, blockIdx.x, smraw);
+}
+
+// x pass with two rows per lane on packed FP32 (rows_pair_body)
+template <typename O, int LOGN>
+__global__ void __launch_bounds__(RowPairCfg<LOGN>::NTH, 3)
+    k_rows_pair(Geo g, const float2* __restrict__ in, long long rstride, O* __restrict__ out, long long ostride,
+                int nreal, int nblk_per_r, double* __restrict__ part, Tw tw) {
+  extern __shared__ __align__(16) unsigned char smraw[];
+  rows_pair_body<O, LOGN>(g, in, rstride, out, ostride, nreal, nblk_per_r, part, tw, blockIdx.x, smraw);
 }
 
 // npx == 1: the x axis is trivial, x[0] = Re X[0]
@@ -824,6 +963,26 @@ static cudaError_t run_rows_warp(const Geo& g, const cpx_t<R>* in, long long rst
   }
 }
 
+// row pass variant 6: two rows per lane on packed FP32, for the lengths
+// RowPairCfg covers (variant 4 elsewhere, and for FP64)
+template <typename R, typename O, int L>
+static cudaError_t run_rows_pair(const Geo& g, const cpx_t<R>* in, long long rstride, O* out, long long ostride,
+                                 int nreal, double* part, int* nblk_out, Tw tw, cudaStream_t st) {
+  using W = RowPairCfg<L>;
+  if constexpr (sizeof(R) != 4 || !W::ok) {
+    return run_rows_warp<R, O, L>(g, in, rstride, out, ostride, nreal, part, nblk_out, tw, st);
+  } else {
+    cudaError_t e = set_smem(k_rows_pair<O, L>, W::smem);
+    if (e != cudaSuccess) return e;
+    int nblk = (g.ny * g.nz + W::ROWS - 1) / W::ROWS;
+    if (nblk_out) *nblk_out = nblk;
+    k_rows_pair<O, L><<<(unsigned)((long long)nblk * nreal), W::NTH, W::smem, st>>>(
+        g, reinterpret_cast<const float2*>(in), rstride, out, ostride, nreal, nblk, part, tw);
+    ++g_launch_count;
+    return cudaGetLastError();
+  }
+}
+
 // variants are compiled for transform lengths 32..1024; other lengths use variant 0
 constexpr bool tuned_len(int L) { return L >= 5 && L <= 10; }
 template <typename R> constexpr int prec_index() { return sizeof(R) == 4 ? 1 : 0; }
@@ -893,7 +1052,9 @@ static cudaError_t run_rows_c2r(const Geo& g, const cpx_t<R>* in, long long rstr
       case 1: return run_rows_c2r_v<R, O, L, 1>(g, in, rstride, out, ostride, nreal, part, nblk_out, tw, st);
       case 2: return run_rows_c2r_v<R, O, L, 2>(g, in, rstride, out, ostride, nreal, part, nblk_out, tw, st);
       case 3: return run_rows_c2r_v<R, O, L, 3>(g, in, rstride, out, ostride, nreal, part, nblk_out, tw, st);
-      case 4: return run_rows_warp<R, O, L>(g, in, rstride, out, ostride, nreal, part, nblk_out, tw, st);
+      case 4:   // 5 (the fused middle + row pass) where it does not apply runs variant 4
+      case 5: return run_rows_warp<R, O, L>(g, in, rstride, out, ostride, nreal, part, nblk_out, tw, st);
+      case 6: return run_rows_pair<R, O, L>(g, in, rstride, out, ostride, nreal, part, nblk_out, tw, st);
       default: break;
     }
   }
@@ -945,17 +1106,82 @@ static cudaError_t run_spec_rows(const Model& m, const double d[3], const Geo& g
   return cudaGetLastError();
 }
 
+// fused middle + row passes (row variant 5): whether it takes grid g, and the launch
+template <int LY, int LX, int CL>
+static cudaError_t run_yx_cl(const Geo& g, const float2* work, long long wstride, int nreal, float* out, Tw tw,
+                             cudaStream_t st) {
+  using Y = YXCfg<LY, LX>;
+  auto kern = k_yx_fused<LY, LX, CL>;
+  cudaError_t e = func_smem(reinterpret_cast<const void*>(kern), Y::SMEM);
+  if (e != cudaSuccess) return e;
+  const long long blocks = (long long)g.nz * nreal * CL;
+  if (blocks >= (1LL << 31)) return cudaErrorInvalidValue;
+  kern<<<(unsigned)blocks, Y::NTH, Y::SMEM, st>>>(g, work, wstride, out, tw);
+  ++g_launch_count;
+  return cudaGetLastError();
+}
+
+template <int LY, int LX>
+static cudaError_t run_yx(const Geo& g, const float2* work, long long wstride, int nreal, float* out, Tw tw,
+                          cudaStream_t st) {
+  using Y = YXCfg<LY, LX>;
+  if constexpr (!Y::ok) {
+    return cudaErrorInvalidValue;
+  } else {
+    const int need = (g.ny + Y::TXR - 1) / Y::TXR;   // CTAs that own rows
+    if (need <= 2) return run_yx_cl<LY, LX, 2>(g, work, wstride, nreal, out, tw, st);
+    if (need <= 4) return run_yx_cl<LY, LX, 4>(g, work, wstride, nreal, out, tw, st);
+    return run_yx_cl<LY, LX, 8>(g, work, wstride, nreal, out, tw, st);
+  }
+}
+
+static bool yx_fused_ok(const Geo& g) {
+  const int Ly = ilog2(g.npy), Lx = ilog2(g.npx) - 1;
+  if (g.npz < 2 || Ly < 6 || Ly > 9 || Lx < 7 || Lx > 9) return false;
+  const int txr = std::min(64, std::max(1, 8192 >> Lx));   // RowCfg<float, Lx, 0>::TX
+  return g.ny <= 8 * txr;
+}
+
+template <int LY>
+static cudaError_t run_yx_lx(const Geo& g, const float2* work, long long wstride, int nreal, float* out, Tw tw,
+                             cudaStream_t st) {
+  switch (ilog2(g.npx) - 1) {
+    case 7: return run_yx<LY, 7>(g, work, wstride, nreal, out, tw, st);
+    case 8: return run_yx<LY, 8>(g, work, wstride, nreal, out, tw, st);
+    case 9: return run_yx<LY, 9>(g, work, wstride, nreal, out, tw, st);
+    default: return cudaErrorInvalidValue;
+  }
+}
+
+static cudaError_t launch_yx_fused(const Geo& g, const float2* work, long long wstride, int nreal, float* out, Tw tw,
+                                   cudaStream_t st) {
+  switch (ilog2(g.npy)) {
+    case 6: return run_yx_lx<6>(g, work, wstride, nreal, out, tw, st);
+    case 7: return run_yx_lx<7>(g, work, wstride, nreal, out, tw, st);
+    case 8: return run_yx_lx<8>(g, work, wstride, nreal, out, tw, st);
+    case 9: return run_yx_lx<9>(g, work, wstride, nreal, out, tw, st);
+    default: return cudaErrorInvalidValue;
+  }
+}
+
 // x pass rows kernel: number of row blocks per realization (for the partial sums)
 int realize_part_blocks(const Geo& g, bool dbl) {
   if (g.npx == 1) return (g.ny * g.nz + NT - 1) / NT;
   int L = ilog2(g.npx) - 1;
   int v = tuned_len(L) ? g_variant[2][dbl ? 0 : 1][L] : 0;
+  // 5 (fused, never with statistics) and 6 outside its lengths run variant 4
+  if (v == 5 || (v == 6 && (dbl || L < 3 || L > 8))) v = 4;
+  if (v == 6) {   // RowPairCfg
+    const int tpc = (1 << L) / 8;                       // lanes per row pair
+    const int rows = 16 * (tpc >= 32 ? 1 : 32 / tpc);   // rows per block
+    return (g.ny * g.nz + rows - 1) / rows;
+  }
   if (v == 4 && L >= 3 && L <= (dbl ? 8 : 9)) {   // RowWarpCfg
     const int tpc = (1 << L) / (L > 8 ? 16 : 8);      // lanes per row
     const int rows = 8 * (tpc >= 32 ? 1 : 32 / tpc);  // rows per block
     return (g.ny * g.nz + rows - 1) / rows;
   }
-  if (v == 4) v = 0;
+  if (v >= 4) v = 0;   // 4 outside its lengths runs variant 0
   int E = (dbl ? 4096 : 8192) >> ((v >> 1) & 1);
   int tx = std::min(64, std::max(1, E >> L));
   return (g.ny * g.nz + tx - 1) / tx;
@@ -1148,6 +1374,15 @@ cudaError_t launch_realize(const Geo& g, const R* amp, const uint32_t* rowstates
     if (e == cudaSuccess) e = first_pass_done();
     if (e != cudaSuccess) return e;
     if (g.npy > 1) {
+      if constexpr (sizeof(R) == 4) {
+        // row variant 5: middle and row passes in one cluster kernel per plane
+        const int Lx = ilog2(g.npx) - 1;
+        if (out_kind == 0 && part == nullptr && Lx >= 0 && Lx < 16 && g_variant[2][1][Lx] == 5 &&
+            yx_fused_ok(g)) {
+          mark(marks, 3, st);
+          return launch_yx_fused(g, work, wstride, nreal, (float*)out, tw, st);
+        }
+      }
       mark(marks, 2, st);
       AxisArgs b{};
       b.S = g.HP;

@@ -133,7 +133,9 @@ def test_variant_selection_ranges():
                 for v in range(4):
                     assert L.ss3d_set_variant(kind, prec, 8, v) == 0
             assert L.ss3d_set_variant(2, prec, 8, 4) == 0
-            assert L.ss3d_set_variant(2, prec, 8, 5) != 0
+            assert (L.ss3d_set_variant(2, prec, 8, 5) == 0) == (prec == ss.FP32)   # fused middle + rows
+            assert (L.ss3d_set_variant(2, prec, 8, 6) == 0) == (prec == ss.FP32)   # two rows per lane
+            assert L.ss3d_set_variant(2, prec, 8, 7) != 0
             assert L.ss3d_set_variant(0, prec, 8, -1) != 0
             assert L.ss3d_set_variant(3, prec, 8, 0) != 0
         for kind in (0, 1):

@@ -161,7 +161,7 @@ def test_tile_variants_give_identical_results(gpu):
         for kind, logn in ((0, 7), (1, 5), (2, 6)):
             L.ss3d_set_variant(kind, prec, logn, 0)
     chosen = gpu.autotune(sp, 1, gpu.FP32, 2)
-    assert chosen["row_pass"] in {0, 1, 2, 3, 4} and set(chosen.values()) <= set(range(10))
+    assert chosen["row_pass"] in set(range(7)) and set(chosen.values()) <= set(range(10))
     assert np.array_equal(sp.realize(77, 2, 1, gpu.FP32), sp.realize(77, 2, 1, gpu.FP32))
 
 
@@ -204,7 +204,7 @@ def test_two_line_variants_identical(gpu, n, ipad, igauss):
     finally:
         for kind, lg in kinds:
             L.ss3d_set_variant(kind, gpu.FP32, lg, 0)
-    assert L.ss3d_set_variant(2, gpu.FP32, 6, 5) != 0      # the row pass has no two-line tiles
+    assert L.ss3d_set_variant(2, gpu.FP32, 6, 7) != 0      # the row pass has no two-line tiles
     assert L.ss3d_set_variant(1, gpu.FP32, 6, 8) != 0      # bulk-copy tiles: middle pass only
     assert L.ss3d_set_variant(0, gpu.FP32, 6, 10) != 0
 
@@ -232,6 +232,42 @@ def test_row_warp_variant_identical(gpu, n, prec):
     finally:
         L.ss3d_set_variant(2, P, lg, 0)
     assert np.array_equal(got, ref), float(np.max(np.abs(got - ref)))
+    assert np.allclose(zgot, zref, rtol=1e-12, atol=1e-12)
+
+
+@pytest.mark.parametrize("n", [(40, 36, 20), (256, 3, 2), (33, 17, 1), (100, 1, 30), (101, 3, 5), (200, 9, 7),
+                               (120, 7, 3), (600, 2, 1), (256, 256, 9)])
+def test_row_pair_variant_identical(gpu, n):
+    """Row pass variant 6 (FP32: two rows per lane on packed FP32) gives the
+    bits of the one-row kernels, for odd and even nx, odd row counts (a pair
+    that straddles two planes, a last row without a partner), row lengths
+    32..256 and, past them, the variant 4 fallback (npx 1024); float32 and
+    float64 outputs, the mean / variance table, and through a batch."""
+    import torch
+    from specsim3d_b200 import _lib
+    L = _lib.lib()
+    sts = [(2, 0.9, 12.0, 7.0, 4.0, 20.0, 0.0, 0.0)]
+    sp = gpu.Spectrum(sts, 0.1, (1.0, 1.0, 1.0), n, 1)
+    lg = int(sp.np[0]).bit_length() - 2
+    if not 5 <= lg <= 10:
+        pytest.skip("row length outside the tuned range")
+    ref, zref = sp.realize(4321, 3, 1, gpu.FP32, dtype=np.float32, zstats=True)
+    ref64 = sp.realize(4321, 3, 1, gpu.FP32, dtype=np.float64)
+    try:
+        assert L.ss3d_set_variant(2, gpu.FP32, lg, 6) == 0
+        got, zgot = sp.realize(4321, 3, 1, gpu.FP32, dtype=np.float32, zstats=True)
+        got64 = sp.realize(4321, 3, 1, gpu.FP32, dtype=np.float64)
+        out = torch.empty((3, n[2], n[1], n[0]), dtype=torch.float32, device="cuda")
+        b = gpu.Batch([(sp, 4321, 1, 0, 3, out)])
+        b.run()
+        b.close()
+        gotb = out.cpu().numpy()
+    finally:
+        L.ss3d_set_variant(2, gpu.FP32, lg, 0)
+    sp.close()
+    assert np.array_equal(got, ref), float(np.max(np.abs(got - ref)))
+    assert np.array_equal(got64, ref64)
+    assert np.array_equal(gotb, ref)
     assert np.allclose(zgot, zref, rtol=1e-12, atol=1e-12)
 
 
@@ -321,3 +357,39 @@ def test_bulk_copy_middle_pass_identical(gpu, n):
             assert np.array_equal(out.cpu().numpy(), ref)
     finally:
         L.ss3d_set_variant(0, gpu.FP32, lg, 0)
+
+
+@pytest.mark.parametrize("n", [(256, 256, 16), (200, 180, 9), (100, 64, 20), (300, 256, 5), (64, 40, 30),
+                               (256, 256, 256)])
+def test_fused_middle_row_pass_identical(gpu, n):
+    """Row variant 5 (FP32): the middle (y) and row (x) passes of a plane in one
+    thread-block cluster, the y output handed to the row tiles through
+    distributed shared memory, gives the bits of the separate passes, per call
+    and batched, for cluster sizes 2..8 (rows per CTA times CTAs >= ny) and
+    row lengths 256..1024."""
+    import torch
+    from specsim3d_b200 import _lib
+    L = _lib.lib()
+    sts = [(2, 1.0, 30.0, 12.0, 6.0, 20.0, 5.0, 0.0)]
+    sp = gpu.Spectrum(sts, 0.05, (1.0, 1.0, 1.0), n, 1)
+    lx = int(sp.np[0]).bit_length() - 2
+    ly = int(sp.np[1]).bit_length() - 1
+    if not (7 <= lx <= 9 and 6 <= ly <= 9 and sp.np[2] > 1):
+        pytest.skip(f"periodic grid {sp.np} outside the fused pass's lengths")
+    k = 2 if n[2] > 64 else 3
+    ref = sp.realize(97531, k, 1, gpu.FP32, dtype=np.float32)
+    try:
+        assert L.ss3d_set_variant(2, gpu.FP32, lx, 5) == 0
+        got = sp.realize(97531, k, 1, gpu.FP32, dtype=np.float32)
+        assert np.array_equal(got, ref), float(np.max(np.abs(got - ref)))
+        out = torch.empty((k, n[2], n[1], n[0]), dtype=torch.float32, device="cuda")
+        b = gpu.Batch([(sp, 97531, 1, 0, k, out)])
+        b.run()
+        b.close()
+        assert np.array_equal(out.cpu().numpy(), ref)
+        # statistics requested: the separate passes run, same values
+        got2, zs = sp.realize(97531, k, 1, gpu.FP32, dtype=np.float32, zstats=True)
+        assert np.array_equal(got2, ref)
+    finally:
+        L.ss3d_set_variant(2, gpu.FP32, lx, 0)
+    sp.close()
