@@ -162,16 +162,33 @@ __device__ __forceinline__ float rsqrt_nr(float x) {
 }
 
 // neighbour search of nodes [node0, node0 + count): writes nn and the
-// neighbour ids (0-based data index) and flags the exact data nodes.  CAP >=
-// ndmax bounds the per-thread candidate list (local memory): a list of 100
-// entries for ndmax 24 spilled about 400 bytes per node to DRAM.
+// neighbour ids (0-based data index) and flags the exact data nodes.
+// sxyz[p] = (x, y, z, id) of the p-th datum in super-block order (the order of
+// sbidx), so that the scan of a super block reads its data directly.  The
+// candidate list of a thread (CAP >= ndmax entries) lives in shared memory,
+// entry m of thread t at [m][t]; BS threads per block keep it within the
+// 48 KB of static shared memory.
+// A candidate is rejected when s = rx^2 + ry^2 + rz^2 > rmax^2, with no
+// division: for correctly rounded division RN(s / c) > 1 holds exactly when
+// s > c (s > c means s >= c + ulp(c), so s / c > 1 + 2^-53, above the midpoint
+// between 1 and its successor), so the test is the reference's d2 > 1
+// (f90:1249-1262); accepted candidates get d2 = RN(s / rmax^2) as there.
+template <int CAP> struct SearchCfg {
+  static constexpr int BS = CAP <= 32 ? 128 : (CAP <= 64 ? 64 : 32);
+};
 template <int CAP>
-__global__ void k_cond_search(CondGeo G, long long node0, int count, const double* __restrict__ dxs,
-                              const double* __restrict__ dys, const double* __restrict__ dzs,
-                              const int* __restrict__ sbstart, const int* __restrict__ sbidx,
-                              const int* __restrict__ ix, const int* __restrict__ iy, const int* __restrict__ iz,
-                              int* __restrict__ nbr, int* __restrict__ nnb) {
-  const int q = blockIdx.x * blockDim.x + threadIdx.x;
+__global__ void __launch_bounds__(SearchCfg<CAP>::BS) k_cond_search(CondGeo G, long long node0, int count,
+                                                                   const double4* __restrict__ sxyz,
+                                                                   const int* __restrict__ sbstart,
+                                                                   const int* __restrict__ ix,
+                                                                   const int* __restrict__ iy,
+                                                                   const int* __restrict__ iz, int* __restrict__ nbr,
+                                                                   int* __restrict__ nnb) {
+  constexpr int BS = SearchCfg<CAP>::BS;
+  __shared__ double cds[CAP][BS];
+  __shared__ int cids[CAP][BS];
+  const int t = threadIdx.x;
+  const int q = blockIdx.x * BS + t;
   if (q >= count) return;
   const long long node = node0 + q;
   const int i = (int)(node % G.nx) + 1;
@@ -183,49 +200,51 @@ __global__ void k_cond_search(CondGeo G, long long node0, int count, const doubl
   const int bx = clampi((int)__ddiv_rn(__dadd_rn(__dsub_rn(x, G.xmin), __dmul_rn(0.5, G.dx)), G.bsx) + 1, 1, G.nsbx);
   const int by = clampi((int)__ddiv_rn(__dadd_rn(__dsub_rn(y, G.ymin), __dmul_rn(0.5, G.dy)), G.bsy) + 1, 1, G.nsby);
   const int bz = clampi((int)__ddiv_rn(__dadd_rn(__dsub_rn(z, G.zmin), __dmul_rn(0.5, G.dz)), G.bsz) + 1, 1, G.nsbz);
-  double cd[CAP];
-  int cid[CAP];
   int nn = 0;
   const int ndmax = G.ndmax;
+  double worst = 0.0;   // cds[nn - 1][t] once the list is full
   for (int kb = max(1, bz - G.mbz); kb <= min(G.nsbz, bz + G.mbz); ++kb)
     for (int jb = max(1, by - G.mby); jb <= min(G.nsby, by + G.mby); ++jb)
       for (int ib = max(1, bx - G.mbx); ib <= min(G.nsbx, bx + G.mbx); ++ib) {
         const int blk = ib + G.nsbx * (jb - 1 + G.nsby * (kb - 1));
         const int p1 = __ldg(sbstart + blk) - 1;
         for (int p = __ldg(sbstart + blk - 1); p <= p1; ++p) {
-          const int d = __ldg(sbidx + p - 1) - 1;
-          const double hx = __dsub_rn(__ldg(dxs + d), x), hy = __dsub_rn(__ldg(dys + d), y),
-                       hz = __dsub_rn(__ldg(dzs + d), z);
+          const double2 a = __ldg(reinterpret_cast<const double2*>(sxyz + p - 1));
+          const double2 b = __ldg(reinterpret_cast<const double2*>(sxyz + p - 1) + 1);
+          const double hx = __dsub_rn(a.x, x), hy = __dsub_rn(a.y, y), hz = __dsub_rn(b.x, z);
           const double rx = __dadd_rn(__dadd_rn(__dmul_rn(G.rot[0], hx), __dmul_rn(G.rot[1], hy)), __dmul_rn(G.rot[2], hz));
           const double ry = __dadd_rn(__dadd_rn(__dmul_rn(G.rot[3], hx), __dmul_rn(G.rot[4], hy)), __dmul_rn(G.rot[5], hz));
           const double rz = __dadd_rn(__dadd_rn(__dmul_rn(G.rot[6], hx), __dmul_rn(G.rot[7], hy)), __dmul_rn(G.rot[8], hz));
-          const double d2 = __ddiv_rn(__dadd_rn(__dadd_rn(__dmul_rn(rx, rx), __dmul_rn(ry, ry)), __dmul_rn(rz, rz)), G.rmax2);
-          if (d2 > 1.0) continue;
+          const double s2 = __dadd_rn(__dadd_rn(__dmul_rn(rx, rx), __dmul_rn(ry, ry)), __dmul_rn(rz, rz));
+          if (s2 > G.rmax2) continue;
+          const double d2 = __ddiv_rn(s2, G.rmax2);
           int m;
           if (nn < ndmax) {
             nn = nn + 1;
             m = nn;
-          } else if (d2 < cd[nn - 1]) {
+          } else if (d2 < worst) {
             m = nn;
           } else {
             continue;
           }
           while (m > 1) {
-            if (cd[m - 2] <= d2) break;
-            cd[m - 1] = cd[m - 2];
-            cid[m - 1] = cid[m - 2];
+            const double prev = cds[m - 2][t];
+            if (prev <= d2) break;
+            cds[m - 1][t] = prev;
+            cids[m - 1][t] = cids[m - 2][t];
             m = m - 1;
           }
-          cd[m - 1] = d2;
-          cid[m - 1] = d;
+          cds[m - 1][t] = d2;
+          cids[m - 1][t] = (int)b.y;
+          if (nn == ndmax) worst = cds[nn - 1][t];
         }
       }
   int* out = nbr + (long long)q * ndmax;
-  for (int m = 0; m < nn; ++m) out[m] = cid[m];
+  for (int m = 0; m < nn; ++m) out[m] = cids[m][t];
   // exact data node: nearest at distance 0 and on this very node
   int flag = 0;
-  if (nn > 0 && cd[0] == 0.0) {
-    const int d = cid[0];
+  if (nn > 0 && cds[0][t] == 0.0) {
+    const int d = cids[0][t];
     if (__ldg(ix + d) == i && __ldg(iy + d) == j && __ldg(iz + d) == k) flag = 1;
   }
   nnb[q] = nn | (flag << 16);
@@ -452,7 +471,7 @@ __global__ void k_cond_krige(CondGeo G, KModel mdl, CovTab ctab, long long node0
     for (int off = 16; off > 0; off >>= 1) zk += __shfl_xor_sync(0xffffffffu, zk, off);
     for (int l = lane; l < G.nreal; l += 32) {
       double sks = 0.0;
-      for (int p = 0; p < nn; ++p) sks += w[p] * simd[id[p] + (long long)G.nd * l];
+      for (int p = 0; p < nn; ++p) sks += w[p] * simd[(long long)id[p] * G.nreal + l];
       res[node + M * l] = zk + res[node + M * l] - sks;
     }
     __syncwarp();
@@ -486,8 +505,19 @@ template <int PREC, int NDT> struct KregLayout {
   static constexpr int BYTES = ((PREC == 0 ? AS : AS + NDT * PITCH * 8) + 15) & ~15;
 };
 
-template <int PREC, int NDT>
-__global__ void __launch_bounds__(256, 2) k_cond_krige_reg(CondGeo G, const KModel* __restrict__ mdl, CovTab ctab,
+// CTAs per SM asked of the register allocator for NDT = 32 (the smaller
+// classes ask for 3)
+#ifndef KREG_MINB32
+#define KREG_MINB32 2
+#endif
+// the strict lower triangle of an NDT x NDT system: entries, and entries per lane
+template <int NDT> struct KregTri {
+  static constexpr int NE = NDT * (NDT - 1) / 2;
+  static constexpr int NIT = (NE + 31) / 32;
+};
+
+template <int PREC, int NDT, int MINB>
+__global__ void __launch_bounds__(256, MINB) k_cond_krige_reg(CondGeo G, const KModel* __restrict__ mdl, CovTab ctab,
                                                         long long node0,
                                                         int count, const int* __restrict__ nbr,
                                                         const int* __restrict__ nnb, const int* __restrict__ ixs,
@@ -496,13 +526,20 @@ __global__ void __launch_bounds__(256, 2) k_cond_krige_reg(CondGeo G, const KMod
                                                         const double* __restrict__ simd, double* __restrict__ res,
                                                         unsigned long long* __restrict__ counters) {
   using Ly = KregLayout<PREC, NDT>;
+  using KT = KregTri<NDT>;
   using T = typename Ly::T;
   constexpr int PITCH = Ly::PITCH;
+  constexpr int KV = 16 / (int)sizeof(T);   // column elements per 16-byte load
+  static_assert(NDT % KV == 0 && Ly::COL % 16 == 0 && Ly::BYTES % 16 == 0, "16-byte column loads");
   extern __shared__ __align__(16) unsigned char smk[];
   __shared__ unsigned long long bcount[4];
+  __shared__ unsigned short tri[KT::NE > 0 ? KT::NE : 1];   // (r << 8) | c of entry e
   const int lane = threadIdx.x & 31, wib = threadIdx.x >> 5;
   const int nwb = blockDim.x >> 5;
   if (threadIdx.x < 4) bcount[threadIdx.x] = 0;
+  for (int r = 1 + (int)threadIdx.x; r < NDT; r += blockDim.x)
+    for (int c = 0; c < r; ++c) tri[r * (r - 1) / 2 + c] = (unsigned short)((r << 8) | c);
+  const double c00 = cov_lat_g(ctab, mdl, 0, 0, 0, G.dx, G.dy, G.dz);
   __syncthreads();
   unsigned char* mine = smk + (size_t)Ly::BYTES * wib;
   int4* lat = reinterpret_cast<int4*>(mine + Ly::LAT);
@@ -539,20 +576,61 @@ __global__ void __launch_bounds__(256, 2) k_cond_krige_reg(CondGeo G, const KMod
     }
     __syncwarp();
     const double b = act ? cov_lat_g(ctab, mdl, me.x - i, me.y - j, me.z - k, G.dx, G.dy, G.dz) : 0.0;
-    // row `lane` of A in shared memory (FP64 in As for the FP32 form, else in Ls)
-    if (lane < NDT) {
-      for (int c = 0; c < NDT; ++c) {
-        double v = 0.0;
-        if (c < nn && act) {
-          const int4 o = lat[c];
-          v = cov_lat_g(ctab, mdl, me.x - o.x, me.y - o.y, me.z - o.z, G.dx, G.dy, G.dz);
+    // A in shared memory (FP64 in As for the FP32 form, else in Ls): the
+    // strict lower triangle spread over the lanes (entry e = r (r-1)/2 + c,
+    // c < r < nn), every table load of a lane issued before any is used, the
+    // lags outside the table evaluated afterwards, each value stored at (r, c)
+    // and (c, r) (C(h) = C(-h) holds bitwise: the rotated components of -h are
+    // the negated components of h); the diagonal is C(0).  Entries of rows or
+    // columns past nn are not written: no valid entry reads them.
+    {
+      double* A = PREC == 1 ? As : reinterpret_cast<double*>(Ls);
+      const int ne = nn * (nn - 1) / 2;
+      double v[KT::NIT];
+      int rc[KT::NIT];
+      bool far[KT::NIT];
+#pragma unroll
+      for (int it = 0; it < KT::NIT; ++it) {
+        const int e = lane + 32 * it;
+        rc[it] = e < ne ? (int)tri[e] : 0;
+        const int4 o = lat[rc[it] >> 8], p = lat[rc[it] & 255];
+        int di = o.x - p.x, dj = o.y - p.y, dk = o.z - p.z;
+        if (dk < 0) {
+          di = -di;
+          dj = -dj;
+          dk = -dk;
         }
+        far[it] = !(ctab.v && dk <= ctab.tz && abs(dj) <= ctab.ty && abs(di) <= ctab.tx);
+        const size_t off =
+            (size_t)(di + ctab.tx) + (size_t)(2 * ctab.tx + 1) * ((dj + ctab.ty) + (size_t)(2 * ctab.ty + 1) * dk);
+        v[it] = far[it] ? 0.0 : __ldg(ctab.v + off);
+      }
+#pragma unroll
+      for (int it = 0; it < KT::NIT; ++it) {
+        const int e = lane + 32 * it;
+        if (e < ne) {
+          const int r = rc[it] >> 8, c = rc[it] & 255;
+          if (far[it]) {   // outside the table (or no table): evaluated directly
+            const int4 o = lat[r], p = lat[c];
+            v[it] = cov_lat_g(ctab, mdl, o.x - p.x, o.y - p.y, o.z - p.z, G.dx, G.dy, G.dz);
+          }
+          if constexpr (PREC == 1) {
+            A[r * PITCH + c] = v[it];
+            A[c * PITCH + r] = v[it];
+          } else {
+            Ls[r * PITCH + c] = v[it];
+            Ls[c * PITCH + r] = v[it];
+          }
+        }
+      }
+      if (act) {
         if constexpr (PREC == 1)
-          As[lane * PITCH + c] = v;
+          A[lane * PITCH + lane] = c00;
         else
-          Ls[lane * PITCH + c] = v;
+          Ls[lane * PITCH + lane] = c00;
       }
     }
+    __syncwarp();
     double ridge = 1.0e-10 * G.c0;
     T a[NDT];
     T myinv = T(0), yv = T(0);
@@ -588,7 +666,15 @@ __global__ void __launch_bounds__(256, 2) k_cond_krige_reg(CondGeo G, const KMod
           if (lane == c) yv = yc;
           bcur = fma(-lrc, yc, bcur);
 #pragma unroll
-          for (int kk = c + 1; kk < NDT; ++kk) a[kk] = fma(-lrc, cb[kk], a[kk]);
+          for (int k0 = (c + 1) / KV * KV; k0 < NDT; k0 += KV) {
+            // the column 16 bytes at a time (every lane reads the same words:
+            // one wavefront per load); elements up to c are loaded, not used
+            T cv[KV];
+            *reinterpret_cast<uint4*>(cv) = *reinterpret_cast<const uint4*>(cb + k0);
+#pragma unroll
+            for (int u = 0; u < KV; ++u)
+              if (k0 + u > c) a[k0 + u] = fma(-lrc, cv[u], a[k0 + u]);
+          }
         }
       }
       if (good) break;
@@ -651,9 +737,16 @@ __global__ void __launch_bounds__(256, 2) k_cond_krige_reg(CondGeo G, const KMod
 #pragma unroll
     for (int off = 16; off > 0; off >>= 1) zk += __shfl_xor_sync(0xffffffffu, zk, off);
     for (int l = lane; l < G.nreal; l += 32) {
+      // all gathers of the realization first, then the sum in neighbour order
+      double sv[NDT];
+#pragma unroll
+      for (int p = 0; p < NDT; ++p) sv[p] = p < nn ? simd[(long long)lat[p].w * G.nreal + l] : 0.0;
+      const double rv = res[node + M * l];
       double sks = 0.0;
-      for (int p = 0; p < nn; ++p) sks += wsm[p] * simd[lat[p].w + (long long)G.nd * l];
-      res[node + M * l] = zk + res[node + M * l] - sks;
+#pragma unroll
+      for (int p = 0; p < NDT; ++p)
+        if (p < nn) sks += wsm[p] * sv[p];
+      res[node + M * l] = zk + rv - sks;
     }
     __syncwarp();
   }
@@ -664,9 +757,11 @@ __global__ void __launch_bounds__(256, 2) k_cond_krige_reg(CondGeo G, const KMod
 __global__ void k_gather_simd(const double* __restrict__ res, long long M, const int* __restrict__ ix,
                               const int* __restrict__ iy, const int* __restrict__ iz, int nd, int nreal, int nx, int ny,
                               double* __restrict__ simd) {
+  // simd[d * nreal + l]: the realizations of one datum side by side, so that
+  // the lanes of a kriging warp (one realization each) read whole lines
   const long long tot = (long long)nd * nreal;
   for (long long q = blockIdx.x * (long long)blockDim.x + threadIdx.x; q < tot; q += (long long)gridDim.x * blockDim.x) {
-    const int d = (int)(q % nd), l = (int)(q / nd);
+    const int l = (int)(q % nreal), d = (int)(q / nreal);
     simd[q] = res[(ix[d] - 1) + (long long)nx * ((iy[d] - 1) + (long long)ny * (iz[d] - 1)) + M * l];
   }
 }
@@ -674,7 +769,10 @@ __global__ void k_gather_simd(const double* __restrict__ res, long long M, const
 // GSLIB back transform (backtr, powint, gcum), f90:628-697
 __device__ __forceinline__ double powint_d(double xlow, double xhigh, double ylow, double yhigh, double xval, double pw) {
   if (xhigh - xlow < 1.0e-20) return 0.5 * (ylow + yhigh);
-  return ylow + (yhigh - ylow) * pow((xval - xlow) / (xhigh - xlow), pw);
+  // t^1 = t exactly (the value a correctly rounded pow returns): the linear
+  // interpolation between table entries, the common case, takes no pow
+  const double t = (xval - xlow) / (xhigh - xlow);
+  return ylow + (yhigh - ylow) * (pw == 1.0 ? t : pow(t, pw));
 }
 __device__ __forceinline__ double gcum_d(double x) { return 0.5 * erfc(-x / 1.4142135623730951); }
 
@@ -989,8 +1087,8 @@ extern "C" int ss3d_condition(double* res, const int n[3], int nreal, const doub
   }
   double *ddx = nullptr, *ddy = nullptr, *ddz = nullptr, *ddg = nullptr, *dsimd = nullptr, *dvr = nullptr,
          *dgt = nullptr;
-  int *dix = nullptr, *diy = nullptr, *diz = nullptr, *dsbs = nullptr, *dsbi = nullptr, *dnbr = nullptr,
-      *dnnb = nullptr;
+  int *dix = nullptr, *diy = nullptr, *diz = nullptr, *dsbs = nullptr, *dnbr = nullptr, *dnnb = nullptr;
+  double4* dsxyz = nullptr;
   unsigned long long* dcnt = nullptr;
   const int chunk = (int)std::min<long long>(M, std::max<long long>(1, ((long long)1 << 30) / (4LL * cp->ndmax + 4)));
   if (e == cudaSuccess) e = bufs.alloc(&ddx, nd);
@@ -1002,7 +1100,7 @@ extern "C" int ss3d_condition(double* res, const int n[3], int nreal, const doub
   if (e == cudaSuccess) e = bufs.alloc(&diy, nd);
   if (e == cudaSuccess) e = bufs.alloc(&diz, nd);
   if (e == cudaSuccess) e = bufs.alloc(&dsbs, nsb + 1);
-  if (e == cudaSuccess) e = bufs.alloc(&dsbi, nd);
+  if (e == cudaSuccess) e = bufs.alloc(&dsxyz, nd);
   if (e == cudaSuccess) e = bufs.alloc(&dnbr, (size_t)chunk * cp->ndmax);
   if (e == cudaSuccess) e = bufs.alloc(&dnnb, chunk);
   if (e == cudaSuccess) e = bufs.alloc(&dcnt, 4);
@@ -1019,7 +1117,13 @@ extern "C" int ss3d_condition(double* res, const int n[3], int nreal, const doub
   h2d(diy, iy.data(), sizeof(int) * nd);
   h2d(diz, iz.data(), sizeof(int) * nd);
   h2d(dsbs, sbstart.data(), sizeof(int) * (nsb + 1));
-  h2d(dsbi, sbidx.data(), sizeof(int) * nd);
+  // the data in super-block order, (x, y, z, id) each
+  std::vector<double4> sxyz(nd);
+  for (int p = 0; p < nd; p++) {
+    const int d = sbidx[p] - 1;
+    sxyz[p] = make_double4(dxs[d], dys[d], dzs[d], (double)d);
+  }
+  h2d(dsxyz, sxyz.data(), sizeof(double4) * nd);
   h2d(dvr, vrt.data(), sizeof(double) * nd);
   h2d(dgt, gtt.data(), sizeof(double) * nd);
   if (e == cudaSuccess) e = cudaMemsetAsync(dcnt, 0, sizeof(unsigned long long) * 4, stm);
@@ -1059,14 +1163,14 @@ extern "C" int ss3d_condition(double* res, const int n[3], int nreal, const doub
   const void* kfn = nullptr;
   size_t per = 0, kfix = 0;
   switch (ndt * 2 + (fp32 ? 1 : 0)) {
-    case 16: kfn = (const void*)k_cond_krige_reg<0, 8>; per = KregLayout<0, 8>::BYTES; break;
-    case 17: kfn = (const void*)k_cond_krige_reg<1, 8>; per = KregLayout<1, 8>::BYTES; break;
-    case 32: kfn = (const void*)k_cond_krige_reg<0, 16>; per = KregLayout<0, 16>::BYTES; break;
-    case 33: kfn = (const void*)k_cond_krige_reg<1, 16>; per = KregLayout<1, 16>::BYTES; break;
-    case 48: kfn = (const void*)k_cond_krige_reg<0, 24>; per = KregLayout<0, 24>::BYTES; break;
-    case 49: kfn = (const void*)k_cond_krige_reg<1, 24>; per = KregLayout<1, 24>::BYTES; break;
-    case 64: kfn = (const void*)k_cond_krige_reg<0, 32>; per = KregLayout<0, 32>::BYTES; break;
-    case 65: kfn = (const void*)k_cond_krige_reg<1, 32>; per = KregLayout<1, 32>::BYTES; break;
+    case 16: kfn = (const void*)k_cond_krige_reg<0, 8, 3>; per = KregLayout<0, 8>::BYTES; break;
+    case 17: kfn = (const void*)k_cond_krige_reg<1, 8, 3>; per = KregLayout<1, 8>::BYTES; break;
+    case 32: kfn = (const void*)k_cond_krige_reg<0, 16, 3>; per = KregLayout<0, 16>::BYTES; break;
+    case 33: kfn = (const void*)k_cond_krige_reg<1, 16, 3>; per = KregLayout<1, 16>::BYTES; break;
+    case 48: kfn = (const void*)k_cond_krige_reg<0, 24, 3>; per = KregLayout<0, 24>::BYTES; break;
+    case 49: kfn = (const void*)k_cond_krige_reg<1, 24, 3>; per = KregLayout<1, 24>::BYTES; break;
+    case 64: kfn = (const void*)k_cond_krige_reg<0, 32, KREG_MINB32>; per = KregLayout<0, 32>::BYTES; break;
+    case 65: kfn = (const void*)k_cond_krige_reg<1, 32, KREG_MINB32>; per = KregLayout<1, 32>::BYTES; break;
     default:
       kfn = fp32 ? (const void*)k_cond_krige<1> : (const void*)k_cond_krige<0>;
       per = cond_warp_bytes(cp->ndmax, fp32 ? 1 : 0);
@@ -1079,20 +1183,23 @@ extern "C" int ss3d_condition(double* res, const int n[3], int nreal, const doub
   if (e == cudaSuccess) e = cudaMemcpyAsync(dmdl, &kmdl, sizeof kmdl, cudaMemcpyHostToDevice, stm);
   for (long long node0 = 0; node0 < M && e == cudaSuccess; node0 += chunk) {
     const int count = (int)std::min<long long>(chunk, M - node0);
-    const unsigned sblk = (unsigned)((count + 127) / 128);
+    auto search = [&](auto cap) {
+      constexpr int CAP = decltype(cap)::value, BS = SearchCfg<CAP>::BS;
+      k_cond_search<CAP><<<(unsigned)((count + BS - 1) / BS), BS, 0, stm>>>(G, node0, count, dsxyz, dsbs, dix, diy,
+                                                                          diz, dnbr, dnnb);
+    };
     if (cp->ndmax <= 8)
-      k_cond_search<8><<<sblk, 128, 0, stm>>>(G, node0, count, ddx, ddy, ddz, dsbs, dsbi, dix, diy, diz, dnbr, dnnb);
+      search(std::integral_constant<int, 8>());
     else if (cp->ndmax <= 16)
-      k_cond_search<16><<<sblk, 128, 0, stm>>>(G, node0, count, ddx, ddy, ddz, dsbs, dsbi, dix, diy, diz, dnbr, dnnb);
+      search(std::integral_constant<int, 16>());
     else if (cp->ndmax <= 24)
-      k_cond_search<24><<<sblk, 128, 0, stm>>>(G, node0, count, ddx, ddy, ddz, dsbs, dsbi, dix, diy, diz, dnbr, dnnb);
+      search(std::integral_constant<int, 24>());
     else if (cp->ndmax <= 32)
-      k_cond_search<32><<<sblk, 128, 0, stm>>>(G, node0, count, ddx, ddy, ddz, dsbs, dsbi, dix, diy, diz, dnbr, dnnb);
+      search(std::integral_constant<int, 32>());
     else if (cp->ndmax <= 64)
-      k_cond_search<64><<<sblk, 128, 0, stm>>>(G, node0, count, ddx, ddy, ddz, dsbs, dsbi, dix, diy, diz, dnbr, dnnb);
+      search(std::integral_constant<int, 64>());
     else
-      k_cond_search<100><<<sblk, 128, 0, stm>>>(G, node0, count, ddx, ddy, ddz, dsbs, dsbi, dix, diy, diz, dnbr,
-                                               dnnb);
+      search(std::integral_constant<int, 100>());
     ++g_launch_count;
     e = cudaGetLastError();
     if (e != cudaSuccess) break;
