@@ -57,6 +57,7 @@ struct CondGeo {
   double rot[9];       // search ellipsoid rotation (setrot of the search "structure")
   double rmax2;        // rmax * rmax
   double c0;           // C(0)
+  int nrow;            // rows of super-block offsets in the scan list
 };
 
 __device__ __forceinline__ int clampi(int v, int lo, int hi) { return v < lo ? lo : (v > hi ? hi : v); }
@@ -173,6 +174,13 @@ __device__ __forceinline__ float rsqrt_nr(float x) {
 // s > c (s > c means s >= c + ulp(c), so s / c > 1 + 2^-53, above the midpoint
 // between 1 and its successor), so the test is the reference's d2 > 1
 // (f90:1249-1262); accepted candidates get d2 = RN(s / rmax^2) as there.
+// rows[r] = (x offset from, x offset to, y offset, z offset): the super-block
+// offsets of the search box by rows along x, in the reference's scan order (z,
+// then y, then x block ascending), without the blocks that can hold no datum
+// inside the ellipsoid for any node of the centre block (super_block_rows):
+// their candidates would all be rejected, so the kept neighbours and their
+// order are the same.  The data of the blocks of one row are contiguous in
+// super-block order, so a row is one range of sxyz.
 template <int CAP> struct SearchCfg {
   static constexpr int BS = CAP <= 32 ? 128 : (CAP <= 64 ? 64 : 32);
 };
@@ -180,6 +188,7 @@ template <int CAP>
 __global__ void __launch_bounds__(SearchCfg<CAP>::BS) k_cond_search(CondGeo G, long long node0, int count,
                                                                    const double4* __restrict__ sxyz,
                                                                    const int* __restrict__ sbstart,
+                                                                   const int4* __restrict__ rows,
                                                                    const int* __restrict__ ix,
                                                                    const int* __restrict__ iy,
                                                                    const int* __restrict__ iz, int* __restrict__ nbr,
@@ -203,42 +212,44 @@ __global__ void __launch_bounds__(SearchCfg<CAP>::BS) k_cond_search(CondGeo G, l
   int nn = 0;
   const int ndmax = G.ndmax;
   double worst = 0.0;   // cds[nn - 1][t] once the list is full
-  for (int kb = max(1, bz - G.mbz); kb <= min(G.nsbz, bz + G.mbz); ++kb)
-    for (int jb = max(1, by - G.mby); jb <= min(G.nsby, by + G.mby); ++jb)
-      for (int ib = max(1, bx - G.mbx); ib <= min(G.nsbx, bx + G.mbx); ++ib) {
-        const int blk = ib + G.nsbx * (jb - 1 + G.nsby * (kb - 1));
-        const int p1 = __ldg(sbstart + blk) - 1;
-        for (int p = __ldg(sbstart + blk - 1); p <= p1; ++p) {
-          const double2 a = __ldg(reinterpret_cast<const double2*>(sxyz + p - 1));
-          const double2 b = __ldg(reinterpret_cast<const double2*>(sxyz + p - 1) + 1);
-          const double hx = __dsub_rn(a.x, x), hy = __dsub_rn(a.y, y), hz = __dsub_rn(b.x, z);
-          const double rx = __dadd_rn(__dadd_rn(__dmul_rn(G.rot[0], hx), __dmul_rn(G.rot[1], hy)), __dmul_rn(G.rot[2], hz));
-          const double ry = __dadd_rn(__dadd_rn(__dmul_rn(G.rot[3], hx), __dmul_rn(G.rot[4], hy)), __dmul_rn(G.rot[5], hz));
-          const double rz = __dadd_rn(__dadd_rn(__dmul_rn(G.rot[6], hx), __dmul_rn(G.rot[7], hy)), __dmul_rn(G.rot[8], hz));
-          const double s2 = __dadd_rn(__dadd_rn(__dmul_rn(rx, rx), __dmul_rn(ry, ry)), __dmul_rn(rz, rz));
-          if (s2 > G.rmax2) continue;
-          const double d2 = __ddiv_rn(s2, G.rmax2);
-          int m;
-          if (nn < ndmax) {
-            nn = nn + 1;
-            m = nn;
-          } else if (d2 < worst) {
-            m = nn;
-          } else {
-            continue;
-          }
-          while (m > 1) {
-            const double prev = cds[m - 2][t];
-            if (prev <= d2) break;
-            cds[m - 1][t] = prev;
-            cids[m - 1][t] = cids[m - 2][t];
-            m = m - 1;
-          }
-          cds[m - 1][t] = d2;
-          cids[m - 1][t] = (int)b.y;
-          if (nn == ndmax) worst = cds[nn - 1][t];
-        }
+  for (int o = 0; o < G.nrow; ++o) {
+    const int4 rw = __ldg(rows + o);
+    const int jb = by + rw.z, kb = bz + rw.w;
+    const int ib0 = max(1, bx + rw.x), ib1 = min(G.nsbx, bx + rw.y);
+    if (jb < 1 || jb > G.nsby || kb < 1 || kb > G.nsbz || ib0 > ib1) continue;
+    const int row0 = G.nsbx * (jb - 1 + G.nsby * (kb - 1));
+    const int p1 = __ldg(sbstart + row0 + ib1) - 1;
+    for (int p = __ldg(sbstart + row0 + ib0 - 1); p <= p1; ++p) {
+      const double2 a = __ldg(reinterpret_cast<const double2*>(sxyz + p - 1));
+      const double2 b = __ldg(reinterpret_cast<const double2*>(sxyz + p - 1) + 1);
+      const double hx = __dsub_rn(a.x, x), hy = __dsub_rn(a.y, y), hz = __dsub_rn(b.x, z);
+      const double rx = __dadd_rn(__dadd_rn(__dmul_rn(G.rot[0], hx), __dmul_rn(G.rot[1], hy)), __dmul_rn(G.rot[2], hz));
+      const double ry = __dadd_rn(__dadd_rn(__dmul_rn(G.rot[3], hx), __dmul_rn(G.rot[4], hy)), __dmul_rn(G.rot[5], hz));
+      const double rz = __dadd_rn(__dadd_rn(__dmul_rn(G.rot[6], hx), __dmul_rn(G.rot[7], hy)), __dmul_rn(G.rot[8], hz));
+      const double s2 = __dadd_rn(__dadd_rn(__dmul_rn(rx, rx), __dmul_rn(ry, ry)), __dmul_rn(rz, rz));
+      if (s2 > G.rmax2) continue;
+      const double d2 = __ddiv_rn(s2, G.rmax2);
+      int m;
+      if (nn < ndmax) {
+        nn = nn + 1;
+        m = nn;
+      } else if (d2 < worst) {
+        m = nn;
+      } else {
+        continue;
       }
+      while (m > 1) {
+        const double prev = cds[m - 2][t];
+        if (prev <= d2) break;
+        cds[m - 1][t] = prev;
+        cids[m - 1][t] = cids[m - 2][t];
+        m = m - 1;
+      }
+      cds[m - 1][t] = d2;
+      cids[m - 1][t] = (int)b.y;
+      if (nn == ndmax) worst = cds[nn - 1][t];
+    }
+  }
   int* out = nbr + (long long)q * ndmax;
   for (int m = 0; m < nn; ++m) out[m] = cids[m][t];
   // exact data node: nearest at distance 0 and on this very node
@@ -900,6 +911,104 @@ struct DevBuf {
 
 }  // namespace
 
+namespace {
+// min of v^T Q v over the box lo <= v <= hi (Q symmetric positive definite),
+// exactly, by its active sets: each coordinate at its lower bound, at its
+// upper bound or free, the free ones solving the reduced stationarity
+// equations; -inf when a reduced system is singular (no pruning then)
+double box_min_quad(const double Q[3][3], const double lo[3], const double hi[3]) {
+  double best = INFINITY;
+  for (int code = 0; code < 27; ++code) {
+    const int st[3] = {code % 3, (code / 3) % 3, code / 9};   // 0 lower, 1 upper, 2 free
+    double v[3];
+    int fr[3], nf = 0;
+    for (int a = 0; a < 3; ++a) {
+      v[a] = st[a] == 0 ? lo[a] : (st[a] == 1 ? hi[a] : 0.0);
+      if (st[a] == 2) fr[nf++] = a;
+    }
+    if (nf > 0) {
+      double A[3][4];
+      for (int i = 0; i < nf; ++i) {
+        double b = 0.0;
+        for (int a = 0; a < 3; ++a)
+          if (st[a] != 2) b -= Q[fr[i]][a] * v[a];
+        for (int j = 0; j < nf; ++j) A[i][j] = Q[fr[i]][fr[j]];
+        A[i][nf] = b;
+      }
+      for (int c = 0; c < nf; ++c) {   // Gaussian elimination, partial pivoting
+        int pr = c;
+        for (int r = c + 1; r < nf; ++r)
+          if (fabs(A[r][c]) > fabs(A[pr][c])) pr = r;
+        if (!(fabs(A[pr][c]) > 1e-300)) return -INFINITY;
+        for (int j = 0; j <= nf; ++j) std::swap(A[c][j], A[pr][j]);
+        for (int r = 0; r < nf; ++r)
+          if (r != c) {
+            const double f = A[r][c] / A[c][c];
+            for (int j = c; j <= nf; ++j) A[r][j] -= f * A[c][j];
+          }
+      }
+      bool inside = true;
+      for (int i = 0; i < nf; ++i) {
+        v[fr[i]] = A[i][nf] / A[i][i];
+        if (v[fr[i]] < lo[fr[i]] || v[fr[i]] > hi[fr[i]]) inside = false;
+      }
+      if (!inside) continue;
+    }
+    double q = 0.0;
+    for (int a = 0; a < 3; ++a)
+      for (int b = 0; b < 3; ++b) q += v[a] * Q[a][b] * v[b];
+    best = std::min(best, q);
+  }
+  return best;
+}
+
+// The super-block offsets of the search box by rows along x, in the
+// reference's scan order (z, then y offset ascending), each row the x offsets
+// from its first to its last block that may hold a point inside the search
+// ellipsoid for some node of the centre block (rows with none are dropped).
+// A node and a datum whose blocks differ by o along an axis differ by a lag
+// in ((o - 1) bs, (o + 1) bs) along it (both are assigned to blocks by the
+// same shifted floor); the box is widened by 1e-6 bs for the rounding of that
+// assignment, and a block may hold such a point unless the smallest |R v|^2
+// over the box exceeds rmax^2 by more than 1e-9 relative (R the search
+// rotation, the d2 of the candidates being |R h|^2 / rmax^2).  Blocks between
+// the first and last of a row are scanned whatever their test: a block
+// scanned needlessly only adds rejected candidates.  Search boxes of more than
+// 4096 blocks keep every block.
+void super_block_rows(const CondGeo& G, std::vector<int4>& rows) {
+  const long long tot = (2LL * G.mbx + 1) * (2LL * G.mby + 1) * (2LL * G.mbz + 1);
+  double Q[3][3];
+  for (int r = 0; r < 3; ++r)
+    for (int c = 0; c < 3; ++c) {
+      double v = 0.0;
+      for (int k = 0; k < 3; ++k) v += G.rot[3 * k + r] * G.rot[3 * k + c];
+      Q[r][c] = v;
+    }
+  const double bs[3] = {G.bsx, G.bsy, G.bsz};
+  for (int dk = -G.mbz; dk <= G.mbz; ++dk)
+    for (int dj = -G.mby; dj <= G.mby; ++dj) {
+      int lo_i = G.mbx + 1, hi_i = -G.mbx - 1;
+      for (int di = -G.mbx; di <= G.mbx; ++di) {
+        bool keep = tot > 4096;
+        if (!keep) {
+          const int o[3] = {di, dj, dk};
+          double lo[3], hi[3];
+          for (int a = 0; a < 3; ++a) {
+            lo[a] = (o[a] - 1) * bs[a] - 1e-6 * bs[a];
+            hi[a] = (o[a] + 1) * bs[a] + 1e-6 * bs[a];
+          }
+          keep = box_min_quad(Q, lo, hi) <= G.rmax2 * (1.0 + 1e-9);
+        }
+        if (keep) {
+          lo_i = std::min(lo_i, di);
+          hi_i = std::max(hi_i, di);
+        }
+      }
+      if (lo_i <= hi_i) rows.push_back(make_int4(lo_i, hi_i, dj, dk));
+    }
+}
+}  // namespace
+
 extern "C" int ss3d_condition(double* res, const int n[3], int nreal, const double xmin3[3], const double d3[3],
                               const ss3d_struct* st, int nst, double nugget, const ss3d_cond_params* cp,
                               const double* rows, int nrows, int nvar, int precision, ss3d_cond_stats* cs,
@@ -1071,6 +1180,9 @@ extern "C" int ss3d_condition(double* res, const int n[3], int nreal, const doub
     for (int c = 0; c < 3; c++) G.rot[3 * r + c] = srot[r][c];
   G.rmax2 = cp->radius[0] * cp->radius[0];
   G.c0 = covariance(mdl, 0.0, 0.0, 0.0);
+  std::vector<int4> srows;
+  super_block_rows(G, srows);
+  G.nrow = (int)srows.size();
   // ---- device work
   cudaStream_t stm = current_stream();
   const long long M = (long long)nx * ny * nz;
@@ -1089,6 +1201,7 @@ extern "C" int ss3d_condition(double* res, const int n[3], int nreal, const doub
          *dgt = nullptr;
   int *dix = nullptr, *diy = nullptr, *diz = nullptr, *dsbs = nullptr, *dnbr = nullptr, *dnnb = nullptr;
   double4* dsxyz = nullptr;
+  int4* dsrow = nullptr;
   unsigned long long* dcnt = nullptr;
   const int chunk = (int)std::min<long long>(M, std::max<long long>(1, ((long long)1 << 30) / (4LL * cp->ndmax + 4)));
   if (e == cudaSuccess) e = bufs.alloc(&ddx, nd);
@@ -1101,6 +1214,7 @@ extern "C" int ss3d_condition(double* res, const int n[3], int nreal, const doub
   if (e == cudaSuccess) e = bufs.alloc(&diz, nd);
   if (e == cudaSuccess) e = bufs.alloc(&dsbs, nsb + 1);
   if (e == cudaSuccess) e = bufs.alloc(&dsxyz, nd);
+  if (e == cudaSuccess) e = bufs.alloc(&dsrow, srows.size());
   if (e == cudaSuccess) e = bufs.alloc(&dnbr, (size_t)chunk * cp->ndmax);
   if (e == cudaSuccess) e = bufs.alloc(&dnnb, chunk);
   if (e == cudaSuccess) e = bufs.alloc(&dcnt, 4);
@@ -1124,6 +1238,7 @@ extern "C" int ss3d_condition(double* res, const int n[3], int nreal, const doub
     sxyz[p] = make_double4(dxs[d], dys[d], dzs[d], (double)d);
   }
   h2d(dsxyz, sxyz.data(), sizeof(double4) * nd);
+  if (G.nrow > 0) h2d(dsrow, srows.data(), sizeof(int4) * G.nrow);
   h2d(dvr, vrt.data(), sizeof(double) * nd);
   h2d(dgt, gtt.data(), sizeof(double) * nd);
   if (e == cudaSuccess) e = cudaMemsetAsync(dcnt, 0, sizeof(unsigned long long) * 4, stm);
@@ -1185,8 +1300,8 @@ extern "C" int ss3d_condition(double* res, const int n[3], int nreal, const doub
     const int count = (int)std::min<long long>(chunk, M - node0);
     auto search = [&](auto cap) {
       constexpr int CAP = decltype(cap)::value, BS = SearchCfg<CAP>::BS;
-      k_cond_search<CAP><<<(unsigned)((count + BS - 1) / BS), BS, 0, stm>>>(G, node0, count, dsxyz, dsbs, dix, diy,
-                                                                          diz, dnbr, dnnb);
+      k_cond_search<CAP><<<(unsigned)((count + BS - 1) / BS), BS, 0, stm>>>(G, node0, count, dsxyz, dsbs, dsrow, dix,
+                                                                          diy, diz, dnbr, dnnb);
     };
     if (cp->ndmax <= 8)
       search(std::integral_constant<int, 8>());
