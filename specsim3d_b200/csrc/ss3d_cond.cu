@@ -860,6 +860,28 @@ void heapsort_idx(const double* key, int* idx, int n) {
   }
 }
 
+// idx (1-based) ordered by key, as heapsort_idx orders it whenever no key
+// occurs more than max_tie times: distinct keys have one sorted order, so a
+// comparison sort with any tie rule gives heapsort's permutation up to the
+// order inside groups of equal keys, which a caller that tolerates max_tie
+// equal keys does not see (the merge of data on one node sums a group, and a
+// sum of two is the same in either order).  Larger groups take the heapsort
+// itself, so the result is always one a caller cannot tell from it.
+void sort_idx(const double* key, int* idx, int n, int max_tie) {
+  std::vector<std::pair<double, int>> kv(n);
+  for (int q = 0; q < n; q++) kv[q] = {key[idx[q] - 1], idx[q]};
+  std::sort(kv.begin(), kv.end());
+  int run = 1;
+  for (int q = 1; q < n; q++) {
+    run = kv[q].first == kv[q - 1].first ? run + 1 : 1;
+    if (run > max_tie) {
+      heapsort_idx(key, idx, n);
+      return;
+    }
+  }
+  for (int q = 0; q < n; q++) idx[q] = kv[q].second;
+}
+
 // inverse standard normal cdf: Acklam's rational approximation refined by one
 // Halley step on erfc (as the reference's gauinv)
 double gauinv(double p0) {
@@ -912,11 +934,40 @@ struct DevBuf {
 }  // namespace
 
 namespace {
+// pinned staging buffer of the conditioning calls of this host thread
+struct CondStage {
+  unsigned char* p = nullptr;
+  size_t bytes = 0;
+  ~CondStage() {
+    if (p) cudaFreeHost(p);
+  }
+};
+thread_local CondStage g_cond_stage;
+
+cudaError_t cond_stage(size_t bytes, unsigned char** out) {
+  CondStage& s = g_cond_stage;
+  if (s.bytes < bytes) {
+    if (s.p) cudaFreeHost(s.p);
+    s.p = nullptr;
+    s.bytes = 0;
+    const size_t want = std::max(bytes, (size_t)1 << 20);
+    cudaError_t e = cudaMallocHost((void**)&s.p, want);
+    if (e != cudaSuccess) {
+      s.p = nullptr;
+      return e;
+    }
+    s.bytes = want;
+  }
+  *out = s.p;
+  return cudaSuccess;
+}
+
 // min of v^T Q v over the box lo <= v <= hi (Q symmetric positive definite),
 // exactly, by its active sets: each coordinate at its lower bound, at its
 // upper bound or free, the free ones solving the reduced stationarity
-// equations; -inf when a reduced system is singular (no pruning then)
-double box_min_quad(const double Q[3][3], const double lo[3], const double hi[3]) {
+// equations; -inf when a reduced system is singular (no pruning then).  Stops
+// at the first value <= stop (the caller only asks whether the min is).
+double box_min_quad(const double Q[3][3], const double lo[3], const double hi[3], double stop) {
   double best = INFINITY;
   for (int code = 0; code < 27; ++code) {
     const int st[3] = {code % 3, (code / 3) % 3, code / 9};   // 0 lower, 1 upper, 2 free
@@ -958,6 +1009,7 @@ double box_min_quad(const double Q[3][3], const double lo[3], const double hi[3]
     for (int a = 0; a < 3; ++a)
       for (int b = 0; b < 3; ++b) q += v[a] * Q[a][b] * v[b];
     best = std::min(best, q);
+    if (best <= stop) break;
   }
   return best;
 }
@@ -997,7 +1049,8 @@ void super_block_rows(const CondGeo& G, std::vector<int4>& rows) {
             lo[a] = (o[a] - 1) * bs[a] - 1e-6 * bs[a];
             hi[a] = (o[a] + 1) * bs[a] + 1e-6 * bs[a];
           }
-          keep = box_min_quad(Q, lo, hi) <= G.rmax2 * (1.0 + 1e-9);
+          const double lim = G.rmax2 * (1.0 + 1e-9);
+          keep = box_min_quad(Q, lo, hi, lim) <= lim;
         }
         if (keep) {
           lo_i = std::min(lo_i, di);
@@ -1064,7 +1117,7 @@ extern "C" int ss3d_condition(double* res, const int n[3], int nreal, const doub
   // ---- merge data of the same node (f90:805-828)
   std::vector<int> ord(nn);
   for (int q = 0; q < nn; q++) ord[q] = q + 1;
-  heapsort_idx(key.data(), ord.data(), nn);
+  sort_idx(key.data(), ord.data(), nn, 2);
   std::vector<int> ix, iy, iz;
   std::vector<double> dval, dwt;
   for (int i = 1; i <= nn;) {
@@ -1094,7 +1147,7 @@ extern "C" int ss3d_condition(double* res, const int n[3], int nreal, const doub
   if (cp->itrans == 1) {
     std::vector<int> idx(nd);
     for (int q = 0; q < nd; q++) idx[q] = q + 1;
-    heapsort_idx(dval.data(), idx.data(), nd);
+    sort_idx(dval.data(), idx.data(), nd, 1);
     double sw = 0.0;
     for (int q = 0; q < nd; q++) sw = sw + dwt[q];
     double cpv = 0.0, oldcp = 0.0;
@@ -1197,51 +1250,65 @@ extern "C" int ss3d_condition(double* res, const int n[3], int nreal, const doub
     e = bufs.alloc(&dres, (size_t)M * nreal);
     if (e == cudaSuccess) e = cudaMemcpyAsync(dres, res, sizeof(double) * M * nreal, cudaMemcpyHostToDevice, stm);
   }
-  double *ddx = nullptr, *ddy = nullptr, *ddz = nullptr, *ddg = nullptr, *dsimd = nullptr, *dvr = nullptr,
-         *dgt = nullptr;
-  int *dix = nullptr, *diy = nullptr, *diz = nullptr, *dsbs = nullptr, *dnbr = nullptr, *dnnb = nullptr;
-  double4* dsxyz = nullptr;
-  int4* dsrow = nullptr;
-  unsigned long long* dcnt = nullptr;
+  // The arrays of the call live in one device allocation; the ones that come
+  // from the host go up in one copy, packed into a pinned staging buffer of
+  // this thread (kept between calls: a call ends with its stream
+  // synchronized, so the buffer is free when the next one starts), which also
+  // takes the counters back.
   const int chunk = (int)std::min<long long>(M, std::max<long long>(1, ((long long)1 << 30) / (4LL * cp->ndmax + 4)));
-  if (e == cudaSuccess) e = bufs.alloc(&ddx, nd);
-  if (e == cudaSuccess) e = bufs.alloc(&ddy, nd);
-  if (e == cudaSuccess) e = bufs.alloc(&ddz, nd);
-  if (e == cudaSuccess) e = bufs.alloc(&ddg, nd);
-  if (e == cudaSuccess) e = bufs.alloc(&dsimd, (size_t)nd * nreal);
-  if (e == cudaSuccess) e = bufs.alloc(&dix, nd);
-  if (e == cudaSuccess) e = bufs.alloc(&diy, nd);
-  if (e == cudaSuccess) e = bufs.alloc(&diz, nd);
-  if (e == cudaSuccess) e = bufs.alloc(&dsbs, nsb + 1);
-  if (e == cudaSuccess) e = bufs.alloc(&dsxyz, nd);
-  if (e == cudaSuccess) e = bufs.alloc(&dsrow, srows.size());
-  if (e == cudaSuccess) e = bufs.alloc(&dnbr, (size_t)chunk * cp->ndmax);
-  if (e == cudaSuccess) e = bufs.alloc(&dnnb, chunk);
-  if (e == cudaSuccess) e = bufs.alloc(&dcnt, 4);
-  if (e == cudaSuccess) e = bufs.alloc(&dvr, nd);
-  if (e == cudaSuccess) e = bufs.alloc(&dgt, nd);
-  auto h2d = [&](void* dst, const void* src, size_t bytes) {
-    if (e == cudaSuccess) e = cudaMemcpyAsync(dst, src, bytes, cudaMemcpyHostToDevice, stm);
+  size_t top = 0;
+  auto place = [&](size_t bytes) {
+    const size_t o = top;
+    top = (top + bytes + 255) & ~(size_t)255;
+    return o;
   };
-  h2d(ddx, dxs.data(), sizeof(double) * nd);
-  h2d(ddy, dys.data(), sizeof(double) * nd);
-  h2d(ddz, dzs.data(), sizeof(double) * nd);
-  h2d(ddg, dg.data(), sizeof(double) * nd);
-  h2d(dix, ix.data(), sizeof(int) * nd);
-  h2d(diy, iy.data(), sizeof(int) * nd);
-  h2d(diz, iz.data(), sizeof(int) * nd);
-  h2d(dsbs, sbstart.data(), sizeof(int) * (nsb + 1));
-  // the data in super-block order, (x, y, z, id) each
-  std::vector<double4> sxyz(nd);
-  for (int p = 0; p < nd; p++) {
-    const int d = sbidx[p] - 1;
-    sxyz[p] = make_double4(dxs[d], dys[d], dzs[d], (double)d);
+  const size_t o_dg = place(sizeof(double) * nd), o_ix = place(sizeof(int) * nd), o_iy = place(sizeof(int) * nd),
+               o_iz = place(sizeof(int) * nd), o_sbs = place(sizeof(int) * (nsb + 1)),
+               o_sxyz = place(sizeof(double4) * nd), o_rows = place(sizeof(int4) * srows.size()),
+               o_vr = place(sizeof(double) * nd), o_gt = place(sizeof(double) * nd), o_mdl = place(sizeof(KModel)),
+               o_cnt = place(sizeof(unsigned long long) * 4);
+  const size_t up_bytes = top;
+  const size_t o_simd = place(sizeof(double) * nd * (size_t)nreal), o_nbr = place(sizeof(int) * (size_t)chunk * cp->ndmax),
+               o_nnb = place(sizeof(int) * (size_t)chunk);
+  unsigned char* stage = nullptr;
+  if (e == cudaSuccess) e = cond_stage(up_bytes, &stage);
+  if (e == cudaSuccess) {
+    auto put = [&](size_t o, const void* src, size_t bytes) {
+      if (bytes) memcpy(stage + o, src, bytes);
+    };
+    put(o_dg, dg.data(), sizeof(double) * nd);
+    put(o_ix, ix.data(), sizeof(int) * nd);
+    put(o_iy, iy.data(), sizeof(int) * nd);
+    put(o_iz, iz.data(), sizeof(int) * nd);
+    put(o_sbs, sbstart.data(), sizeof(int) * (nsb + 1));
+    double4* sx = reinterpret_cast<double4*>(stage + o_sxyz);   // the data in super-block order, (x, y, z, id)
+    for (int p = 0; p < nd; p++) {
+      const int d = sbidx[p] - 1;
+      sx[p] = make_double4(dxs[d], dys[d], dzs[d], (double)d);
+    }
+    put(o_rows, srows.data(), sizeof(int4) * srows.size());
+    put(o_vr, vrt.data(), sizeof(double) * nd);
+    put(o_gt, gtt.data(), sizeof(double) * nd);
+    put(o_mdl, &kmdl, sizeof(KModel));
+    memset(stage + o_cnt, 0, sizeof(unsigned long long) * 4);
   }
-  h2d(dsxyz, sxyz.data(), sizeof(double4) * nd);
-  if (G.nrow > 0) h2d(dsrow, srows.data(), sizeof(int4) * G.nrow);
-  h2d(dvr, vrt.data(), sizeof(double) * nd);
-  h2d(dgt, gtt.data(), sizeof(double) * nd);
-  if (e == cudaSuccess) e = cudaMemsetAsync(dcnt, 0, sizeof(unsigned long long) * 4, stm);
+  unsigned char* arena = nullptr;
+  if (e == cudaSuccess) e = bufs.alloc(&arena, top);
+  if (e == cudaSuccess) e = cudaMemcpyAsync(arena, stage, up_bytes, cudaMemcpyHostToDevice, stm);
+  double* ddg = reinterpret_cast<double*>(arena + o_dg);
+  int* dix = reinterpret_cast<int*>(arena + o_ix);
+  int* diy = reinterpret_cast<int*>(arena + o_iy);
+  int* diz = reinterpret_cast<int*>(arena + o_iz);
+  int* dsbs = reinterpret_cast<int*>(arena + o_sbs);
+  double4* dsxyz = reinterpret_cast<double4*>(arena + o_sxyz);
+  int4* dsrow = reinterpret_cast<int4*>(arena + o_rows);
+  double* dvr = reinterpret_cast<double*>(arena + o_vr);
+  double* dgt = reinterpret_cast<double*>(arena + o_gt);
+  KModel* dmdl = reinterpret_cast<KModel*>(arena + o_mdl);   // the register kernels read the model from global memory
+  unsigned long long* dcnt = reinterpret_cast<unsigned long long*>(arena + o_cnt);
+  double* dsimd = reinterpret_cast<double*>(arena + o_simd);
+  int* dnbr = reinterpret_cast<int*>(arena + o_nbr);
+  int* dnnb = reinterpret_cast<int*>(arena + o_nnb);
   if (e == cudaSuccess) {
     k_gather_simd<<<std::max(1, std::min(1024, (int)(((long long)nd * nreal + 255) / 256))), 256, 0, stm>>>(
         dres, M, dix, diy, diz, nd, nreal, nx, ny, dsimd);
@@ -1293,9 +1360,6 @@ extern "C" int ss3d_condition(double* res, const int n[3], int nreal, const doub
   }
   const int wpb = (int)std::max<size_t>(1, std::min<size_t>(8, (size_t)(96 * 1024) / per));
   if (e == cudaSuccess) e = func_smem(kfn, kfix + per * wpb);
-  KModel* dmdl = nullptr;   // the register kernels read the model from global memory
-  if (e == cudaSuccess) e = bufs.alloc(&dmdl, 1);
-  if (e == cudaSuccess) e = cudaMemcpyAsync(dmdl, &kmdl, sizeof kmdl, cudaMemcpyHostToDevice, stm);
   for (long long node0 = 0; node0 < M && e == cudaSuccess; node0 += chunk) {
     const int count = (int)std::min<long long>(chunk, M - node0);
     auto search = [&](auto cap) {
@@ -1343,14 +1407,17 @@ extern "C" int ss3d_condition(double* res, const int n[3], int nreal, const doub
     e = cudaGetLastError();
   }
   unsigned long long cnt[4] = {0, 0, 0, 0};
-  if (e == cudaSuccess) e = cudaMemcpyAsync(cnt, dcnt, sizeof cnt, cudaMemcpyDeviceToHost, stm);
+  if (e == cudaSuccess) e = cudaMemcpyAsync(stage + o_cnt, dcnt, sizeof cnt, cudaMemcpyDeviceToHost, stm);
   if (e == cudaSuccess && !dev_res)
     e = cudaMemcpyAsync(res, dres, sizeof(double) * M * nreal, cudaMemcpyDeviceToHost, stm);
-  if (e == cudaSuccess) e = cudaStreamSynchronize(stm);
+  // synchronized on every path: the staging buffer is free again on return
+  const cudaError_t es = cudaStreamSynchronize(stm);
+  if (e == cudaSuccess) e = es;
   if (e != cudaSuccess) {
     cudaGetLastError();
     return set_error(SS3D_ECUDA, (std::string("condition: ") + cudaGetErrorString(e)).c_str());
   }
+  memcpy(cnt, stage + o_cnt, sizeof cnt);
   if (cs) {
     cs->nd = nd;
     cs->nmerged = nn - nd;

@@ -121,6 +121,38 @@ def test_search_tilted_ellipsoids(gpu, angles, radii, ndmax, n):
     assert np.max(np.abs(a - b)) <= 1e-9
 
 
+@pytest.mark.parametrize("maxdup,ties", [(2, False), (4, False), (1, True), (3, True)])
+def test_merged_nodes_and_tied_values(gpu, maxdup, ties):
+    """Data sharing nodes (groups of up to maxdup data on one node, merged by
+    weighted average) and, with ties, repeated data values before the normal
+    scores: the merged values, the normal-score table and every statistic
+    equal the oracle's bit for bit, and the fields agree to 1e-9 (the sort of
+    the merge and of the scores must order equal keys as the reference does
+    wherever that order shows)."""
+    rng = np.random.default_rng(17 * maxdup + ties)
+    n = (40, 36, 12)
+    nodes = rng.choice(n[0] * n[1] * n[2], 120, replace=False)
+    i, j, k = np.unravel_index(nodes, (n[0], n[1], n[2]), order="F")
+    reps = rng.integers(1, maxdup + 1, size=120)
+    pts = np.repeat(np.c_[i, j, k].astype(float), reps, axis=0)
+    pts += rng.uniform(-0.3, 0.3, size=pts.shape)           # snapped back to the same node
+    vals = np.exp(rng.normal(size=len(pts)))
+    if ties:
+        vals = np.round(vals, 1)                             # repeated values
+    wts = rng.uniform(0.5, 2.0, size=len(pts))
+    rows = np.c_[pts, vals, wts]
+    sts = [(2, 1.0, 15.0, 10.0, 5.0, 30.0, 0.0, 0.0)]
+    p = _params(iwc=5, tmin=0.0, itrans=1, zlo=0.0, zhi=2 * float(vals.max()), rmax=20.0, rmed=15.0, rvert=6.0,
+                sa1=30.0, ndmax=16)
+    a, b, so, sg, eo, eg = _run_both(gpu, sts, 0.05, n, (0, 0, 0), (1, 1, 1), p, rows, 2, 1357, gpu.FP64)
+    _check_stats(so, sg)
+    if maxdup >= 2:
+        assert so["nmerged"] > 0
+    for key in ("dval", "vrt", "gtt", "dg"):
+        assert np.array_equal(eo[key], eg[key]), key
+    assert np.max(np.abs(a - b)) <= 1e-9
+
+
 def test_condition_device_array(gpu):
     import torch
     rng = np.random.default_rng(8)
