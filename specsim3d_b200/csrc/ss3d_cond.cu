@@ -491,6 +491,75 @@ __global__ void k_cond_krige(CondGeo G, KModel mdl, CovTab ctab, long long node0
   if (threadIdx.x < 4 && bcount[threadIdx.x]) atomicAdd(&counters[threadIdx.x], bcount[threadIdx.x]);
 }
 
+// GSLIB back transform (backtr, powint, gcum), f90:628-697, of one value.
+// mode 0: none; 1: back transform through the normal-score table (gt, vr),
+// itrans 1; 2: add the simple-kriging mean (itrans 0, skmean != 0).  The
+// bracket gt[lo-1] <= y < gt[lo] of the table's bisection is the count of
+// entries <= y; it is found from a bucket index (base[k] = entries <= gt[0] +
+// k w) and corrected by steps along the table, so it is exactly the
+// bisection's whatever bucket the rounding of k picks.
+struct BackTr {
+  const double* vr;
+  const double* gt;
+  const int* base;   // nbucket + 1 counts; NULL: bisection
+  int nt, nbucket, mode, lt, ut;
+  double zmin, zmax, ltp, utp, skmean, g0, inv_w;
+};
+__device__ __forceinline__ double powint_d(double xlow, double xhigh, double ylow, double yhigh, double xval, double pw) {
+  if (xhigh - xlow < 1.0e-20) return 0.5 * (ylow + yhigh);
+  // t^1 = t exactly (the value a correctly rounded pow returns): the linear
+  // interpolation between table entries, the common case, takes no pow
+  const double t = (xval - xlow) / (xhigh - xlow);
+  return ylow + (yhigh - ylow) * (pw == 1.0 ? t : pow(t, pw));
+}
+__device__ __forceinline__ double gcum_d(double x) { return 0.5 * erfc(-x / 1.4142135623730951); }
+__device__ __forceinline__ double backtr_value(const BackTr& B, double y) {
+  const double* gt = B.gt;
+  const double* vr = B.vr;
+  const int nt = B.nt;
+  if (y <= gt[0]) {
+    const double cdflo = gcum_d(gt[0]), cdfbt = gcum_d(y);
+    double z = powint_d(0.0, cdflo, B.zmin, vr[0], cdfbt, B.lt == 2 ? B.ltp : 1.0);
+    if (nt == 1) z = vr[0];
+    return z;
+  }
+  if (y >= gt[nt - 1]) {
+    const double cdfhi = gcum_d(gt[nt - 1]), cdfbt = gcum_d(y);
+    if (B.ut == 2) return powint_d(cdfhi, 1.0, vr[nt - 1], B.zmax, cdfbt, B.utp);
+    if (B.ut == 4) {
+      const double lam = pow(vr[nt - 1], B.utp) * (1.0 - cdfhi);
+      return pow(lam / fmax(1.0 - cdfbt, 1.0e-300), 1.0 / B.utp);
+    }
+    return powint_d(cdfhi, 1.0, vr[nt - 1], B.zmax, cdfbt, 1.0);
+  }
+  int lo;
+  if (B.base) {
+    const double f = (y - B.g0) * B.inv_w;
+    const int kb = f <= 0.0 ? 0 : (f >= (double)B.nbucket ? B.nbucket - 1 : (int)f);
+    int c = __ldg(B.base + kb);
+    while (c > 0 && gt[c - 1] > y) --c;
+    while (c < nt && gt[c] <= y) ++c;
+    lo = c;
+  } else {
+    lo = 1;
+    int hi = nt;
+    while (hi - lo > 1) {
+      const int mid = (lo + hi) / 2;
+      if (gt[mid - 1] <= y) lo = mid;
+      else hi = mid;
+    }
+  }
+  return powint_d(gt[lo - 1], gt[lo], vr[lo - 1], vr[lo], y, 1.0);
+}
+__device__ __forceinline__ double backtr_apply(const BackTr& B, double y) {
+  return B.mode == 1 ? backtr_value(B, y) : (B.mode == 2 ? y + B.skmean : y);
+}
+
+__global__ void k_backtr(double* __restrict__ res, long long tot, BackTr B) {
+  for (long long q = blockIdx.x * (long long)blockDim.x + threadIdx.x; q < tot; q += (long long)gridDim.x * blockDim.x)
+    res[q] = backtr_apply(B, res[q]);
+}
+
 // ---------------------------------------------------------------- kriging, rows in registers
 // The same kriging for ndmax <= 32, with the system of a node held by one warp
 // in registers: lane r owns row r of the covariance matrix (NDT >= ndmax
@@ -640,6 +709,22 @@ __global__ void __launch_bounds__(256, MINB) k_cond_krige_reg(CondGeo G, const K
         else
           Ls[lane * PITCH + lane] = c00;
       }
+      // fewer neighbours than NDT: the system is padded to NDT with identity
+      // rows and columns (and zero right-hand sides), so that every step below
+      // runs for all NDT columns without a test.  A padded column's entries in
+      // the real rows are exact zeros, so every update it makes subtracts an
+      // exact zero: the real entries of L, y and w keep their bits.
+      if (nn < NDT) {
+        for (int e = lane; e < NDT * NDT; e += 32) {
+          const int r = e / NDT, c = e - r * NDT;
+          if (r >= nn || c >= nn) {
+            if constexpr (PREC == 1)
+              A[r * PITCH + c] = r == c ? 1.0 : 0.0;
+            else
+              Ls[r * PITCH + c] = r == c ? 1.0 : 0.0;
+          }
+        }
+      }
     }
     __syncwarp();
     double ridge = 1.0e-10 * G.c0;
@@ -660,32 +745,29 @@ __global__ void __launch_bounds__(256, MINB) k_cond_krige_reg(CondGeo G, const K
       good = true;
 #pragma unroll
       for (int c = 0; c < NDT; ++c) {
-        if (c < nn) {
-          const T piv = __shfl_sync(0xffffffffu, a[c], c);
-          if (!(piv > T(0))) {   // the same value in every lane: a uniform exit
-            good = false;
-            break;
-          }
-          const T inv = rsqrt_nr(piv);
-          const T lrc = a[c] * inv;
-          a[c] = lrc;
-          if (lane == c) myinv = inv;
-          T* cb = colb + (c & 1) * 32;
-          cb[lane] = lrc;
-          __syncwarp();
-          const T yc = __shfl_sync(0xffffffffu, bcur * inv, c);
-          if (lane == c) yv = yc;
-          bcur = fma(-lrc, yc, bcur);
+        const T piv = __shfl_sync(0xffffffffu, a[c], c);
+        // the same value in every lane; a failed factor is recomputed from
+        // A (with a larger ridge), so the steps after a failure only waste work
+        good = good && piv > T(0);
+        const T inv = rsqrt_nr(piv);
+        const T lrc = a[c] * inv;
+        a[c] = lrc;
+        if (lane == c) myinv = inv;
+        T* cb = colb + (c & 1) * 32;
+        cb[lane] = lrc;
+        __syncwarp();
+        const T yc = __shfl_sync(0xffffffffu, bcur * inv, c);
+        if (lane == c) yv = yc;
+        bcur = fma(-lrc, yc, bcur);
 #pragma unroll
-          for (int k0 = (c + 1) / KV * KV; k0 < NDT; k0 += KV) {
-            // the column 16 bytes at a time (every lane reads the same words:
-            // one wavefront per load); elements up to c are loaded, not used
-            T cv[KV];
-            *reinterpret_cast<uint4*>(cv) = *reinterpret_cast<const uint4*>(cb + k0);
+        for (int k0 = (c + 1) / KV * KV; k0 < NDT; k0 += KV) {
+          // the column 16 bytes at a time (every lane reads the same words:
+          // one wavefront per load); elements up to c are loaded, not used
+          T cv[KV];
+          *reinterpret_cast<uint4*>(cv) = *reinterpret_cast<const uint4*>(cb + k0);
 #pragma unroll
-            for (int u = 0; u < KV; ++u)
-              if (k0 + u > c) a[k0 + u] = fma(-lrc, cv[u], a[k0 + u]);
-          }
+          for (int u = 0; u < KV; ++u)
+            if (k0 + u > c) a[k0 + u] = fma(-lrc, cv[u], a[k0 + u]);
         }
       }
       if (good) break;
@@ -706,13 +788,11 @@ __global__ void __launch_bounds__(256, MINB) k_cond_krige_reg(CondGeo G, const K
     T acc = yv, w = T(0);
 #pragma unroll
     for (int r = NDT - 1; r >= 0; --r) {
-      if (r < nn) {
-        const T wr = __shfl_sync(0xffffffffu, acc * myinv, r);
-        if (lane == r) w = wr;
-        if (lane < r) acc = fma(-Ls[r * PITCH + lane], wr, acc);
-      }
+      const T wr = __shfl_sync(0xffffffffu, acc * myinv, r);
+      if (lane == r) w = wr;
+      if (lane < r) acc = fma(-Ls[r * PITCH + lane], wr, acc);
     }
-    if (act) wsm[lane] = (double)w;
+    if (lane < NDT) wsm[lane] = (double)w;   // 0 in padded rows
     __syncwarp();
     if constexpr (PREC == 1) {
       // one refinement: residual b - (A + ridge I) w in FP64, then
@@ -720,25 +800,27 @@ __global__ void __launch_bounds__(256, MINB) k_cond_krige_reg(CondGeo G, const K
       double rres = 0.0;
       if (act) {
         rres = b - ridge * wsm[lane];
-        for (int c = 0; c < nn; ++c) rres -= As[lane * PITCH + c] * wsm[c];
+        // the padded columns add exact zeros (A and w are 0 there)
+#pragma unroll
+        for (int c0 = 0; c0 < NDT; c0 += 2) {
+          const double2 wv = *reinterpret_cast<const double2*>(wsm + c0);
+          rres -= As[lane * PITCH + c0] * wv.x;
+          rres -= As[lane * PITCH + c0 + 1] * wv.y;
+        }
       }
       T dcur = (T)rres, dy = T(0);
 #pragma unroll
       for (int c = 0; c < NDT; ++c) {
-        if (c < nn) {
-          const T yc = __shfl_sync(0xffffffffu, dcur * myinv, c);
-          if (lane == c) dy = yc;
-          dcur = fma(-a[c], yc, dcur);
-        }
+        const T yc = __shfl_sync(0xffffffffu, dcur * myinv, c);
+        if (lane == c) dy = yc;
+        dcur = fma(-a[c], yc, dcur);
       }
       T acc2 = dy, d = T(0);
 #pragma unroll
       for (int r = NDT - 1; r >= 0; --r) {
-        if (r < nn) {
-          const T wr = __shfl_sync(0xffffffffu, acc2 * myinv, r);
-          if (lane == r) d = wr;
-          if (lane < r) acc2 = fma(-Ls[r * PITCH + lane], wr, acc2);
-        }
+        const T wr = __shfl_sync(0xffffffffu, acc2 * myinv, r);
+        if (lane == r) d = wr;
+        if (lane < r) acc2 = fma(-Ls[r * PITCH + lane], wr, acc2);
       }
       __syncwarp();
       if (act) wsm[lane] += (double)d;
@@ -775,54 +857,6 @@ __global__ void k_gather_simd(const double* __restrict__ res, long long M, const
     const int l = (int)(q % nreal), d = (int)(q / nreal);
     simd[q] = res[(ix[d] - 1) + (long long)nx * ((iy[d] - 1) + (long long)ny * (iz[d] - 1)) + M * l];
   }
-}
-
-// GSLIB back transform (backtr, powint, gcum), f90:628-697
-__device__ __forceinline__ double powint_d(double xlow, double xhigh, double ylow, double yhigh, double xval, double pw) {
-  if (xhigh - xlow < 1.0e-20) return 0.5 * (ylow + yhigh);
-  // t^1 = t exactly (the value a correctly rounded pow returns): the linear
-  // interpolation between table entries, the common case, takes no pow
-  const double t = (xval - xlow) / (xhigh - xlow);
-  return ylow + (yhigh - ylow) * (pw == 1.0 ? t : pow(t, pw));
-}
-__device__ __forceinline__ double gcum_d(double x) { return 0.5 * erfc(-x / 1.4142135623730951); }
-
-__global__ void k_backtr(double* __restrict__ res, long long tot, int nt, const double* __restrict__ vr,
-                         const double* __restrict__ gt, double zmin, double zmax, int lt, double ltp, int ut,
-                         double utp) {
-  for (long long q = blockIdx.x * (long long)blockDim.x + threadIdx.x; q < tot; q += (long long)gridDim.x * blockDim.x) {
-    const double y = res[q];
-    double z;
-    if (y <= gt[0]) {
-      const double cdflo = gcum_d(gt[0]), cdfbt = gcum_d(y);
-      z = powint_d(0.0, cdflo, zmin, vr[0], cdfbt, lt == 2 ? ltp : 1.0);
-      if (nt == 1) z = vr[0];
-    } else if (y >= gt[nt - 1]) {
-      const double cdfhi = gcum_d(gt[nt - 1]), cdfbt = gcum_d(y);
-      if (ut == 2) {
-        z = powint_d(cdfhi, 1.0, vr[nt - 1], zmax, cdfbt, utp);
-      } else if (ut == 4) {
-        const double lam = pow(vr[nt - 1], utp) * (1.0 - cdfhi);
-        z = pow(lam / fmax(1.0 - cdfbt, 1.0e-300), 1.0 / utp);
-      } else {
-        z = powint_d(cdfhi, 1.0, vr[nt - 1], zmax, cdfbt, 1.0);
-      }
-    } else {
-      int lo = 1, hi = nt;
-      while (hi - lo > 1) {
-        const int mid = (lo + hi) / 2;
-        if (gt[mid - 1] <= y) lo = mid;
-        else hi = mid;
-      }
-      z = powint_d(gt[lo - 1], gt[hi - 1], vr[lo - 1], vr[hi - 1], y, 1.0);
-    }
-    res[q] = z;
-  }
-}
-
-__global__ void k_add(double* __restrict__ res, long long tot, double v) {
-  for (long long q = blockIdx.x * (long long)blockDim.x + threadIdx.x; q < tot; q += (long long)gridDim.x * blockDim.x)
-    res[q] += v;
 }
 
 }  // namespace ss3d
@@ -1267,6 +1301,10 @@ extern "C" int ss3d_condition(double* res, const int n[3], int nreal, const doub
                o_sxyz = place(sizeof(double4) * nd), o_rows = place(sizeof(int4) * srows.size()),
                o_vr = place(sizeof(double) * nd), o_gt = place(sizeof(double) * nd), o_mdl = place(sizeof(KModel)),
                o_cnt = place(sizeof(unsigned long long) * 4);
+  // bucket index of the normal-score table for the back transform: one
+  // bucket per entry over [gt[0], gt[nt-1]]
+  const int nbucket = (cp->itrans == 1 && nt >= 2 && gtt[nt - 1] > gtt[0]) ? nt : 0;
+  const size_t o_base = place(sizeof(int) * (size_t)(nbucket + 1));
   const size_t up_bytes = top;
   const size_t o_simd = place(sizeof(double) * nd * (size_t)nreal), o_nbr = place(sizeof(int) * (size_t)chunk * cp->ndmax),
                o_nnb = place(sizeof(int) * (size_t)chunk);
@@ -1291,6 +1329,12 @@ extern "C" int ss3d_condition(double* res, const int n[3], int nreal, const doub
     put(o_gt, gtt.data(), sizeof(double) * nd);
     put(o_mdl, &kmdl, sizeof(KModel));
     memset(stage + o_cnt, 0, sizeof(unsigned long long) * 4);
+    if (nbucket) {
+      int* base = reinterpret_cast<int*>(stage + o_base);
+      const double w = (gtt[nt - 1] - gtt[0]) / nbucket;
+      for (int kb = 0; kb <= nbucket; kb++)
+        base[kb] = (int)(std::upper_bound(gtt.begin(), gtt.begin() + nt, gtt[0] + kb * w) - gtt.begin());
+    }
   }
   unsigned char* arena = nullptr;
   if (e == cudaSuccess) e = bufs.alloc(&arena, top);
@@ -1309,6 +1353,22 @@ extern "C" int ss3d_condition(double* res, const int n[3], int nreal, const doub
   double* dsimd = reinterpret_cast<double*>(arena + o_simd);
   int* dnbr = reinterpret_cast<int*>(arena + o_nbr);
   int* dnnb = reinterpret_cast<int*>(arena + o_nnb);
+  BackTr bt{};
+  bt.mode = cp->itrans == 1 ? 1 : (cp->skmean != 0.0 ? 2 : 0);
+  bt.vr = dvr;
+  bt.gt = dgt;
+  bt.base = nbucket ? reinterpret_cast<const int*>(arena + o_base) : nullptr;
+  bt.nt = nt;
+  bt.nbucket = nbucket;
+  bt.lt = cp->ltail;
+  bt.ut = cp->utail;
+  bt.zmin = cp->zmin;
+  bt.zmax = cp->zmax;
+  bt.ltp = cp->ltpar;
+  bt.utp = cp->utpar;
+  bt.skmean = cp->skmean;
+  bt.g0 = nbucket ? gtt[0] : 0.0;
+  bt.inv_w = nbucket ? nbucket / (gtt[nt - 1] - gtt[0]) : 0.0;
   if (e == cudaSuccess) {
     k_gather_simd<<<std::max(1, std::min(1024, (int)(((long long)nd * nreal + 255) / 256))), 256, 0, stm>>>(
         dres, M, dix, diy, diz, nd, nreal, nx, ny, dsimd);
@@ -1396,13 +1456,8 @@ extern "C" int ss3d_condition(double* res, const int n[3], int nreal, const doub
     if (e == cudaSuccess) e = cudaGetLastError();
   }
   const long long tot = M * nreal;
-  if (e == cudaSuccess && cp->itrans == 1) {
-    k_backtr<<<(int)std::min<long long>(148 * 32, (tot + 255) / 256), 256, 0, stm>>>(
-        dres, tot, nt, dvr, dgt, cp->zmin, cp->zmax, cp->ltail, cp->ltpar, cp->utail, cp->utpar);
-    ++g_launch_count;
-    e = cudaGetLastError();
-  } else if (e == cudaSuccess && cp->skmean != 0.0) {
-    k_add<<<(int)std::min<long long>(148 * 32, (tot + 255) / 256), 256, 0, stm>>>(dres, tot, cp->skmean);
+  if (e == cudaSuccess && bt.mode) {
+    k_backtr<<<(int)std::min<long long>(148 * 32, (tot + 255) / 256), 256, 0, stm>>>(dres, tot, bt);
     ++g_launch_count;
     e = cudaGetLastError();
   }
