@@ -212,6 +212,8 @@ __global__ void __launch_bounds__(SearchCfg<CAP>::BS) k_cond_search(CondGeo G, l
   int nn = 0;
   const int ndmax = G.ndmax;
   double worst = 0.0;   // cds[nn - 1][t] once the list is full
+  const double r0 = G.rot[0], r1 = G.rot[1], r2 = G.rot[2], r3 = G.rot[3], r4 = G.rot[4], r5 = G.rot[5],
+               r6 = G.rot[6], r7 = G.rot[7], r8 = G.rot[8], rmax2 = G.rmax2;
   for (int o = 0; o < G.nrow; ++o) {
     const int4 rw = __ldg(rows + o);
     const int jb = by + rw.z, kb = bz + rw.w;
@@ -223,12 +225,12 @@ __global__ void __launch_bounds__(SearchCfg<CAP>::BS) k_cond_search(CondGeo G, l
       const double2 a = __ldg(reinterpret_cast<const double2*>(sxyz + p - 1));
       const double2 b = __ldg(reinterpret_cast<const double2*>(sxyz + p - 1) + 1);
       const double hx = __dsub_rn(a.x, x), hy = __dsub_rn(a.y, y), hz = __dsub_rn(b.x, z);
-      const double rx = __dadd_rn(__dadd_rn(__dmul_rn(G.rot[0], hx), __dmul_rn(G.rot[1], hy)), __dmul_rn(G.rot[2], hz));
-      const double ry = __dadd_rn(__dadd_rn(__dmul_rn(G.rot[3], hx), __dmul_rn(G.rot[4], hy)), __dmul_rn(G.rot[5], hz));
-      const double rz = __dadd_rn(__dadd_rn(__dmul_rn(G.rot[6], hx), __dmul_rn(G.rot[7], hy)), __dmul_rn(G.rot[8], hz));
+      const double rx = __dadd_rn(__dadd_rn(__dmul_rn(r0, hx), __dmul_rn(r1, hy)), __dmul_rn(r2, hz));
+      const double ry = __dadd_rn(__dadd_rn(__dmul_rn(r3, hx), __dmul_rn(r4, hy)), __dmul_rn(r5, hz));
+      const double rz = __dadd_rn(__dadd_rn(__dmul_rn(r6, hx), __dmul_rn(r7, hy)), __dmul_rn(r8, hz));
       const double s2 = __dadd_rn(__dadd_rn(__dmul_rn(rx, rx), __dmul_rn(ry, ry)), __dmul_rn(rz, rz));
-      if (s2 > G.rmax2) continue;
-      const double d2 = __ddiv_rn(s2, G.rmax2);
+      if (s2 > rmax2) continue;
+      const double d2 = __ddiv_rn(s2, rmax2);
       int m;
       if (nn < ndmax) {
         nn = nn + 1;
@@ -902,18 +904,42 @@ void heapsort_idx(const double* key, int* idx, int n) {
 // sum of two is the same in either order).  Larger groups take the heapsort
 // itself, so the result is always one a caller cannot tell from it.
 void sort_idx(const double* key, int* idx, int n, int max_tie) {
-  std::vector<std::pair<double, int>> kv(n);
-  for (int q = 0; q < n; q++) kv[q] = {key[idx[q] - 1], idx[q]};
-  std::sort(kv.begin(), kv.end());
+  // LSD radix sort, 8 bits a pass, on the doubles' bits mapped to an order-
+  // preserving unsigned key (sign bit set for positives, all bits flipped for
+  // negatives; -0 is taken as +0, which the comparisons of heapsort equal)
+  std::vector<uint64_t> k(n), k2(n);
+  std::vector<int> v(n), v2(n);
+  for (int q = 0; q < n; q++) {
+    uint64_t b;
+    std::memcpy(&b, &key[idx[q] - 1], 8);
+    if (b == 0x8000000000000000ull) b = 0;
+    k[q] = (b >> 63) ? ~b : (b | 0x8000000000000000ull);
+    v[q] = idx[q];
+  }
+  uint64_t diff = 0;   // bits that differ between keys: passes over constant bytes are skipped
+  for (int q = 1; q < n; q++) diff |= k[q] ^ k[0];
+  for (int sh = 0; sh < 64; sh += 8) {
+    if (!((diff >> sh) & 0xff)) continue;
+    int cnt[257] = {0};
+    for (int q = 0; q < n; q++) cnt[((k[q] >> sh) & 0xff) + 1]++;
+    for (int c = 0; c < 256; c++) cnt[c + 1] += cnt[c];
+    for (int q = 0; q < n; q++) {
+      const int d = cnt[(k[q] >> sh) & 0xff]++;
+      k2[d] = k[q];
+      v2[d] = v[q];
+    }
+    k.swap(k2);
+    v.swap(v2);
+  }
   int run = 1;
   for (int q = 1; q < n; q++) {
-    run = kv[q].first == kv[q - 1].first ? run + 1 : 1;
+    run = k[q] == k[q - 1] ? run + 1 : 1;
     if (run > max_tie) {
       heapsort_idx(key, idx, n);
       return;
     }
   }
-  for (int q = 0; q < n; q++) idx[q] = kv[q].second;
+  for (int q = 0; q < n; q++) idx[q] = v[q];
 }
 
 // inverse standard normal cdf: Acklam's rational approximation refined by one
@@ -1126,6 +1152,7 @@ extern "C" int ss3d_condition(double* res, const int n[3], int nreal, const doub
   std::vector<double> raw;
   std::vector<double> key;
   raw.reserve((size_t)nrows * 5);
+  key.reserve((size_t)nrows);
   int nn = 0, nout = 0;
   for (int q = 0; q < nrows; q++) {
     const double* row = rows + (size_t)q * nvar;
@@ -1154,6 +1181,8 @@ extern "C" int ss3d_condition(double* res, const int n[3], int nreal, const doub
   sort_idx(key.data(), ord.data(), nn, 2);
   std::vector<int> ix, iy, iz;
   std::vector<double> dval, dwt;
+  for (auto* vi : {&ix, &iy, &iz}) vi->reserve(nn);
+  for (auto* vd : {&dval, &dwt}) vd->reserve(nn);
   for (int i = 1; i <= nn;) {
     int j = i;
     while (j < nn && key[ord[j] - 1] == key[ord[i - 1] - 1]) j++;
