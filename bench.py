@@ -54,6 +54,9 @@ def parse():
                     help="profiling case, no timing: realize (the bench grid, 1 realization, three FP32 calls), "
                          "cond (the conditional workload, one FP64 and one FP32 conditioning call), vario (one FP64 "
                          "256^3 realization, directions x, y, z, lags 1..100), spectrum (one 512^3 spectrum build)")
+    ap.add_argument("--tile-variant", action="append", default=[], metavar="PASS=V",
+                    help="realize profiling case: after the autotuner, run pass PASS (middle, synthesis, rows) of "
+                         "the bench grid with FP32 tile variant V instead (may be repeated)")
     return ap.parse_args()
 
 
@@ -761,7 +764,7 @@ def run_ours(args):
     return 0
 
 
-def run_profile_case(kind="realize"):
+def run_profile_case(kind="realize", variants=()):
     """Small cases for ncu.  realize: the bench grid with one realization per
     call (about 1.5 GB on the device), tile variants autotuned as in the bench,
     then three FP32 calls into a device buffer inside the NVTX range "profile".
@@ -769,7 +772,9 @@ def run_profile_case(kind="realize"):
     about 0.2 GB), one FP64 then one FP32 conditioning call.  vario: one FP64
     realization of the bench grid (134 MB) and its variograms along x, y, z,
     lags 1..100.  spectrum: one spectrum build of the bench model (512^3
-    periodic grid, about 3 GB of temporaries)."""
+    periodic grid, about 3 GB of temporaries).  variants: (pass, variant)
+    pairs set after the autotuner in the realize case (the other tile variants
+    of a pass give the same bits; this profiles one of them)."""
     import torch
     import specsim3d_b200 as ss
     n = WL["n"]
@@ -807,6 +812,15 @@ def run_profile_case(kind="realize"):
         return 0
     sp = ss.Spectrum(WL["structs"], WL["nugget"], WL["d"], n, WL["ipad"])
     ss.autotune(sp, WL["igauss"], ss.FP32, 1)
+    from specsim3d_b200 import _lib
+    kinds = {"middle": 0, "synthesis": 1, "rows": 2}
+    for pas, v in variants:
+        # the log2 length a pass's variant is registered under: middle / synthesis
+        # passes of npy / npz points, the row pass of npx / 2
+        lg = {0: int(sp.np[1]).bit_length() - 1, 1: int(sp.np[2]).bit_length() - 1,
+              2: int(sp.np[0]).bit_length() - 2}[kinds[pas]]
+        if _lib.lib().ss3d_set_variant(kinds[pas], ss.FP32, lg, int(v)) != 0:
+            raise SystemExit(f"invalid tile variant {pas}={v}")
     out = torch.empty((1, n[2], n[1], n[0]), dtype=torch.float32, device="cuda")
     torch.cuda.synchronize()
     torch.cuda.nvtx.range_push("profile")
@@ -821,7 +835,13 @@ def run_profile_case(kind="realize"):
 def main():
     args = parse()
     if args.profile_case:
-        return run_profile_case(args.profile_case)
+        pairs = []
+        for tv in args.tile_variant:
+            pas, _, v = tv.partition("=")
+            if pas not in ("middle", "synthesis", "rows") or not v.isdigit():
+                raise SystemExit(f"--tile-variant wants PASS=V with PASS middle, synthesis or rows, got {tv!r}")
+            pairs.append((pas, int(v)))
+        return run_profile_case(args.profile_case, pairs)
     if args.impl == "reference":
         return run_reference(args)
     return run_ours(args)

@@ -538,7 +538,7 @@ __device__ __forceinline__ double backtr_value(const BackTr& B, double y) {
   if (B.base) {
     const double f = (y - B.g0) * B.inv_w;
     const int kb = f <= 0.0 ? 0 : (f >= (double)B.nbucket ? B.nbucket - 1 : (int)f);
-    int c = __ldg(B.base + kb);
+    int c = B.base[kb];   // a generic load: the table may be in shared memory
     while (c > 0 && gt[c - 1] > y) --c;
     while (c < nt && gt[c] <= y) ++c;
     lo = c;
@@ -560,6 +560,31 @@ __device__ __forceinline__ double backtr_apply(const BackTr& B, double y) {
 __global__ void k_backtr(double* __restrict__ res, long long tot, BackTr B) {
   for (long long q = blockIdx.x * (long long)blockDim.x + threadIdx.x; q < tot; q += (long long)gridDim.x * blockDim.x)
     res[q] = backtr_apply(B, res[q]);
+}
+// the same with the table (gt, vr and the bucket index) copied into the
+// shared memory of each block of a resident grid: the lookups of one value
+// are dependent loads, which shared memory serves with far less latency
+__host__ __device__ inline size_t backtr_smem_bytes(int nt, int nbucket) {
+  return (size_t)nt * 16 + (size_t)(nbucket + 1) * 4;
+}
+__global__ void __launch_bounds__(256) k_backtr_smem(double* __restrict__ res, long long tot, BackTr B) {
+  extern __shared__ __align__(16) unsigned char smb[];
+  double* sgt = reinterpret_cast<double*>(smb);
+  double* svr = sgt + B.nt;
+  int* sbase = reinterpret_cast<int*>(svr + B.nt);
+  for (int q = threadIdx.x; q < B.nt; q += blockDim.x) {
+    sgt[q] = B.gt[q];
+    svr[q] = B.vr[q];
+  }
+  if (B.base)
+    for (int q = threadIdx.x; q <= B.nbucket; q += blockDim.x) sbase[q] = B.base[q];
+  __syncthreads();
+  BackTr S = B;
+  S.gt = sgt;
+  S.vr = svr;
+  S.base = B.base ? sbase : nullptr;
+  for (long long q = blockIdx.x * (long long)blockDim.x + threadIdx.x; q < tot; q += (long long)gridDim.x * blockDim.x)
+    res[q] = backtr_apply(S, res[q]);
 }
 
 // ---------------------------------------------------------------- kriging, rows in registers
@@ -1486,9 +1511,21 @@ extern "C" int ss3d_condition(double* res, const int n[3], int nreal, const doub
   }
   const long long tot = M * nreal;
   if (e == cudaSuccess && bt.mode) {
-    k_backtr<<<(int)std::min<long long>(148 * 32, (tot + 255) / 256), 256, 0, stm>>>(dres, tot, bt);
-    ++g_launch_count;
-    e = cudaGetLastError();
+    const size_t tb = backtr_smem_bytes(nt, nbucket);
+    if (bt.mode == 1 && tb <= (64u << 10)) {   // 4 blocks of 256 threads per SM
+      e = func_smem((const void*)k_backtr_smem, tb);
+      if (e == cudaSuccess) {
+        int nsm = 148;
+        cudaDeviceGetAttribute(&nsm, cudaDevAttrMultiProcessorCount, cur_dev);
+        k_backtr_smem<<<(int)std::min<long long>(4LL * nsm, (tot + 255) / 256), 256, tb, stm>>>(dres, tot, bt);
+        ++g_launch_count;
+        e = cudaGetLastError();
+      }
+    } else {
+      k_backtr<<<(int)std::min<long long>(148 * 32, (tot + 255) / 256), 256, 0, stm>>>(dres, tot, bt);
+      ++g_launch_count;
+      e = cudaGetLastError();
+    }
   }
   unsigned long long cnt[4] = {0, 0, 0, 0};
   if (e == cudaSuccess) e = cudaMemcpyAsync(stage + o_cnt, dcnt, sizeof cnt, cudaMemcpyDeviceToHost, stm);
