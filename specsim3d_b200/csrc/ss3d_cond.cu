@@ -1019,31 +1019,17 @@ struct DevBuf {
 }  // namespace
 
 namespace {
-// pinned staging buffer of the conditioning calls of this host thread
-struct CondStage {
-  unsigned char* p = nullptr;
-  size_t bytes = 0;
-  ~CondStage() {
-    if (p) cudaFreeHost(p);
-  }
-};
-thread_local CondStage g_cond_stage;
+// Staging buffer of the conditioning calls of this host thread, in pageable
+// memory.  A page-locked allocation would serialise the work of every stream
+// of the device (an implicit synchronisation of cudaMallocHost), which in a
+// serving loop stalls the requests of the other slots behind a running
+// kriging call; a copy from pageable memory is staged by the driver without
+// such a synchronisation.
+thread_local std::vector<unsigned char> g_cond_stage;
 
 cudaError_t cond_stage(size_t bytes, unsigned char** out) {
-  CondStage& s = g_cond_stage;
-  if (s.bytes < bytes) {
-    if (s.p) cudaFreeHost(s.p);
-    s.p = nullptr;
-    s.bytes = 0;
-    const size_t want = std::max(bytes, (size_t)1 << 20);
-    cudaError_t e = cudaMallocHost((void**)&s.p, want);
-    if (e != cudaSuccess) {
-      s.p = nullptr;
-      return e;
-    }
-    s.bytes = want;
-  }
-  *out = s.p;
+  if (g_cond_stage.size() < bytes) g_cond_stage.resize(std::max(bytes, (size_t)1 << 20));
+  *out = g_cond_stage.data();
   return cudaSuccess;
 }
 
@@ -1339,10 +1325,10 @@ extern "C" int ss3d_condition(double* res, const int n[3], int nreal, const doub
     if (e == cudaSuccess) e = cudaMemcpyAsync(dres, res, sizeof(double) * M * nreal, cudaMemcpyHostToDevice, stm);
   }
   // The arrays of the call live in one device allocation; the ones that come
-  // from the host go up in one copy, packed into a pinned staging buffer of
-  // this thread (kept between calls: a call ends with its stream
-  // synchronized, so the buffer is free when the next one starts), which also
-  // takes the counters back.
+  // from the host go up in one copy, packed into a staging buffer of this
+  // thread (kept between calls: a call ends with its stream synchronized, so
+  // the buffer is free when the next one starts), which also takes the
+  // counters back.
   const int chunk = (int)std::min<long long>(M, std::max<long long>(1, ((long long)1 << 30) / (4LL * cp->ndmax + 4)));
   size_t top = 0;
   auto place = [&](size_t bytes) {
