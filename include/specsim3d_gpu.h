@@ -167,13 +167,26 @@ int ss3d_realize_noalloc(const ss3d_spectrum *sp, int iseed, int64_t r_first, in
  * variants picked for {middle pass, synthesis pass, row pass}. */
 int ss3d_autotune(const ss3d_spectrum *sp, int igauss, int precision, int nreal, int chosen[3]);
 
+/* Loads every kernel of the library on the current device now.  CUDA loads a
+ * kernel when it is first launched by default, and loading one may
+ * synchronise the device: a process that runs other work beside the library
+ * (a server, several threads) can take the loads up front.  ss3d_server_create
+ * calls it.  No counterpart in the reference. */
+int ss3d_preload_kernels(void);
+
 /* Explicit variant of kernel kind 0 middle pass, 1 synthesis pass, 2 row
  * pass, for one precision and transform length 2^logn: 0..3 one line per
  * thread; for the FP32 column passes (kinds 0, 1) also 4..7, two adjacent
- * lines per thread on the packed FP32 instructions; for the row pass also 4,
- * each row held in the registers of one warp (row lengths 8..512 in FP32,
- * 8..256 in FP64; other lengths run variant 0).  Every variant computes the
- * same values; they differ in tile shape and instruction form only. */
+ * lines per thread on the packed FP32 instructions; for the FP32 middle pass
+ * also 8 and 9, tiles brought into shared memory by bulk tensor copies (one
+ * and two lines per thread); for the row pass also 4, each row held in the
+ * registers of one warp (row lengths 8..512 in FP32, 8..256 in FP64; other
+ * lengths run variant 0), and in FP32 5, the middle and row passes of a plane
+ * in one thread-block cluster (3-D grids, float output without statistics,
+ * y lengths 64..512, row lengths 128..512; elsewhere variant 4), and 6, two
+ * rows per lane on the packed FP32 instructions (row lengths 8..256;
+ * elsewhere variant 4).  Every variant computes the same values; they differ
+ * in tile shape and instruction form only. */
 int ss3d_set_variant(int kind, int precision, int logn, int variant);
 
 /* ---------------------------------------------------------------- batched form */

@@ -80,6 +80,12 @@ def profile_read():
     return {name: (float(ms[q]), int(ln[q])) for q, name in enumerate(STAGES)}, int(tot.value)
 
 
+def preload_kernels():
+    """Load every kernel of the library on the current device now (CUDA loads
+    a kernel on its first launch, and a load may synchronise the device)."""
+    L.check(L.lib().ss3d_preload_kernels())
+
+
 def autotune(spectrum, igauss=1, precision=FP32, nreal=2):
     """Pick the fastest tile variant of each realization kernel for this grid (kept for the process)."""
     ch = np.zeros(3, dtype=np.int32)

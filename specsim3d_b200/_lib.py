@@ -24,6 +24,7 @@ EXPORTS = (
     "ss3d_realize", "ss3d_debug_states", "ss3d_debug_coefficients", "ss3d_row_state",
     "ss3d_vario", "ss3d_condition", "ss3d_fft3d",
     "ss3d_set_stream", "ss3d_last_error", "ss3d_version", "ss3d_profile", "ss3d_profile_read", "ss3d_autotune", "ss3d_set_variant",
+    "ss3d_preload_kernels",
     "ss3d_realize_workspace_bytes", "ss3d_release_workspace", "ss3d_trim_pool",
     "ss3d_batch_create", "ss3d_batch_run", "ss3d_batch_autotune", "ss3d_batch_info", "ss3d_batch_time",
     "ss3d_batch_schedule", "ss3d_batch_set_schedule", "ss3d_batch_split", "ss3d_batch_set_split", "ss3d_batch_free",
@@ -140,6 +141,7 @@ def lib():
         "ss3d_profile_read": (I, [P, P, P]),
         "ss3d_autotune": (I, [P, I, I, I, P]),
         "ss3d_set_variant": (I, [I, I, I, I]),
+        "ss3d_preload_kernels": (I, []),
         "ss3d_realize_workspace_bytes": (I64, [P, I, I, I]),
         "ss3d_release_workspace": (I, []),
         "ss3d_trim_pool": (I, []),

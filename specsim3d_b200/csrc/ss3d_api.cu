@@ -1,6 +1,7 @@
 // ss3d_api.cu -- host side of the C ABI declared in include/specsim3d_gpu.h:
 // model setup (setrot, grid sizing), device context (twiddle and jump-ahead
 // tables), spectrum handles, realization batching with host/device output.
+#include <cuda.h>
 #include <cuda_runtime.h>
 
 #include <algorithm>
@@ -111,6 +112,51 @@ cudaError_t ss3d::func_smem(const void* kernel, size_t bytes) {
   e = cudaFuncSetAttribute(kernel, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)bytes);
   if (e == cudaSuccess) have = bytes;
   return e;
+}
+
+// ---------------------------------------------------------------- kernel loading
+// CUDA loads a kernel when it is first launched (lazy module loading, the
+// default), and loading one may synchronise the context: in a serving loop
+// the first request that needs a kernel not yet loaded would stall the work
+// of every stream behind whatever runs.  ss3d_preload_kernels loads every
+// kernel of the library's modules on the current device at once, through the
+// driver's module enumeration (entry points fetched at run time).
+namespace {
+template <typename F> F driver_fn(const char* name) {
+  void* p = nullptr;
+  cudaDriverEntryPointQueryResult q;
+  if (cudaGetDriverEntryPoint(name, &p, cudaEnableDefault, &q) != cudaSuccess || q != cudaDriverEntryPointSuccess)
+    p = nullptr;
+  cudaGetLastError();
+  return reinterpret_cast<F>(p);
+}
+}  // namespace
+
+extern "C" int ss3d_preload_kernels(void) {
+  using GetModule = CUresult (*)(CUmodule*, CUfunction);
+  using Count = CUresult (*)(unsigned int*, CUmodule);
+  using Enumerate = CUresult (*)(CUfunction*, unsigned int, CUmodule);
+  using Load = CUresult (*)(CUfunction);
+  static const GetModule get_module = driver_fn<GetModule>("cuFuncGetModule");
+  static const Count count = driver_fn<Count>("cuModuleGetFunctionCount");
+  static const Enumerate enumerate = driver_fn<Enumerate>("cuModuleEnumerateFunctions");
+  static const Load load = driver_fn<Load>("cuFuncLoad");
+  if (!get_module || !count || !enumerate || !load)
+    return fail(SS3D_ECUDA, "the CUDA driver does not offer module enumeration and kernel loading");
+  for (const void* anchor : {module_anchor_fft(), module_anchor_cond(), module_anchor_vario(), module_anchor_batch()}) {
+    cudaFunction_t f = nullptr;
+    CK(cudaGetFuncBySymbol(&f, anchor));
+    CUmodule mod = nullptr;
+    unsigned int n = 0;
+    if (get_module(&mod, reinterpret_cast<CUfunction>(f)) != CUDA_SUCCESS || count(&n, mod) != CUDA_SUCCESS)
+      return fail(SS3D_ECUDA, "could not enumerate the kernels of a library module");
+    std::vector<CUfunction> fs(n);
+    if (n > 0 && enumerate(fs.data(), n, mod) != CUDA_SUCCESS)
+      return fail(SS3D_ECUDA, "could not enumerate the kernels of a library module");
+    for (CUfunction fn : fs)
+      if (load(fn) != CUDA_SUCCESS) return fail(SS3D_ECUDA, "could not load a kernel of the library");
+  }
+  return SS3D_OK;
 }
 
 // ---------------------------------------------------------------- device context

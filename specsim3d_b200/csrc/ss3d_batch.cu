@@ -170,6 +170,8 @@ const BatchKernel kBatchKernels[3][NETV] = {{k_batch_pass<0, 0>, k_batch_pass<0,
                                             {k_batch_pass<1, 0>, k_batch_pass<1, 1>},
                                             {k_batch_pass<2, 0>, k_batch_pass<2, 1>}};
 
+const void* module_anchor_batch() { return reinterpret_cast<const void*>(kBatchKernels[0][0]); }
+
 }  // namespace ss3d
 
 using namespace ss3d;

@@ -1479,4 +1479,6 @@ template cudaError_t launch_gen<float>(const Geo&, const float*, const uint32_t*
 template cudaError_t launch_gen<double>(const Geo&, const double*, const uint32_t*, const uint32_t*, double2*,
                                         long long, int, cudaStream_t);
 
+const void* module_anchor_fft() { return reinterpret_cast<const void*>(k_rowstates); }
+
 }  // namespace ss3d

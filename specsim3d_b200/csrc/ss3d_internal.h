@@ -73,6 +73,11 @@ void mark(Marks* m, int stage, cudaStream_t st);   // records an event opening `
 // size: changing a function attribute while instances of it run on other
 // streams can make the call wait for them, so repeated calls return at once.
 cudaError_t func_smem(const void* kernel, size_t bytes);
+// one kernel of each translation unit with kernels: its module holds them all
+const void* module_anchor_fft();
+const void* module_anchor_cond();
+const void* module_anchor_vario();
+const void* module_anchor_batch();
 extern std::atomic<unsigned long long> g_launch_count;   // kernels launched by the library (all threads)
 // launches of kernels that stage tiles with bulk copies and bounded waits;
 // after work that contains one, pipe_error_take reads (and clears) the flag a

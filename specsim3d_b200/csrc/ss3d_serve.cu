@@ -379,6 +379,10 @@ extern "C" int ss3d_server_create(const ss3d_server_config* cfg, ss3d_server** o
     // few MB)
     if (s->cfg.premap_bytes > 0)
       pool_premap((size_t)std::min<int64_t>(s->cfg.premap_bytes, s->cfg.hbm_budget));
+    // load every kernel now: a kernel loaded on its first launch, while
+    // requests run, may synchronise the device under all of them (a driver
+    // without the loading entry points leaves the loads to the launches)
+    if (ss3d_preload_kernels() != SS3D_OK) cudaGetLastError();
   } else if (s->cfg.hbm_budget <= 0) {
     delete s;
     return set_error(SS3D_EINVAL, "dry run needs an explicit hbm_budget");

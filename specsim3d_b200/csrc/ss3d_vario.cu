@@ -240,6 +240,8 @@ __global__ void k_vario_reduce(const double* __restrict__ part, int ncta, int l0
   }
 }
 
+const void* module_anchor_vario() { return reinterpret_cast<const void*>(k_vario_reduce); }
+
 }  // namespace ss3d
 
 using namespace ss3d;

@@ -393,3 +393,15 @@ def test_fused_middle_row_pass_identical(gpu, n):
     finally:
         L.ss3d_set_variant(2, gpu.FP32, lx, 0)
     sp.close()
+
+
+def test_preload_kernels(gpu):
+    """ss3d_preload_kernels loads every kernel of the library's modules (a
+    second call finds them loaded); realizations are the same after it."""
+    n, sts, nug, d, ipad = CASES[1]
+    sp = gpu.Spectrum(sts, nug, d, n, ipad)
+    before = sp.realize(2718, 2, 1, gpu.FP32)
+    gpu.preload_kernels()
+    gpu.preload_kernels()
+    assert np.array_equal(sp.realize(2718, 2, 1, gpu.FP32), before)
+    sp.close()
