@@ -333,9 +333,16 @@ def bench_serving(ss, rates=SERVING_RATES, count=4000, slots=8, budget=64 << 30,
     srv.close()
 
     def open_loop(rate):
+        import gc
         reqs = workloads.request_stream(rate, count=count)
         srv = ss.Server(slots=slots, hbm_budget=budget, premap_bytes=premap)
         tickets = [None] * count
+        lag = np.zeros(count)   # submission time - scheduled arrival (the harness's own delay)
+        # no garbage collection of the harness while it feeds requests: a
+        # collection pause would delay submissions and count as latency
+        gc.collect()
+        gc.freeze()
+        gc.disable()
         t_start = srv.clock() + 0.05
 
         def feeder():
@@ -346,6 +353,7 @@ def bench_serving(ss, rates=SERVING_RATES, count=4000, slots=8, budget=64 << 30,
                     time.sleep(dt)
                 tickets[k] = srv.submit(pool[q["model"]], q["iseed"], q["nreal"], 1, prec, out=outs[k],
                                         t_arrival=t_arr, cond=conds[k])
+                lag[k] = srv.clock() - t_arr
 
         th = threading.Thread(target=feeder)
         th.start()
@@ -355,16 +363,18 @@ def bench_serving(ss, rates=SERVING_RATES, count=4000, slots=8, budget=64 << 30,
                 time.sleep(0.0005)
             res.append(srv.wait(tickets[k]))
         th.join()
+        gc.enable()
+        gc.unfreeze()
         st = srv.stats()
         srv.close()
-        return res, st, t_start
+        return res, st, t_start, lag
 
     # one unmeasured open-loop pass at the highest rate maps the pages of an
     # open-loop run's peak footprint before any timing
     open_loop(max(rates))
     torch.cuda.synchronize()
     for rate in rates:
-        res, st, t_start = open_loop(rate)
+        res, st, t_start, lag = open_loop(rate)
         ok = np.array([r["status"] == 0 for r in res])
         lat = np.array([r["t_done"] - r["t_arrival"] for r in res]) * 1e3
         span = max(r["t_done"] for r in res) - t_start
@@ -374,7 +384,9 @@ def bench_serving(ss, rates=SERVING_RATES, count=4000, slots=8, budget=64 << 30,
             "failed": int((~ok).sum()), "unconditional": _pcts(lat[ok & ~is_cond]),
             "conditional": _pcts(lat[ok & is_cond]), "cache_hits": st["cache_hits"],
             "cache_misses": st["cache_misses"], "peak_running": st["peak_running"],
-            "peak_gb": round(st["peak_bytes"] / 2 ** 30, 2)}
+            "peak_gb": round(st["peak_bytes"] / 2 ** 30, 2),
+            "submit_lag_ms": {"p99": round(1e3 * float(np.percentile(lag, 99)), 3),
+                              "max": round(1e3 * float(lag.max()), 3)}}
     # plain path: one request at a time, no cache
     svc = []
     for k, q in enumerate(base_reqs):

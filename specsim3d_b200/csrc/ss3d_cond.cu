@@ -1501,7 +1501,9 @@ extern "C" int ss3d_condition(double* res, const int n[3], int nreal, const doub
   if (e == cudaSuccess && bt.mode) {
     const size_t tb = backtr_smem_bytes(nt, nbucket);
     if (bt.mode == 1 && tb <= (64u << 10)) {   // 4 blocks of 256 threads per SM
-      e = func_smem((const void*)k_backtr_smem, tb);
+      // the attribute is set once, to the largest table: changing it while
+      // instances run on other streams (a server's other slots) may wait for them
+      e = func_smem((const void*)k_backtr_smem, 64u << 10);
       if (e == cudaSuccess) {
         int nsm = 148;
         cudaDeviceGetAttribute(&nsm, cudaDevAttrMultiProcessorCount, cur_dev);
