@@ -275,7 +275,7 @@ def _pcts(lat_ms):
             "p99_ms": round(float(np.percentile(a, 99)), 3)}
 
 
-def bench_serving(ss, rates=SERVING_RATES, count=4000, slots=8, budget=64 << 30, premap=24 << 30,
+def bench_serving(ss, rates=SERVING_RATES, count=4000, slots=8, budget=64 << 30, premap=40 << 30,
                   arena_bytes=40 << 30):
     """Serving form on the stated configuration: a Poisson request stream of
     `count` requests (seed 2024) at each rate over a pool of 64 models (seed
@@ -371,10 +371,25 @@ def bench_serving(ss, rates=SERVING_RATES, count=4000, slots=8, budget=64 << 30,
 
     # one unmeasured open-loop pass at the highest rate maps the pages of an
     # open-loop run's peak footprint before any timing
+    def pool_reserved_gb():
+        # reserved bytes of the device's stream-ordered pool (high-water mark
+        # and current): growth while requests run maps new pages under all of them
+        try:
+            from cuda.bindings import runtime as rt
+            dev = torch.cuda.current_device()
+            _, pool_h = rt.cudaDeviceGetDefaultMemPool(dev)
+            _, hi = rt.cudaMemPoolGetAttribute(pool_h, rt.cudaMemPoolAttr.cudaMemPoolAttrReservedMemHigh)
+            _, cur = rt.cudaMemPoolGetAttribute(pool_h, rt.cudaMemPoolAttr.cudaMemPoolAttrReservedMemCurrent)
+            return round(int(hi) / 2 ** 30, 2), round(int(cur) / 2 ** 30, 2)
+        except Exception:
+            return None, None
+
     open_loop(max(rates))
     torch.cuda.synchronize()
     for rate in rates:
+        pool_before = pool_reserved_gb()
         res, st, t_start, lag = open_loop(rate)
+        pool_after = pool_reserved_gb()
         ok = np.array([r["status"] == 0 for r in res])
         lat = np.array([r["t_done"] - r["t_arrival"] for r in res]) * 1e3
         span = max(r["t_done"] for r in res) - t_start
@@ -386,7 +401,9 @@ def bench_serving(ss, rates=SERVING_RATES, count=4000, slots=8, budget=64 << 30,
             "cache_misses": st["cache_misses"], "peak_running": st["peak_running"],
             "peak_gb": round(st["peak_bytes"] / 2 ** 30, 2),
             "submit_lag_ms": {"p99": round(1e3 * float(np.percentile(lag, 99)), 3),
-                              "max": round(1e3 * float(lag.max()), 3)}}
+                              "max": round(1e3 * float(lag.max()), 3)},
+            "pool_reserved_gb": {"high_before": pool_before[0], "high_after": pool_after[0],
+                                 "current_after": pool_after[1]}}
     # plain path: one request at a time, no cache
     svc = []
     for k, q in enumerate(base_reqs):

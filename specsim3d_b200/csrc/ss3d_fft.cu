@@ -495,6 +495,31 @@ __global__ void k_reduce_zstats(const double* __restrict__ part, int nblk, doubl
 // (f90:1256-1270): row (j,k) of c(i,j,k) = C(ip dx, jp dy, kp dz) with minimum
 // image lags, R2C of length npx = 2N through a length-N complex FFT:
 //   X[q] = (Z[q] + conj Z[N-q])/2 - i/2 w^q (Z[q] - conj Z[N-q]),  w = e^{-2 pi i/(2N)}
+// C at the lag whose range-scaled rotated components are b + ip s per
+// structure (b: the row's lag (0, jp dy, kp dz), s: one x step, both rotated
+// and divided by the range): the covariance of f90:153-178 with the rotation
+// of a row done once, no division per point, and for the gaussian model no
+// square root (it needs only h^2)
+__device__ __forceinline__ double cov_row_point(const Model& m, const double* __restrict__ b,
+                                                const double* __restrict__ sx, double ip, bool origin) {
+  double c = origin ? m.nugget : 0.0;
+  for (int st = 0; st < m.nst; st++) {
+    const double rx = fma(ip, sx[3 * st], b[3 * st]);
+    const double ry = fma(ip, sx[3 * st + 1], b[3 * st + 1]);
+    const double rz = fma(ip, sx[3 * st + 2], b[3 * st + 2]);
+    const double h2 = rx * rx + ry * ry + rz * rz;
+    if (m.itype[st] == 1) {
+      const double hr = sqrt(h2);
+      if (hr < 1.0) c = c + m.sill[st] * (1.0 - 1.5 * hr + 0.5 * (hr * hr * hr));
+    } else if (m.itype[st] == 2) {
+      c = c + m.sill[st] * exp(-3.0 * sqrt(h2));
+    } else {
+      c = c + m.sill[st] * exp(-(3.0 * h2));
+    }
+  }
+  return c;
+}
+
 template <int LOGN>
 __global__ void __launch_bounds__(NT) k_spec_rows(Model m, double dx, double dy, double dz, Geo g,
                                                   double2* __restrict__ out, Tw tw) {
@@ -507,20 +532,37 @@ __global__ void __launch_bounds__(NT) k_spec_rows(Model m, double dx, double dy,
   C* stw = s + (N + 1) * PITCH;
   const int nrows = g.npy * g.npz;
   const int row0 = blockIdx.x * TX;
+  double* rb = reinterpret_cast<double*>(stw + 2 * N);   // [TX][MAXST][3] rotated row lags / range
+  double* rsx = rb + TX * MAXST * 3;                      // [MAXST][3] rotated x step / range
   load_tw(stw, tw.d, 2 * N, 2 * N);
+  for (int q = threadIdx.x; q < (TX + 1) * m.nst; q += NT) {
+    const int t = q / m.nst, st = q - t * m.nst;
+    const double* r = m.rot[st];
+    const double ia = 1.0 / m.ahmax[st];
+    if (t == TX) {
+      for (int c = 0; c < 3; c++) rsx[3 * st + c] = r[3 * c] * dx * ia;
+    } else {
+      const int row = min(row0 + t, nrows - 1);
+      const int j = row % g.npy, k = row / g.npy;
+      const double y = (double)(j > g.npy / 2 ? j - g.npy : j) * dy;
+      const double z = (double)(k > g.npz / 2 ? k - g.npz : k) * dz;
+      for (int c = 0; c < 3; c++) rb[(t * MAXST + st) * 3 + c] = (r[3 * c + 1] * y + r[3 * c + 2] * z) * ia;
+    }
+  }
+  __syncthreads();
   for (int q = threadIdx.x; q < N * TX; q += NT) {
     int t = q / N, p = q % N;
     int row = row0 + t;
     C v = cmk<C>(0.0, 0.0);
     if (row < nrows) {
-      int j = row % g.npy, k = row / g.npy;
-      int kp = k > g.npz / 2 ? k - g.npz : k;
-      int jp = j > g.npy / 2 ? j - g.npy : j;
+      const int j = row % g.npy, k = row / g.npy;
+      const bool jk0 = j == 0 && k == 0;
       int i0 = 2 * p, i1 = 2 * p + 1;
       int ip0 = i0 > g.npx / 2 ? i0 - g.npx : i0;
       int ip1 = i1 > g.npx / 2 ? i1 - g.npx : i1;
-      v.x = covariance(m, (double)ip0 * dx, (double)jp * dy, (double)kp * dz);
-      v.y = covariance(m, (double)ip1 * dx, (double)jp * dy, (double)kp * dz);
+      const double* b = rb + t * MAXST * 3;
+      v.x = cov_row_point(m, b, rsx, (double)ip0, jk0 && ip0 == 0);
+      v.y = cov_row_point(m, b, rsx, (double)ip1, jk0 && ip1 == 0);
     }
     s[p * PITCH + t] = v;
   }
@@ -1097,7 +1139,7 @@ static cudaError_t run_spec_rows(const Model& m, const double d[3], const Geo& g
                                  cudaStream_t st) {
   constexpr int TX = RowTX<double, L>::TX;
   constexpr int N = 1 << L;
-  size_t smem = (size_t)((N + 1) * (TX + 1) + 2 * N) * sizeof(double2);
+  size_t smem = (size_t)((N + 1) * (TX + 1) + 2 * N) * sizeof(double2) + (size_t)(TX + 1) * MAXST * 3 * sizeof(double);
   cudaError_t e = set_smem(k_spec_rows<L>, smem);
   if (e != cudaSuccess) return e;
   int nblk = (g.npy * g.npz + TX - 1) / TX;
