@@ -599,6 +599,112 @@ __global__ void __launch_bounds__(NT) k_spec_rows(Model m, double dx, double dy,
   }
 }
 
+// The same rows (covariance and R2C) with each row in the registers of the
+// TPC lanes of one warp, for N = npx/2 <= 256 (8 complex values per lane):
+// a lane computes its 16 covariance values (the real pairs at x = 2q, 2q + 1)
+// straight into the registers of the first radix pass, the register engine
+// transforms them on the warp's shared slice, the transform is staged once in
+// that slice in natural order, and the split reads Z[k] and Z[N-k] and stores
+// X[k] and X[N-k] of the row (k <= N/2).  The shared-memory row tile of
+// k_spec_rows also stages the input, runs every radix pass through shared
+// memory and splits in place.
+template <int LOGN> struct SpecWarpCfg {
+  static constexpr int N = 1 << LOGN;
+  static constexpr int ET = 8;                  // complex values per lane
+  static constexpr int TPC = N / ET;            // lanes per row
+  static constexpr int RPW = TPC >= 32 ? 1 : 32 / TPC;
+  static constexpr int NW = 8;                  // warps per block
+  static constexpr int NTH = 32 * NW;
+  static constexpr int ROWS = NW * RPW;         // rows per block
+  static constexpr int SLICE = N * RPW;         // exchange elements per warp
+  static constexpr bool ok = LOGN >= 3 && LOGN <= 8;
+  static constexpr size_t smem =
+      (size_t)(3 * N + NW * SLICE) * sizeof(double2) + (size_t)(ROWS + 1) * MAXST * 3 * sizeof(double);
+};
+
+template <int LOGN>
+__global__ void __launch_bounds__(SpecWarpCfg<LOGN>::NTH) k_spec_rows_warp(Model m, double dx, double dy, double dz,
+                                                                          Geo g, double2* __restrict__ out, Tw tw) {
+  using C = double2;
+  using W = SpecWarpCfg<LOGN>;
+  constexpr int N = W::N, ET = W::ET, TPC = W::TPC, RPW = W::RPW;
+  static_assert(W::ok && TPC * RPW == 32, "rows of whole warps");
+  extern __shared__ __align__(16) unsigned char smraw[];
+  C* stw = reinterpret_cast<C*>(smraw);   // 2N entries e^{-2 pi i m/(2N)} (the split)
+  C* stwN = stw + 2 * N;                  // N entries e^{-2 pi i m/N} (the transform)
+  C* slices = stwN + N;
+  double* rb = reinterpret_cast<double*>(slices + W::NW * W::SLICE);   // [ROWS][MAXST][3]
+  double* rsx = rb + W::ROWS * MAXST * 3;                             // [MAXST][3]
+  const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
+  C* sx = slices + warp * W::SLICE;
+  const int nrows = g.npy * g.npz;
+  const int rowb = blockIdx.x * W::ROWS;
+  for (int q = threadIdx.x; q < 2 * N; q += W::NTH) stw[q] = tw.d[2 * N - 1 + q];
+  for (int q = threadIdx.x; q < N; q += W::NTH) stwN[q] = tw.d[N - 1 + q];
+  for (int q = threadIdx.x; q < (W::ROWS + 1) * m.nst; q += W::NTH) {
+    const int t = q / m.nst, st = q - t * m.nst;
+    const double* r = m.rot[st];
+    const double ia = 1.0 / m.ahmax[st];
+    if (t == W::ROWS) {
+      for (int cc = 0; cc < 3; cc++) rsx[3 * st + cc] = r[3 * cc] * dx * ia;
+    } else {
+      const int row = min(rowb + t, nrows - 1);
+      const int j = row % g.npy, k = row / g.npy;
+      const double y = (double)(j > g.npy / 2 ? j - g.npy : j) * dy;
+      const double z = (double)(k > g.npz / 2 ? k - g.npz : k) * dz;
+      for (int cc = 0; cc < 3; cc++) rb[(t * MAXST + st) * 3 + cc] = (r[3 * cc + 1] * y + r[3 * cc + 2] * z) * ia;
+    }
+  }
+  __syncthreads();
+  const int t = lane % RPW, c = lane / RPW;
+  const int rw = warp * RPW + t;
+  const int row = rowb + rw;
+  const bool ok = row < nrows;
+  const int j = ok ? row % g.npy : 0, k = ok ? row / g.npy : 0;
+  const bool jk0 = j == 0 && k == 0;
+  const double* b = rb + rw * MAXST * 3;
+  constexpr int R0 = Sched<LOGN>::radix(0), NBT = ET / R0;
+  C v[ET];
+  // pass-0 order of the engine: v[mm R0 + r] holds position c + TPC mm + r N / R0
+#pragma unroll
+  for (int mm = 0; mm < NBT; ++mm)
+#pragma unroll
+    for (int r = 0; r < R0; ++r) {
+      const int q = c + TPC * mm + r * (N / R0);
+      const int i0 = 2 * q, i1 = 2 * q + 1;
+      const int ip0 = i0 > g.npx / 2 ? i0 - g.npx : i0;
+      const int ip1 = i1 > g.npx / 2 ? i1 - g.npx : i1;
+      C zv = cmk<C>(0.0, 0.0);
+      if (ok) {
+        zv.x = cov_row_point(m, b, rsx, (double)ip0, jk0 && ip0 == 0);
+        zv.y = cov_row_point(m, b, rsx, (double)ip1, jk0 && ip1 == 0);
+      }
+      v[mm * R0 + r] = zv;
+    }
+  fft_tile_regs<LOGN, RPW, TPC, -1, RPW, false, true, -1>(
+      sx, stwN, v, t, c, [&](int pos, C zz) { sx[xidx<RPW, -1>(pos, t)] = zz; });
+  __syncwarp();
+  if (ok) {
+    C* orow = out + ((long long)k * g.npy + j) * g.HP;
+    for (int kk = c; kk <= N / 2; kk += TPC) {
+      const int kc = N - kk;
+      const C zk = sx[xidx<RPW, -1>(kk, t)];
+      const C zc = sx[xidx<RPW, -1>(kc & (N - 1), t)];
+      const C zcc = cmk<C>(zc.x, -zc.y), zkc = cmk<C>(zk.x, -zk.y);
+      const C w = stw[kk];
+      const C sum = cadd(zk, zcc), dif = csub(zk, zcc);
+      const C wd = cmul(w, dif);
+      orow[kk] = cadd(cmk<C>(0.5 * sum.x, 0.5 * sum.y), cmk<C>(0.5 * wd.y, -0.5 * wd.x));   // - i/2 w dif
+      if (kc != kk) {
+        const C w2 = stw[kc];
+        const C sum2 = cadd(zc, zkc), dif2 = csub(zc, zkc);
+        const C wd2 = cmul(w2, dif2);
+        orow[kc] = cadd(cmk<C>(0.5 * sum2.x, 0.5 * sum2.y), cmk<C>(0.5 * wd2.y, -0.5 * wd2.x));
+      }
+    }
+  }
+}
+
 // c2c transform of nrows contiguous rows of length 2^LOGN in place, unscaled
 // (the x pass of the full-grid transform ss3d_fft3d): TX rows staged in
 // shared memory, the shared-memory Stockham engine, rows written back
@@ -1139,6 +1245,15 @@ static cudaError_t run_spec_rows(const Model& m, const double d[3], const Geo& g
                                  cudaStream_t st) {
   constexpr int TX = RowTX<double, L>::TX;
   constexpr int N = 1 << L;
+  if constexpr (SpecWarpCfg<L>::ok) {   // rows in warps
+    using W = SpecWarpCfg<L>;
+    cudaError_t e = set_smem(k_spec_rows_warp<L>, W::smem);
+    if (e != cudaSuccess) return e;
+    const int nblk = (g.npy * g.npz + W::ROWS - 1) / W::ROWS;
+    k_spec_rows_warp<L><<<nblk, W::NTH, W::smem, st>>>(m, d[0], d[1], d[2], g, out, tw);
+    ++g_launch_count;
+    return cudaGetLastError();
+  }
   size_t smem = (size_t)((N + 1) * (TX + 1) + 2 * N) * sizeof(double2) + (size_t)(TX + 1) * MAXST * 3 * sizeof(double);
   cudaError_t e = set_smem(k_spec_rows<L>, smem);
   if (e != cudaSuccess) return e;
