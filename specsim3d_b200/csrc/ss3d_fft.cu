@@ -749,7 +749,9 @@ __global__ void k_spec_rows_n1(Model m, double dx, double dy, double dz, Geo g, 
 __global__ void k_spec_amp(Geo g, const double2* __restrict__ X, double* __restrict__ amp64,
                            float* __restrict__ amp32, SpecPartial* part) {
   const long long tot = (long long)g.npz * g.npy * g.HP;
-  const double rn = (double)g.npx * (double)g.npy * (double)g.npz;
+  // 1/N: N = npx npy npz is a power of two, so the product by its reciprocal
+  // is exactly the division X / N of f90:1273-1274
+  const double irn = 1.0 / ((double)g.npx * (double)g.npy * (double)g.npz);
   double mi = 0, mr = 0, sp = 0, sn = 0;
   for (long long q = blockIdx.x * (long long)blockDim.x + threadIdx.x; q < tot;
        q += (long long)gridDim.x * blockDim.x) {
@@ -757,7 +759,7 @@ __global__ void k_spec_amp(Geo g, const double2* __restrict__ X, double* __restr
     double a = 0.0;
     if (i < g.H) {
       double2 v = X[q];
-      double re = v.x / rn, im = v.y / rn;
+      double re = v.x * irn, im = v.y * irn;
       double w = (i == 0 || 2 * i == g.npx) ? 1.0 : 2.0;
       mi = fmax(mi, fabs(im));
       mr = fmax(mr, fabs(re));
@@ -825,7 +827,9 @@ __global__ void __launch_bounds__(ColCfg<double, LOGN, 0>::NTH)
   const bool valid = inside && i < g.H;
   const C* src = in + (valid ? line : 0);
   const int S = (int)a.S;
-  const double rn = (double)g.npx * (double)g.npy * (double)g.npz;
+  // 1/N: N = npx npy npz is a power of two, so the product by its reciprocal
+  // is exactly the division X / N of f90:1273-1274
+  const double irn = 1.0 / ((double)g.npx * (double)g.npy * (double)g.npz);
   const double wgt = (i == 0 || 2 * i == g.npx) ? 1.0 : 2.0;
   double mi = 0.0, mr = 0.0, sp = 0.0, sn = 0.0;
   for (int q = threadIdx.x; q < N; q += NTH) stw[q] = tw.d[N - 1 + q];
@@ -834,7 +838,7 @@ __global__ void __launch_bounds__(ColCfg<double, LOGN, 0>::NTH)
       s, stw, [&](int jb, int r) { return src[(jb + r * NR0) * S]; },
       [&](int pos, C v) {
         if (valid) {
-          const double re = v.x / rn, im = v.y / rn;
+          const double re = v.x * irn, im = v.y * irn;
           mi = fmax(mi, fabs(im));
           mr = fmax(mr, fabs(re));
           double am = 0.0;

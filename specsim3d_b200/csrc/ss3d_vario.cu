@@ -287,13 +287,14 @@ extern "C" int ss3d_vario(const double* res, const int n[3], int nreal, int ndir
   long long* npdev = nullptr;
   cudaError_t e = cudaSuccess;
   if (!dev_in) {
-    e = cudaMalloc(&fbuf, sizeof(double) * M * nreal);
+    e = cudaMallocAsync((void**)&fbuf, sizeof(double) * M * nreal, st);
     if (e == cudaSuccess) e = cudaMemcpyAsync(fbuf, res, sizeof(double) * M * nreal, cudaMemcpyHostToDevice, st);
     fdev = fbuf;
   }
-  if (e == cudaSuccess) e = cudaMalloc(&gdev, sizeof(double) * ngam);
+  // temporaries from the stream-ordered pool: no device-wide synchronisation
+  if (e == cudaSuccess) e = cudaMallocAsync((void**)&gdev, sizeof(double) * ngam, st);
   if (e == cudaSuccess) e = cudaMemsetAsync(gdev, 0, sizeof(double) * ngam, st);
-  if (e == cudaSuccess) e = cudaMalloc(&npdev, sizeof(long long) * VLCH);
+  if (e == cudaSuccess) e = cudaMallocAsync((void**)&npdev, sizeof(long long) * VLCH, st);
   // largest partial buffer over directions
   size_t part_elems = 0;
   std::vector<VarioGeo> geos(ndir);
@@ -358,7 +359,7 @@ extern "C" int ss3d_vario(const double* res, const int n[3], int nreal, int ndir
   if (part_elems) rgroup = (int)std::max<size_t>(1, ((size_t)256 << 20) / (part_elems * sizeof(double)));
   rgroup = std::min(std::min(rgroup, nreal), 65535);
   part_elems *= (size_t)rgroup;
-  if (e == cudaSuccess && part_elems) e = cudaMalloc(&part, sizeof(double) * part_elems);
+  if (e == cudaSuccess && part_elems) e = cudaMallocAsync((void**)&part, sizeof(double) * part_elems, st);
   for (int d = 0; d < ndir && e == cudaSuccess; d++) {
     const VarioGeo& G = geos[d];
     if (nlag[d] == 0 || G.ncta == 0) continue;
@@ -406,10 +407,10 @@ extern "C" int ss3d_vario(const double* res, const int n[3], int nreal, int ndir
     e = cudaMemcpyAsync(gam, gdev, sizeof(double) * ngam, dev_gam ? cudaMemcpyDeviceToDevice : cudaMemcpyDeviceToHost,
                         st);
   if (e == cudaSuccess) e = cudaStreamSynchronize(st);
-  if (fbuf) cudaFree(fbuf);
-  if (gdev) cudaFree(gdev);
-  if (part) cudaFree(part);
-  if (npdev) cudaFree(npdev);
+  if (fbuf) cudaFreeAsync(fbuf, st);
+  if (gdev) cudaFreeAsync(gdev, st);
+  if (part) cudaFreeAsync(part, st);
+  if (npdev) cudaFreeAsync(npdev, st);
   if (e != cudaSuccess) {
     cudaGetLastError();
     return set_error(SS3D_ECUDA, (std::string("vario: ") + cudaGetErrorString(e)).c_str());
