@@ -1484,9 +1484,12 @@ extern "C" int ss3d_condition(double* res, const int n[3], int nreal, const doub
     ++g_launch_count;
     e = cudaGetLastError();
     if (e != cudaSuccess) break;
-    // one block per wpb nodes (short blocks): work of other streams, e.g. of a
-    // serving loop's higher-priority requests, gets SMs as blocks finish
-    const int nblk = (int)(((long long)count + wpb - 1) / wpb);
+    // short blocks (wpb warps of one node each, four nodes per warp in turn in
+    // the register kernels, whose block setup would otherwise be paid per
+    // node): work of other streams, e.g. of a serving loop's higher-priority
+    // requests, gets SMs as blocks finish
+    const long long per_blk = (long long)wpb * (ndt ? 4 : 1);
+    const int nblk = (int)(((long long)count + per_blk - 1) / per_blk);
     const size_t ksm = kfix + per * wpb;
     void* kargs_reg[] = {&G, &dmdl, &ctab, &node0, (void*)&count, &dnbr, &dnnb, &dix, &diy, &diz, &ddg, &dsimd,
                          &dres, &dcnt};
