@@ -100,7 +100,12 @@ __host__ __device__ __forceinline__ uint32_t pm_mulmod(uint32_t a, uint32_t b) {
   const uint32_t lo = (uint32_t)p, hi = (uint32_t)(p >> 32);
 #endif
   uint32_t r = (lo & PM_M) + ((hi << 1) | (lo >> 31));   // <= 2m - 2 for a, b < m
+  // r - m wraps above r when r < m: the unsigned minimum is the reduced value
+#ifdef __CUDA_ARCH__
+  return min(r, r - PM_M);
+#else
   return r >= PM_M ? r - PM_M : r;
+#endif
 }
 
 // the same product without the final conditional subtraction: a value in
