@@ -185,6 +185,19 @@ __device__ __forceinline__ cpair coef_pair(uint32_t s0, uint32_t s1, float2 am, 
   }
 }
 
+// Row state that the draw of position p takes (rs_own: its own rows, rs_par:
+// the partner rows).  Row states are [j][k] with k fastest, so consecutive
+// positions along z hold consecutive states; along y (the first pass of a 2D
+// grid) npz = 1 makes them consecutive too.  The partner position (N - p) mod N
+// is N - p in the slots r >= 1 of pass 0 (p >= N/R0 > 0); in slot 0 only p = 0
+// takes the partner's draw, whose partner position is 0.  r is a compile-time
+// constant in the loaders, so every address is a per-thread base plus an
+// immediate offset.
+__device__ __forceinline__ const uint32_t* partner_state(const uint32_t* rs_own, const uint32_t* rs_par, int p,
+                                                         int r, bool greater, int N) {
+  return greater ? (r == 0 ? rs_par : rs_par + (N - p)) : rs_own + p;
+}
+
 // First inverse pass with the coefficient synthesis fused into the loader.
 // axis 2: columns are (i, j) plane offsets, positions k;  axis 1 (npz = 1):
 // columns are i, positions j.  Along the transformed axis (length N) the
@@ -225,7 +238,6 @@ __device__ __forceinline__ void colgen_body(const AxisArgs& a, const Geo& g, con
   const int jp0 = (-j0) & (g.npy - 1);
   const bool cgt = zaxis && j0 > jp0;                      // mid positions: partner's draw
   const bool selfcol = (!zaxis || j0 == jp0) && iedge;     // mid positions: self-conjugate
-  const int rowstride = zaxis ? 1 : g.npz;   // row states [j][k]: k runs fastest
   const uint32_t* rs = rowstates + (size_t)r * g.npy * g.npz;
   const uint32_t* rs_own = rs + (zaxis ? (size_t)j0 * g.npz : 0);
   const uint32_t* rs_par = rs + (zaxis ? (size_t)jp0 * g.npz : 0);
@@ -252,8 +264,7 @@ __device__ __forceinline__ void colgen_body(const AxisArgs& a, const Geo& g, con
           mid = false;
           greater = 2 * rr > R0;
         }
-        const int pp = (N - p) & (N - 1);
-        const uint32_t st = __ldg(greater ? rs_par + pp * rowstride : rs_own + p * rowstride);
+        const uint32_t st = __ldg(partner_state(rs_own, rs_par, p, rr, greater, N));
         const uint32_t s1 = pm_mulmod(st, greater ? aip : ai);
         return coef_from_state<R, GAUSS>(s1, am, mid && selfcol, greater);
       },
@@ -355,7 +366,6 @@ __device__ __forceinline__ void colgen_body_pair(const AxisArgs& a, const Geo& g
   const bool cgt = zaxis && j0 > jp0;
   const bool selfrow = !zaxis || j0 == jp0;
   const bool self0 = selfrow && iedge0, self1 = selfrow && iedge1;
-  const int rowstride = zaxis ? 1 : g.npz;
   const uint32_t* rs = rowstates + (size_t)r * g.npy * g.npz;
   const uint32_t* rs_own = rs + (zaxis ? (size_t)j0 * g.npz : 0);
   const uint32_t* rs_par = rs + (zaxis ? (size_t)jp0 * g.npz : 0);
@@ -382,8 +392,7 @@ __device__ __forceinline__ void colgen_body_pair(const AxisArgs& a, const Geo& g
           mid = false;
           greater = 2 * rr > R0;
         }
-        const int pp = (N - p) & (N - 1);
-        const uint32_t st = __ldg(greater ? rs_par + pp * rowstride : rs_own + p * rowstride);
+        const uint32_t st = __ldg(partner_state(rs_own, rs_par, p, rr, greater, N));
         return coef_pair<GAUSS>(pm_mulmod(st, greater ? aip0 : ai0), pm_mulmod(st, greater ? aip1 : ai1), am,
                                 mid && self0, mid && self1, greater);
       },
