@@ -55,7 +55,7 @@ template <typename R, int LOGN, int V = 0> struct ColCfg {
 };
 
 // c2c transform along a strided axis (in place allowed), unscaled, pruned store
-template <typename R, int LOGN, int TX, int TPC, int SIGN>
+template <typename R, int LOGN, int TX, int TPC, int SIGN, bool HALF = false>
 __device__ __forceinline__ void col_body(const AxisArgs& a, const Geo& g, const cpx_t<R>* in, cpx_t<R>* out,
                                          const Tw& tw, int item, unsigned char* smraw) {
   using C = cpx_t<R>;
@@ -78,7 +78,7 @@ __device__ __forceinline__ void col_body(const AxisArgs& a, const Geo& g, const 
   constexpr int NR0 = N / Sched<LOGN>::radix(0);
   for (int q = threadIdx.x; q < N; q += NTH) stw[q] = twtab<R>(tw)[N - 1 + q];
   __syncthreads();
-  fft_tile<LOGN, TX, TPC, SIGN>(
+  fft_tile<LOGN, TX, TPC, SIGN, TX, false, false, HALF>(
       s, stw, [&](int jb, int r) { return src[(jb + r * NR0) * S]; },
       [&](int pos, C v) {
         if (valid && pos < nout) dst[pos * S] = v;
@@ -146,36 +146,40 @@ __device__ __forceinline__ float2 m2log_f2(uint32_t s0, uint32_t s1) {
                           kconst<float2>(M2LOG_C31));
   return make_float2(s0 >= 1610612736u ? near1.x : far.x, s1 >= 1610612736u ? near1.y : far.y);
 }
-// cos and sin of the two remainders; odd0/odd1 as phasor_half_f returns them
-__device__ __forceinline__ void phasor_half_f2(uint32_t s0, uint32_t s1, float2& c, float2& sn, bool& odd0,
-                                               bool& odd1) {
+// cos and sin of the two remainders; sb0/sb1 hold the sign of the phasor in
+// bit 31 (set for an odd half-turn count, as phasor_half_f's result), for
+// callers that apply it to a factor by flipping that bit
+__device__ __forceinline__ void phasor_half_f2(uint32_t s0, uint32_t s1, float2& c, float2& sn, uint32_t& sb0,
+                                               uint32_t& sb1) {
   const int n0 = half_turns(s0), n1 = half_turns(s1);
   const float2 x = kmul(make_float2((float)half_turn_rem(s0, n0), (float)half_turn_rem(s1, n1)),
                         kconst<float2>(1.4629181e-9f));
   sn = make_float2(sin_hw(x.x), sin_hw(x.y));
   c = make_float2(cos_hw(x.x), cos_hw(x.y));
-  odd0 = n0 & 1;
-  odd1 = n1 & 1;
+  sb0 = (uint32_t)n0 << 31;
+  sb1 = (uint32_t)n1 << 31;
 }
+// v with its sign bit flipped where sb has bit 31 set (exactly -v then)
+__device__ __forceinline__ float sign_flip(float v, uint32_t sb) { return __uint_as_float(__float_as_uint(v) ^ sb); }
 template <int GAUSS>
 __device__ __forceinline__ cpair coef_pair(uint32_t s0, uint32_t s1, float2 am, bool self0, bool self1, bool conj) {
   if constexpr (GAUSS) {
     const float2 L = m2log_f2(s0, s1);
     const float2 rr = kmul(L, make_float2(rsqrt_hw(L.x), rsqrt_hw(L.y)));
     float2 cs, sn;
-    bool odd0, odd1;
-    phasor_half_f2(pm_mulmod_lazy(s0, PM_A), pm_mulmod_lazy(s1, PM_A), cs, sn, odd0, odd1);
+    uint32_t sb0, sb1;
+    phasor_half_f2(pm_mulmod_lazy(s0, PM_A), pm_mulmod_lazy(s1, PM_A), cs, sn, sb0, sb1);
     const float2 ah = kmul(am, kconst<float2>(0.70710678118654752f));
     const float2 t0 = kmul(make_float2(self0 ? am.x : ah.x, self1 ? am.y : ah.y), rr);
-    const float2 t = make_float2(odd0 ? -t0.x : t0.x, odd1 ? -t0.y : t0.y);
+    const float2 t = make_float2(sign_flip(t0.x, sb0), sign_flip(t0.y, sb1));
     const float2 re = kmul(t, cs);
     const float2 im = kmul(conj ? kneg(t) : t, sn);
     return cpair{re, make_float2(self0 ? 0.f : im.x, self1 ? 0.f : im.y)};
   } else {
     float2 cs, sn;
-    bool odd0, odd1;
-    phasor_half_f2(s0, s1, cs, sn, odd0, odd1);
-    const float2 a = make_float2(odd0 ? -am.x : am.x, odd1 ? -am.y : am.y);
+    uint32_t sb0, sb1;
+    phasor_half_f2(s0, s1, cs, sn, sb0, sb1);
+    const float2 a = make_float2(sign_flip(am.x, sb0), sign_flip(am.y, sb1));
     const float2 re = kmul(a, cs);
     const float2 im0 = kmul(a, sn);
     const float2 im = conj ? kneg(im0) : im0;
@@ -207,7 +211,7 @@ __device__ __forceinline__ const uint32_t* partner_state(const uint32_t* rs_own,
 // as the reference's lin/linp comparison (f90:1315-1331) does.  The pass-0
 // loader sees p = jb + r N/R0 with r constant, so only the two slots r = 0 and
 // r = R0/2 of the butterflies with jb = 0 need a run-time decision.
-template <typename R, int LOGN, int TX, int TPC, int GAUSS>
+template <typename R, int LOGN, int TX, int TPC, int GAUSS, bool HALF = false>
 __device__ __forceinline__ void colgen_body(const AxisArgs& a, const Geo& g, const R* __restrict__ amp,
                                             const uint32_t* __restrict__ rowstates,
                                             const uint32_t* __restrict__ apow, cpx_t<R>* out, const Tw& tw,
@@ -248,7 +252,7 @@ __device__ __forceinline__ void colgen_body(const AxisArgs& a, const Geo& g, con
   const int nout = a.nout;
   for (int q = threadIdx.x; q < N; q += NTH) stw[q] = twtab<R>(tw)[N - 1 + q];
   __syncthreads();
-  fft_tile<LOGN, TX, TPC, +1>(
+  fft_tile<LOGN, TX, TPC, +1, TX, false, false, HALF>(
       s, stw,
       [&](int jb, int rr) {
         const int p = jb + rr * NR0;
@@ -305,7 +309,7 @@ __device__ __forceinline__ void load_tw_pair(cpair* stw, const Tw& tw) {
 __device__ __forceinline__ cpair pair_of(float4 v) { return cpair{make_float2(v.x, v.z), make_float2(v.y, v.w)}; }
 __device__ __forceinline__ float4 quad_of(cpair v) { return make_float4(v.x.x, v.y.x, v.x.y, v.y.y); }
 
-template <int LOGN, int TX, int TPC, int SIGN>
+template <int LOGN, int TX, int TPC, int SIGN, bool HALF = false>
 __device__ __forceinline__ void col_body_pair(const AxisArgs& a, const Geo& g, const float2* in, float2* out,
                                               const Tw& tw, int item, unsigned char* smraw) {
   constexpr int N = 1 << LOGN;
@@ -326,7 +330,7 @@ __device__ __forceinline__ void col_body_pair(const AxisArgs& a, const Geo& g, c
   constexpr int NR0 = N / Sched<LOGN>::radix(0);
   load_tw_pair<N, NTH>(stw, tw);
   __syncthreads();
-  fft_tile<LOGN, TX, TPC, SIGN>(
+  fft_tile<LOGN, TX, TPC, SIGN, TX, false, false, HALF>(
       s, stw,
       [&](int jb, int rr) { return pair_of(src[(jb + rr * NR0) * S2]); },
       [&](int pos, cpair v) {
@@ -337,7 +341,7 @@ __device__ __forceinline__ void col_body_pair(const AxisArgs& a, const Geo& g, c
 // synthesis + first inverse pass for two lines (indices i0 = even, i1 = i0 + 1
 // of one row); the row state of a position serves both, the two amplitudes
 // are one 8-byte load.  Decisions as in colgen_body.
-template <int LOGN, int TX, int TPC, int GAUSS>
+template <int LOGN, int TX, int TPC, int GAUSS, bool HALF = false>
 __device__ __forceinline__ void colgen_body_pair(const AxisArgs& a, const Geo& g, const float* __restrict__ amp,
                                                  const uint32_t* __restrict__ rowstates,
                                                  const uint32_t* __restrict__ apow, float2* out, const Tw& tw,
@@ -376,7 +380,7 @@ __device__ __forceinline__ void colgen_body_pair(const AxisArgs& a, const Geo& g
   const int nout = a.nout;
   load_tw_pair<N, NTH>(stw, tw);
   __syncthreads();
-  fft_tile<LOGN, TX, TPC, +1>(
+  fft_tile<LOGN, TX, TPC, +1, TX, false, false, HALF>(
       s, stw,
       [&](int jb, int rr) {
         const int p = jb + rr * NR0;
@@ -590,7 +594,7 @@ template <typename R, int LOGN> struct RowWarpCfg {
   static constexpr size_t smem = (size_t)(2 * N + NW * SLICE) * sizeof(cpx_t<R>);
 };
 
-template <typename R, typename O, int LOGN>
+template <typename R, typename O, int LOGN, bool HALF = false>
 __device__ __forceinline__ void rows_warp_body(const Geo& g, const cpx_t<R>* __restrict__ in, long long rstride,
                                                O* __restrict__ out, long long ostride, int nreal, int nblk_per_r,
                                                double* __restrict__ part, const Tw& tw, int item,
@@ -654,7 +658,7 @@ __device__ __forceinline__ void rows_warp_body(const Geo& g, const cpx_t<R>* __r
   O* orow = out + (long long)r * ostride + (long long)(ok ? row : 0) * g.nx;
   const int nxh = (g.nx + 1) / 2;
   const bool even = (g.nx & 1) == 0;
-  fft_tile_regs<LOGN, RPW, TPC, +1, RPW, false, false, -1>(sx, stwN, v, t, c, [&](int pos, C zz) {
+  fft_tile_regs<LOGN, RPW, TPC, +1, RPW, false, false, -1, HALF>(sx, stwN, v, t, c, [&](int pos, C zz) {
     if (ok && pos < nxh) {
       const O a0 = (O)zz.x, a1 = (O)zz.y;
       const bool second = even || 2 * pos + 1 < g.nx;

@@ -59,7 +59,8 @@ template <int PITCH, int EB> struct Swizzle {
   static constexpr int M = (pow2 && row < 128) ? (128 / row > 8 ? 7 : 128 / row - 1) : 0;
 };
 
-template <int LOGN, int TX, int TPC, int SIGN, int P, int PITCH, bool STORE_SYNC, int SWM, typename C, class Store>
+template <int LOGN, int TX, int TPC, int SIGN, int P, int PITCH, bool STORE_SYNC, int SWM, bool HALF, typename C,
+          class Store>
 __device__ __forceinline__ void fft_tile_rest(C* __restrict__ s, const C* __restrict__ tw, C* v, int t, int c,
                                               Store&& store) {
   constexpr int N = 1 << LOGN;
@@ -91,7 +92,8 @@ __device__ __forceinline__ void fft_tile_rest(C* __restrict__ s, const C* __rest
         const int k = jb % NS;
         const int idxD = (jb / NS) * NS * R + k;
 #pragma unroll
-        for (int r = 0; r < R; ++r) store(idxD + r * NS, v[m * R + r]);
+        for (int r = 0; r < R; ++r)
+          if (!HALF || 2 * r < R) store(idxD + r * NS, v[m * R + r]);   // position < N/2 iff 2r < R
       }
     } else {
       tile_sync<TX * TPC>();
@@ -104,7 +106,7 @@ __device__ __forceinline__ void fft_tile_rest(C* __restrict__ s, const C* __rest
         for (int r = 0; r < R; ++r) s[xidx<PITCH, SWM>(idxD + r * NS, t)] = v[m * R + r];
       }
       tile_sync<TX * TPC>();
-      fft_tile_rest<LOGN, TX, TPC, SIGN, P + 1, PITCH, STORE_SYNC, SWM>(s, tw, v, t, c, store);
+      fft_tile_rest<LOGN, TX, TPC, SIGN, P + 1, PITCH, STORE_SYNC, SWM, HALF>(s, tw, v, t, c, store);
     }
   }
 }
@@ -114,8 +116,8 @@ __device__ __forceinline__ void fft_tile_rest(C* __restrict__ s, const C* __rest
 // holds position jb + r * N / R0, jb = c + TPC * m (R0 the radix of pass 0).
 // t = column, c = rank of the thread in its column.  SWM: exchange layout
 // (xidx).  LOAD_SYNC / STORE_SYNC as for fft_tile.
-template <int LOGN, int TX, int TPC, int SIGN, int PITCH, bool LOAD_SYNC, bool STORE_SYNC, int SWM, typename C,
-          class Store>
+template <int LOGN, int TX, int TPC, int SIGN, int PITCH, bool LOAD_SYNC, bool STORE_SYNC, int SWM,
+          bool HALF = false, typename C, class Store>
 __device__ __forceinline__ void fft_tile_regs(C* __restrict__ s, const C* __restrict__ tw, C* v, int t, int c,
                                               Store&& store) {
   constexpr int N = 1 << LOGN;
@@ -132,7 +134,8 @@ __device__ __forceinline__ void fft_tile_regs(C* __restrict__ s, const C* __rest
     for (int m = 0; m < NBT; ++m) {
       const int jb = c + TPC * m;
 #pragma unroll
-      for (int r = 0; r < R; ++r) store(jb * R + r, v[m * R + r]);
+      for (int r = 0; r < R; ++r)
+        if (!HALF || 2 * r < R) store(jb * R + r, v[m * R + r]);   // one pass: jb = 0, position r
     }
   } else {
 #pragma unroll
@@ -142,7 +145,7 @@ __device__ __forceinline__ void fft_tile_regs(C* __restrict__ s, const C* __rest
       for (int r = 0; r < R; ++r) s[xidx<PITCH, SWM>(jb * R + r, t)] = v[m * R + r];
     }
     tile_sync<TX * TPC>();
-    fft_tile_rest<LOGN, TX, TPC, SIGN, 1, PITCH, STORE_SYNC, SWM>(s, tw, v, t, c, store);
+    fft_tile_rest<LOGN, TX, TPC, SIGN, 1, PITCH, STORE_SYNC, SWM, HALF>(s, tw, v, t, c, store);
   }
 }
 
@@ -153,8 +156,12 @@ __device__ __forceinline__ void fft_tile_regs(C* __restrict__ s, const C* __rest
 // PITCH: shared-memory row pitch (>= TX).  LOAD_SYNC: barrier between the
 // pass-0 loads and the pass-0 shared-memory writes (loader reads s).
 // STORE_SYNC: barrier before the final stores (storer writes s).
+// HALF: the storer keeps only positions below N/2 (a pruned transform whose
+// kept outputs all lie there); store is not called for the others, so the
+// arithmetic that only feeds them is dropped at compile time, and the kept
+// outputs are computed by the same operations as without HALF.
 template <int LOGN, int TX, int TPC, int SIGN, int PITCH = TX, bool LOAD_SYNC = false, bool STORE_SYNC = false,
-          typename C, class Load, class Store>
+          bool HALF = false, typename C, class Load, class Store>
 __device__ __forceinline__ void fft_tile(C* __restrict__ s, const C* __restrict__ tw, Load&& load, Store&& store) {
   constexpr int N = 1 << LOGN;
   constexpr int ET = N / TPC;
@@ -170,7 +177,7 @@ __device__ __forceinline__ void fft_tile(C* __restrict__ s, const C* __restrict_
 #pragma unroll
     for (int r = 0; r < R; ++r) v[m * R + r] = load(jb, r);   // position jb + r * N / R
   }
-  fft_tile_regs<LOGN, TX, TPC, SIGN, PITCH, LOAD_SYNC, STORE_SYNC, SWM>(s, tw, v, t, c, store);
+  fft_tile_regs<LOGN, TX, TPC, SIGN, PITCH, LOAD_SYNC, STORE_SYNC, SWM, HALF>(s, tw, v, t, c, store);
 }
 
 }  // namespace ss3d

@@ -81,15 +81,16 @@ constexpr int col_min_blocks() {
              ? 1024 / AxisCfg<R, LOGN, V>::NTH
              : 1;
 }
-template <typename R, int LOGN, int SIGN, int V>
+// HALF: every kept output position lies below N/2 (a.nout <= N/2)
+template <typename R, int LOGN, int SIGN, int V, bool HALF = false>
 __global__ void __launch_bounds__(AxisCfg<R, LOGN, V>::NTH, (col_min_blocks<R, LOGN, V>()))
     k_col(AxisArgs a, Geo g, const cpx_t<R>* in, cpx_t<R>* out, Tw tw) {
   extern __shared__ __align__(16) unsigned char smraw[];
   using CF = AxisCfg<R, LOGN, V>;
   if constexpr (V >= 4)
-    col_body_pair<LOGN, CF::TX, CF::TPC, SIGN>(a, g, in, out, tw, blockIdx.x, smraw);
+    col_body_pair<LOGN, CF::TX, CF::TPC, SIGN, HALF>(a, g, in, out, tw, blockIdx.x, smraw);
   else
-    col_body<R, LOGN, CF::TX, CF::TPC, SIGN>(a, g, in, out, tw, blockIdx.x, smraw);
+    col_body<R, LOGN, CF::TX, CF::TPC, SIGN, HALF>(a, g, in, out, tw, blockIdx.x, smraw);
 }
 
 // ---------------------------------------------------------------- middle pass fed by bulk tensor copies
@@ -346,8 +347,9 @@ __global__ void __cluster_dims__(CL, 1, 1) __launch_bounds__(512, 2)
 }
 
 // first inverse pass with the coefficient synthesis fused into the loader
-// (GAUSS: igauss of the realizations, 0 phases, 1 Gaussian coefficients)
-template <typename R, int LOGN, int V, int GAUSS>
+// (GAUSS: igauss of the realizations, 0 phases, 1 Gaussian coefficients;
+// HALF: every kept output position lies below N/2)
+template <typename R, int LOGN, int V, int GAUSS, bool HALF = false>
 __global__ void __launch_bounds__(AxisCfg<R, LOGN, V>::NTH) k_colgen(AxisArgs a, Geo g, const R* __restrict__ amp,
                                                                     const uint32_t* __restrict__ rowstates,
                                                                     const uint32_t* __restrict__ apow,
@@ -355,9 +357,9 @@ __global__ void __launch_bounds__(AxisCfg<R, LOGN, V>::NTH) k_colgen(AxisArgs a,
   extern __shared__ __align__(16) unsigned char smraw[];
   using CF = AxisCfg<R, LOGN, V>;
   if constexpr (V >= 4)
-    colgen_body_pair<LOGN, CF::TX, CF::TPC, GAUSS>(a, g, amp, rowstates, apow, out, tw, blockIdx.x, smraw);
+    colgen_body_pair<LOGN, CF::TX, CF::TPC, GAUSS, HALF>(a, g, amp, rowstates, apow, out, tw, blockIdx.x, smraw);
   else
-    colgen_body<R, LOGN, CF::TX, CF::TPC, GAUSS>(a, g, amp, rowstates, apow, out, tw, blockIdx.x, smraw);
+    colgen_body<R, LOGN, CF::TX, CF::TPC, GAUSS, HALF>(a, g, amp, rowstates, apow, out, tw, blockIdx.x, smraw);
 }
 
 // Standalone synthesis of the full half spectrum of nreal realizations.
@@ -433,13 +435,14 @@ __global__ void __launch_bounds__(RowCfg<R, LOGN, V>::NTH) k_rows_c2r(Geo g, con
                                          smraw);
 }
 
-// x pass with the rows held in warps (rows_warp_body)
-template <typename R, typename O, int LOGN>
+// x pass with the rows held in warps (rows_warp_body); HALF: the crop keeps
+// at most the first N/2 complex values of each packed row ((nx + 1)/2 <= N/2)
+template <typename R, typename O, int LOGN, bool HALF = false>
 __global__ void __launch_bounds__(RowWarpCfg<R, LOGN>::NTH)
     k_rows_warp(Geo g, const cpx_t<R>* __restrict__ in, long long rstride, O* __restrict__ out, long long ostride,
                 int nreal, int nblk_per_r, double* __restrict__ part, Tw tw) {
   extern __shared__ __align__(16) unsigned char smraw[];
-  rows_warp_body<R, O, LOGN>(g, in, rstride, out, ostride, nreal, nblk_per_r, part, tw, blockIdx.x, smraw);
+  rows_warp_body<R, O, LOGN, HALF>(g, in, rstride, out, ostride, nreal, nblk_per_r, part, tw, blockIdx.x, smraw);
 }
 
 // x pass with two rows per lane on packed FP32 (rows_pair_body)
@@ -953,6 +956,9 @@ static cudaError_t set_smem(K kernel, size_t bytes) {
     default: return cudaErrorInvalidValue;                       \
   }
 
+// lengths with pruned (HALF) forms of the inverse passes
+constexpr bool half_len(int L) { return L >= 5 && L <= 10; }
+
 template <typename R> struct MaxL { static constexpr int v = MAX_LOGN_F; };
 template <> struct MaxL<double> { static constexpr int v = MAX_LOGN_D; };
 
@@ -966,12 +972,19 @@ static cudaError_t run_axis_c2c_v(const AxisArgs& a, const Geo& g, const cpx_t<R
     return cudaSuccess;
   } else {
     size_t smem = (size_t)(CF::N * CF::TX + CF::N) * CF::EB;
-    cudaError_t e = set_smem(k_col<R, L, SIGN, V>, smem);
+    auto kern = k_col<R, L, SIGN, V>;
+    // pruned inverse passes that keep at most half of the positions (the
+    // padded grid is at least twice the simulated one along most axes); the
+    // two-line tiles (V >= 4) keep the unpruned form: built pruned, they did
+    // not reproduce the bits of the other tiles at every length
+    if constexpr (SIGN > 0 && half_len(L) && V < 4)
+      if (2 * a.nout <= CF::N) kern = k_col<R, L, SIGN, V, true>;
+    cudaError_t e = set_smem(kern, smem);
     if (e != cudaSuccess) return e;
     AxisArgs b = a;
     b.tpg = (a.lines + CF::LPT - 1) / CF::LPT;
     unsigned blocks = (unsigned)((long long)b.tpg * a.ngroups * a.nreal);
-    k_col<R, L, SIGN, V><<<blocks, CF::NTH, smem, st>>>(b, g, in, out, tw);
+    kern<<<blocks, CF::NTH, smem, st>>>(b, g, in, out, tw);
     ++g_launch_count;
     return cudaGetLastError();
   }
@@ -1069,6 +1082,9 @@ static cudaError_t run_axis_gen_v(const AxisArgs& a, const Geo& g, const R* amp,
   } else {
     size_t smem = (size_t)(CF::N * CF::TX + CF::N) * CF::EB;
     auto kern = g.d == 2 ? k_colgen<R, L, V, 1> : k_colgen<R, L, V, 0>;
+    // pruned form as in run_axis_c2c_v, one-line tiles only
+    if constexpr (half_len(L) && V < 4)
+      if (2 * a.nout <= CF::N) kern = g.d == 2 ? k_colgen<R, L, V, 1, true> : k_colgen<R, L, V, 0, true>;
     cudaError_t e = set_smem(kern, smem);
     if (e != cudaSuccess) return e;
     AxisArgs b = a;
@@ -1104,12 +1120,15 @@ static cudaError_t run_rows_warp(const Geo& g, const cpx_t<R>* in, long long rst
   if constexpr (!W::ok) {
     return run_rows_c2r_v<R, O, L, 0>(g, in, rstride, out, ostride, nreal, part, nblk_out, tw, st);
   } else {
-    cudaError_t e = set_smem(k_rows_warp<R, O, L>, W::smem);
+    auto kern = k_rows_warp<R, O, L>;
+    if constexpr (half_len(L))
+      if ((g.nx + 1) / 2 <= W::N / 2) kern = k_rows_warp<R, O, L, true>;
+    cudaError_t e = set_smem(kern, W::smem);
     if (e != cudaSuccess) return e;
     int nblk = (g.ny * g.nz + W::ROWS - 1) / W::ROWS;
     if (nblk_out) *nblk_out = nblk;
-    k_rows_warp<R, O, L><<<(unsigned)((long long)nblk * nreal), W::NTH, W::smem, st>>>(g, in, rstride, out, ostride,
-                                                                                    nreal, nblk, part, tw);
+    kern<<<(unsigned)((long long)nblk * nreal), W::NTH, W::smem, st>>>(g, in, rstride, out, ostride, nreal, nblk,
+                                                                       part, tw);
     ++g_launch_count;
     return cudaGetLastError();
   }

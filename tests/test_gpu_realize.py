@@ -175,12 +175,14 @@ def _kinds_of(np3):
 
 @pytest.mark.parametrize("igauss", [0, 1])
 @pytest.mark.parametrize("n,ipad", [((40, 36, 20), 1), ((64, 64, 16), 1), ((33, 17, 1), 1), ((1, 24, 12), 1),
-                                     ((100, 1, 30), 1)])
+                                     ((100, 1, 30), 1), ((24, 12, 40), 1), ((4, 4, 200), 1), ((8, 200, 4), 1),
+                                     ((20, 70, 9), 0)])
 def test_two_line_variants_identical(gpu, n, ipad, igauss):
     """FP32 column passes with two adjacent lines per thread (packed FP32
     instructions, variants 4-7) give the bits of the one-line tiles, including
-    grids whose half-spectrum rows end in a padding element and 2D grids whose
-    synthesis runs along y."""
+    grids whose half-spectrum rows end in a padding element, 2D grids whose
+    synthesis runs along y, and columns of 512 (pruned one-line tiles against
+    unpruned two-line tiles) and of 64 positions."""
     from specsim3d_b200 import _lib
     L = _lib.lib()
     sts = [(2, 0.8, 14.0, 9.0, 5.0, 35.0, 10.0, 5.0)]
