@@ -975,9 +975,9 @@ static cudaError_t run_axis_c2c_v(const AxisArgs& a, const Geo& g, const cpx_t<R
     auto kern = k_col<R, L, SIGN, V>;
     // pruned inverse passes that keep at most half of the positions (the
     // padded grid is at least twice the simulated one along most axes); the
-    // two-line tiles (V >= 4) keep the unpruned form: built pruned, they did
-    // not reproduce the bits of the other tiles at every length
-    if constexpr (SIGN > 0 && half_len(L) && V < 4)
+    // two-line tiles (V >= 4) of 64 positions keep the unpruned form: built
+    // pruned, they did not reproduce the bits of the other tiles
+    if constexpr (SIGN > 0 && half_len(L) && (V < 4 || L >= 7))
       if (2 * a.nout <= CF::N) kern = k_col<R, L, SIGN, V, true>;
     cudaError_t e = set_smem(kern, smem);
     if (e != cudaSuccess) return e;
@@ -1082,8 +1082,8 @@ static cudaError_t run_axis_gen_v(const AxisArgs& a, const Geo& g, const R* amp,
   } else {
     size_t smem = (size_t)(CF::N * CF::TX + CF::N) * CF::EB;
     auto kern = g.d == 2 ? k_colgen<R, L, V, 1> : k_colgen<R, L, V, 0>;
-    // pruned form as in run_axis_c2c_v, one-line tiles only
-    if constexpr (half_len(L) && V < 4)
+    // pruned forms as in run_axis_c2c_v
+    if constexpr (half_len(L) && (V < 4 || L >= 7))
       if (2 * a.nout <= CF::N) kern = g.d == 2 ? k_colgen<R, L, V, 1, true> : k_colgen<R, L, V, 0, true>;
     cudaError_t e = set_smem(kern, smem);
     if (e != cudaSuccess) return e;
